@@ -1,0 +1,341 @@
+"""Python view of libdrape_b200.so (the C ABI in include/drape_b200.h) through ctypes.
+
+The names follow the reference's GPU stage: ``solve_equilibrium`` (drape-e7.ts:156-180), the kernel checks
+(run-e7.ts:140-145), ``pcg`` (solver.ts:179-191). The product path is the CUDA library only: importing this module
+raises when the shared object is missing, and there is no CPU fallback.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libdrape_b200.so")
+P = ctypes.c_void_p
+_lib = None
+
+STATUS = {0: "ok", 1: "invalid argument", 2: "cuda error", 3: "diverged", 4: "timeout", 5: "io error", 6: "bad state"}
+REASON = {0: "tolerance", 1: "cap", 2: "stalled", 3: "time_budget"}
+PCG_STATUS = {0: "running", 1: "converged", 2: "iteration_limit", 3: "breakdown", 4: "timeout"}
+
+
+class DrapeError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+class Options(ctypes.Structure):
+    _fields_ = [
+        ("controller", ctypes.c_int32), ("h0", ctypes.c_double), ("h_max", ctypes.c_double),
+        ("h_min_factor", ctypes.c_double), ("growth", ctypes.c_double), ("shrink", ctypes.c_double),
+        ("inner_tolerance", ctypes.c_double), ("inner_max", ctypes.c_int32), ("max_rejections", ctypes.c_int32),
+        ("max_steps", ctypes.c_int32), ("equilibrium_relative", ctypes.c_double),
+        ("equilibrium_absolute", ctypes.c_double), ("pcg_rtol", ctypes.c_double),
+        ("pcg_max_iterations", ctypes.c_int32), ("forcing", ctypes.c_int32), ("replace_every", ctypes.c_int32),
+        ("replace_above", ctypes.c_double), ("refine", ctypes.c_int32), ("refine_rtol", ctypes.c_double),
+        ("curvature", ctypes.c_int32), ("preconditioner", ctypes.c_int32), ("armijo", ctypes.c_double),
+        ("max_halvings", ctypes.c_int32), ("time_budget_s", ctypes.c_double), ("pcg_grid", ctypes.c_int32),
+        ("pcg_threads", ctypes.c_int32), ("pcg_lanes", ctypes.c_int32), ("progress", ctypes.c_int32),
+    ]
+
+
+class RunLog(ctypes.Structure):
+    _fields_ = [
+        ("ptc_steps", ctypes.c_int32), ("newton_iterations", ctypes.c_int32), ("pcg_iterations", ctypes.c_int32),
+        ("rejected_attempts", ctypes.c_int32), ("mu_retries", ctypes.c_int32), ("reason", ctypes.c_int32),
+        ("final_residual", ctypes.c_double), ("final_relative_residual", ctypes.c_double),
+        ("final_h", ctypes.c_double), ("gravity_load", ctypes.c_double), ("static_energy", ctypes.c_double),
+        ("seconds", ctypes.c_double), ("ms_assembly", ctypes.c_double), ("ms_pcg", ctypes.c_double),
+        ("ms_line_search", ctypes.c_double), ("ms_ccd", ctypes.c_double), ("ms_other", ctypes.c_double),
+    ]
+
+    def as_dict(self):
+        d = {name: getattr(self, name) for name, _ in self._fields_}
+        d["reason"] = REASON.get(self.reason, str(self.reason))
+        return d
+
+
+class ProblemView(ctypes.Structure):
+    _fields_ = [
+        ("columns", ctypes.c_int32), ("vertices", ctypes.c_int32), ("triangles", ctypes.c_int32),
+        ("hinges", ctypes.c_int32), ("rows", ctypes.c_int32), ("blocks", ctypes.c_int32),
+        ("start_xyz", P), ("elem_vertices", P), ("elem_geom", P), ("hinge_vertices", P), ("hinge_stiffness", P),
+        ("row_vertex", P), ("row_unit_mass", P), ("row_ptr", P), ("col_idx", P),
+        ("wale", ctypes.c_double), ("course", ctypes.c_double), ("coupling", ctypes.c_double),
+        ("shear", ctypes.c_double), ("gravity", ctypes.c_double * 3), ("colliders", ctypes.c_int32),
+        ("collider_data", P), ("dhat", ctypes.c_double), ("kappa", ctypes.c_double),
+    ]
+
+
+class StepRecord(ctypes.Structure):
+    _fields_ = [("step", ctypes.c_int32), ("inner", ctypes.c_int32), ("rejected", ctypes.c_int32),
+                ("pcg_iterations", ctypes.c_int32), ("h", ctypes.c_double), ("residual", ctypes.c_double),
+                ("min_distance", ctypes.c_double)]
+
+
+def load():
+    """Loads the CUDA library (raises if it has not been built: `python -m drape_b200.build`)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m drape_b200.build`")
+    lib = ctypes.CDLL(LIB_PATH)
+    lib.drape_version.restype = ctypes.c_char_p
+    lib.drape_last_error.restype = ctypes.c_char_p
+    lib.drape_last_error.argtypes = [P]
+    lib.drape_default_options.argtypes = [ctypes.POINTER(Options)]
+    lib.drape_create_sheet.argtypes = [ctypes.c_int32, ctypes.c_uint64, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_int32, ctypes.POINTER(Options), ctypes.c_int32, ctypes.POINTER(P)]
+    lib.drape_create_reference.argtypes = [ctypes.c_int32, ctypes.c_char_p, ctypes.POINTER(Options), ctypes.c_int32,
+                                           ctypes.POINTER(P)]
+    lib.drape_create_from_files.argtypes = [ctypes.c_char_p, ctypes.POINTER(Options), ctypes.c_int32, ctypes.POINTER(P)]
+    lib.drape_destroy.argtypes = [P]
+    lib.drape_sizes.argtypes = [P, P]
+    lib.drape_set_options.argtypes = [P, ctypes.POINTER(Options)]
+    lib.drape_set_state.argtypes = [P, P]
+    lib.drape_get_state.argtypes = [P, P, P]
+    lib.drape_solve_equilibrium.argtypes = [P, P, ctypes.c_double, ctypes.POINTER(RunLog)]
+    lib.drape_step_records.argtypes = [P, P, ctypes.c_int32, P]
+    lib.drape_assemble.argtypes = [P, P, P, ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_int32, P, P]
+    lib.drape_pcg.argtypes = [P, P, P, ctypes.c_double, ctypes.c_int32, P, P, P]
+    lib.drape_energy_change.argtypes = [P, P, P, ctypes.c_double, P, ctypes.c_double, ctypes.c_int32, P]
+    lib.drape_max_step.argtypes = [P, P, P, P]
+    lib.drape_static_residual.argtypes = [P, P, P]
+    lib.drape_static_energy.argtypes = [P, P, P]
+    lib.drape_time_spmv.argtypes = [P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, P]
+    lib.drape_time_assembly.argtypes = [P, ctypes.c_int32, P]
+    lib.drape_create.argtypes = [ctypes.POINTER(ProblemView), ctypes.POINTER(Options), ctypes.c_int32, ctypes.POINTER(P)]
+    lib.drape_write_sheet_problem.argtypes = [ctypes.c_int32, ctypes.c_uint64, ctypes.c_double, ctypes.c_double,
+                                              ctypes.c_int32, ctypes.c_char_p]
+    lib.drape_write_reference_problem.argtypes = [ctypes.c_int32, ctypes.c_char_p, ctypes.c_char_p]
+    lib.drape_inspect_problem.argtypes = [ctypes.c_char_p, P]
+    _lib = lib
+    return lib
+
+
+def default_options(**overrides):
+    o = Options()
+    load().drape_default_options(ctypes.byref(o))
+    for k, v in overrides.items():
+        if not hasattr(o, k):
+            raise AttributeError(f"unknown option {k}")
+        setattr(o, k, v)
+    return o
+
+
+def _ptr(a):
+    return a.ctypes.data_as(P) if a is not None else None
+
+
+def _f64(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Drape:
+    """One drape context on one GPU (``drape_ctx``)."""
+
+    def __init__(self, handle):
+        self.lib = load()
+        self.h = handle
+        sz = np.zeros(6, np.int64)
+        self._check(self.lib.drape_sizes(self.h, _ptr(sz)))
+        self.V, self.T, self.H, self.R, self.B, self.colliders = (int(v) for v in sz)
+
+    @classmethod
+    def _create(cls, fn, *args, options=None, device=0):
+        lib = load()
+        h = P()
+        st = fn(*args, ctypes.byref(options) if options is not None else None, device, ctypes.byref(h))
+        if st != 0:
+            raise DrapeError(st, lib.drape_last_error(None).decode())
+        return cls(h)
+
+    @classmethod
+    def sheet(cls, columns, seed=0, radius=0.25, young=5e5, plane=False, options=None, device=0):
+        return cls._create(load().drape_create_sheet, columns, seed, radius, young, int(plane), options=options,
+                           device=device)
+
+    @classmethod
+    def reference(cls, columns, edit="base", options=None, device=0):
+        return cls._create(load().drape_create_reference, columns, edit.encode(), options=options, device=device)
+
+    @classmethod
+    def from_files(cls, directory, options=None, device=0):
+        return cls._create(load().drape_create_from_files, os.fsencode(directory), options=options, device=device)
+
+    @classmethod
+    def from_arrays(cls, start, row_vertex, unit_mass, row_ptr, col_idx, tri=None, geom=None, hinge=None,
+                    hinge_k=None, material=(0.0, 0.0, 0.0, 0.0), gravity=(0.0, 0.0, -9.81), colliders=None,
+                    dhat=0.0, kappa=0.0, columns=0, options=None, device=0):
+        """A context over caller-owned arrays (the drape_problem_view of the C ABI)."""
+        keep = {
+            "start": _f64(start), "row_vertex": np.ascontiguousarray(row_vertex, np.uint32),
+            "mass": _f64(unit_mass), "row_ptr": np.ascontiguousarray(row_ptr, np.uint32),
+            "col_idx": np.ascontiguousarray(col_idx, np.uint32),
+            "tri": np.ascontiguousarray(tri if tri is not None else np.zeros(0), np.uint32),
+            "geom": _f64(geom if geom is not None else np.zeros(0)),
+            "hinge": np.ascontiguousarray(hinge if hinge is not None else np.zeros(0), np.uint32),
+            "hinge_k": _f64(hinge_k if hinge_k is not None else np.zeros(0)),
+            "colliders": _f64(colliders if colliders is not None else np.zeros(0)),
+        }
+        v = ProblemView()
+        v.columns = columns
+        v.vertices = len(keep["start"]) // 3
+        v.triangles = len(keep["tri"]) // 3
+        v.hinges = len(keep["hinge"]) // 4
+        v.rows = len(keep["row_vertex"])
+        v.blocks = len(keep["col_idx"])
+        v.start_xyz, v.row_vertex, v.row_unit_mass = _ptr(keep["start"]), _ptr(keep["row_vertex"]), _ptr(keep["mass"])
+        v.row_ptr, v.col_idx = _ptr(keep["row_ptr"]), _ptr(keep["col_idx"])
+        v.elem_vertices, v.elem_geom = _ptr(keep["tri"]), _ptr(keep["geom"])
+        v.hinge_vertices, v.hinge_stiffness = _ptr(keep["hinge"]), _ptr(keep["hinge_k"])
+        v.wale, v.course, v.coupling, v.shear = material
+        v.gravity[:] = list(gravity)
+        v.colliders = len(keep["colliders"]) // 8
+        v.collider_data = _ptr(keep["colliders"])
+        v.dhat, v.kappa = dhat, kappa
+        return cls._create(load().drape_create, ctypes.byref(v), options=options, device=device)
+
+    def close(self):
+        if self.h:
+            self.lib.drape_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, st):
+        if st != 0:
+            raise DrapeError(st, self.lib.drape_last_error(self.h).decode())
+
+    def set_options(self, options):
+        self._check(self.lib.drape_set_options(self.h, ctypes.byref(options)))
+
+    @property
+    def state(self):
+        x = np.zeros(3 * self.V)
+        self._check(self.lib.drape_get_state(self.h, _ptr(x), None))
+        return x
+
+    @state.setter
+    def state(self, xyz):
+        self._check(self.lib.drape_set_state(self.h, _ptr(_f64(xyz))))
+
+    def final_h(self):
+        h = ctypes.c_double()
+        self._check(self.lib.drape_get_state(self.h, None, ctypes.byref(h)))
+        return h.value
+
+    def solve_equilibrium(self, start=None, h0=0.0, check=True):
+        log = RunLog()
+        st = self.lib.drape_solve_equilibrium(self.h, _ptr(_f64(start)), h0, ctypes.byref(log))
+        if check:
+            self._check(st)
+        out = log.as_dict()
+        out["status"] = st
+        return out
+
+    def step_records(self):
+        n = ctypes.c_int32()
+        self._check(self.lib.drape_step_records(self.h, None, 0, ctypes.byref(n)))
+        recs = (StepRecord * max(n.value, 1))()
+        self._check(self.lib.drape_step_records(self.h, recs, n.value, ctypes.byref(n)))
+        return [{k: getattr(r, k) for k, _ in StepRecord._fields_} for r in recs[: n.value]]
+
+    def assemble(self, x, x_hat=None, h=0.0, mu=0.0, mode=0, curvature=False, blocks=True):
+        g = np.zeros(3 * self.R)
+        b = np.zeros(9 * self.B, np.float32) if blocks else None
+        self._check(self.lib.drape_assemble(self.h, _ptr(_f64(x)), _ptr(_f64(x_hat)), h, mu, mode, int(curvature),
+                                            _ptr(g), _ptr(b)))
+        return g, b
+
+    def pcg(self, rhs, rtol, max_iterations, blocks=None):
+        sol = np.zeros(3 * self.R)
+        info = np.zeros(3, np.int32)
+        rel = ctypes.c_double()
+        blk = None if blocks is None else np.ascontiguousarray(blocks, np.float32)
+        self._check(self.lib.drape_pcg(self.h, _ptr(blk), _ptr(_f64(rhs)), rtol, max_iterations, _ptr(sol), _ptr(info),
+                                       ctypes.byref(rel)))
+        return sol, {"iterations": int(info[0]), "status": PCG_STATUS.get(int(info[1]), int(info[1])),
+                     "replacements": int(info[2]), "relative": rel.value}
+
+    def energy_change(self, x, d, alpha, x_hat=None, h=0.0, mode=0):
+        out = ctypes.c_double()
+        self._check(self.lib.drape_energy_change(self.h, _ptr(_f64(x)), _ptr(_f64(x_hat)), h, _ptr(_f64(d)), alpha,
+                                                 mode, ctypes.byref(out)))
+        return out.value
+
+    def max_step(self, x, d):
+        out = ctypes.c_double()
+        self._check(self.lib.drape_max_step(self.h, _ptr(_f64(x)), _ptr(_f64(d)), ctypes.byref(out)))
+        return out.value
+
+    def static_residual(self, x=None):
+        out = ctypes.c_double()
+        self._check(self.lib.drape_static_residual(self.h, _ptr(_f64(x)), ctypes.byref(out)))
+        return out.value
+
+    def static_energy(self, x=None):
+        out = ctypes.c_double()
+        self._check(self.lib.drape_static_energy(self.h, _ptr(_f64(x)), ctypes.byref(out)))
+        return out.value
+
+    def time_spmv(self, launches=100, lanes_per_row=8, threads=256):
+        ms = ctypes.c_float()
+        self._check(self.lib.drape_time_spmv(self.h, launches, lanes_per_row, threads, ctypes.byref(ms)))
+        return ms.value
+
+    def time_assembly(self, launches=50):
+        ms = ctypes.c_float()
+        self._check(self.lib.drape_time_assembly(self.h, launches, ctypes.byref(ms)))
+        return ms.value
+
+
+def version():
+    return load().drape_version().decode()
+
+
+def _host_call(st):
+    if st != 0:
+        raise DrapeError(st, load().drape_last_error(None).decode())
+
+
+def write_sheet_problem(directory, columns, seed=0, radius=0.25, young=5e5, plane=False):
+    """problem.json / problem.bin of the sheet over a sphere (host only)."""
+    _host_call(load().drape_write_sheet_problem(columns, seed, radius, young, int(plane), os.fsencode(directory)))
+
+
+def write_reference_problem(directory, columns, edit="base"):
+    """problem.json / problem.bin of the reference's sphere-on-floor scene (host only)."""
+    _host_call(load().drape_write_reference_problem(columns, edit.encode(), os.fsencode(directory)))
+
+
+def inspect_problem(directory):
+    """Reads and validates a problem pair (host only): (V, T, H, R, B, colliders)."""
+    sz = np.zeros(6, np.int64)
+    _host_call(load().drape_inspect_problem(os.fsencode(directory), _ptr(sz)))
+    return tuple(int(v) for v in sz)
+
+
+def read_problem_arrays(directory):
+    """The arrays of a problem.bin as numpy arrays, keyed by manifest name."""
+    import json
+
+    meta = json.load(open(os.path.join(directory, "problem.json")))
+    raw = open(os.path.join(directory, "problem.bin"), "rb").read()
+    out = {}
+    for a in meta["arrays"]:
+        dt = {"f32": np.float32, "f64": np.float64, "u32": np.uint32}[a["dtype"]]
+        out[a["name"]] = np.frombuffer(raw, dt, a["length"], a["offset"]).copy()
+    return meta, out

@@ -1,0 +1,330 @@
+// extern "C" boundary of libdrape_b200.so (declarations and reference citations: include/drape_b200.h).
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "../../include/drape_b200.h"
+#include "context.h"
+
+struct drape_ctx {
+  std::unique_ptr<drape::Context> impl;
+};
+
+namespace {
+
+thread_local std::string g_create_error;
+
+drape_status fail(drape_ctx* ctx, const std::string& msg, drape_status code) {
+  if (ctx && ctx->impl) ctx->impl->last_error = msg;
+  else g_create_error = msg;
+  return code;
+}
+
+template <class F> drape_status guarded(drape_ctx* ctx, F&& fn) {
+  if (!ctx || !ctx->impl) return fail(nullptr, "null or destroyed context", DRAPE_E_STATE);
+  try {
+    return fn(*ctx->impl);
+  } catch (const drape::CudaError& e) {
+    return fail(ctx, e.what(), e.code == cudaErrorLaunchTimeout ? DRAPE_E_TIMEOUT : DRAPE_E_CUDA);
+  } catch (const std::invalid_argument& e) {
+    return fail(ctx, e.what(), DRAPE_E_ARG);
+  } catch (const std::exception& e) {
+    return fail(ctx, e.what(), DRAPE_E_ARG);
+  }
+}
+
+drape_status create(const drape::HostProblem& p, const drape_options* options, int32_t device, drape_ctx** out) {
+  if (!out) return fail(nullptr, "out is null", DRAPE_E_ARG);
+  *out = nullptr;
+  drape_options opt;
+  if (options) opt = *options;
+  else drape_default_options(&opt);
+  try {
+    auto ctx = std::make_unique<drape_ctx>();
+    ctx->impl = std::make_unique<drape::Context>(p, opt, device);
+    *out = ctx.release();
+    return DRAPE_OK;
+  } catch (const drape::CudaError& e) {
+    return fail(nullptr, e.what(), DRAPE_E_CUDA);
+  } catch (const std::exception& e) {
+    return fail(nullptr, e.what(), DRAPE_E_ARG);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* drape_version(void) { return "drape_b200 0.1 (sm_100a)"; }
+
+void drape_default_options(drape_options* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof *o);
+  o->controller = 1;
+  o->h0 = 1e-3;
+  o->h_max = 1.0;
+  o->h_min_factor = 0.1;
+  o->growth = 2.0;
+  o->shrink = 0.5;
+  o->inner_tolerance = 0.1;
+  o->inner_max = 10;
+  o->max_rejections = 12;
+  o->max_steps = 1000;
+  o->equilibrium_relative = 0.0;
+  o->equilibrium_absolute = 1e-6;
+  o->pcg_rtol = 1e-6;
+  o->pcg_max_iterations = 2000;
+  o->forcing = 0;
+  o->replace_every = 0;
+  o->replace_above = 1e-2;
+  o->refine = 1;
+  o->refine_rtol = 0.1;
+  o->curvature = 0;
+  o->preconditioner = 0;
+  o->armijo = 1e-4;
+  o->max_halvings = 30;
+  o->time_budget_s = 0.0;
+}
+
+drape_status drape_create(const drape_problem_view* v, const drape_options* options, int32_t device, drape_ctx** out) {
+  if (!v) return fail(nullptr, "problem view is null", DRAPE_E_ARG);
+  if (v->vertices <= 0 || v->rows <= 0 || v->triangles < 0 || v->hinges < 0 || v->blocks <= 0 || v->colliders < 0)
+    return fail(nullptr, "negative or empty problem sizes", DRAPE_E_ARG);
+  if (!v->start_xyz || !v->row_vertex || !v->row_unit_mass || !v->row_ptr || !v->col_idx ||
+      (v->triangles && (!v->elem_vertices || !v->elem_geom)) ||
+      (v->hinges && (!v->hinge_vertices || !v->hinge_stiffness)) || (v->colliders && !v->collider_data))
+    return fail(nullptr, "a required problem array is null", DRAPE_E_ARG);
+  drape::HostProblem p;
+  p.columns = v->columns;
+  p.V = v->vertices;
+  p.T = v->triangles;
+  p.H = v->hinges;
+  p.R = v->rows;
+  p.B = v->blocks;
+  p.start.assign(v->start_xyz, v->start_xyz + 3 * size_t(p.V));
+  p.tri.assign(v->elem_vertices, v->elem_vertices + 3 * size_t(p.T));
+  p.tri_geom.assign(v->elem_geom, v->elem_geom + 7 * size_t(p.T));
+  p.hinge.assign(v->hinge_vertices, v->hinge_vertices + 4 * size_t(p.H));
+  p.hinge_k.assign(v->hinge_stiffness, v->hinge_stiffness + p.H);
+  p.row_vertex.assign(v->row_vertex, v->row_vertex + p.R);
+  p.unit_mass.assign(v->row_unit_mass, v->row_unit_mass + p.R);
+  p.row_ptr.assign(v->row_ptr, v->row_ptr + p.R + 1);
+  p.col_idx.assign(v->col_idx, v->col_idx + p.B);
+  p.wale = v->wale;
+  p.course = v->course;
+  p.coupling = v->coupling;
+  p.shear = v->shear;
+  for (int k = 0; k < 3; ++k) p.gravity[k] = v->gravity[k];
+  p.colliders.assign(v->collider_data, v->collider_data + 8 * size_t(v->colliders));
+  p.dhat = v->dhat;
+  p.kappa = v->kappa;
+  std::string err = drape::validate(p);
+  if (!err.empty()) return fail(nullptr, "inconsistent problem: " + err, DRAPE_E_ARG);
+  return create(p, options, device, out);
+}
+
+drape_status drape_create_from_files(const char* dir, const drape_options* options, int32_t device, drape_ctx** out) {
+  if (!dir) return fail(nullptr, "dir is null", DRAPE_E_ARG);
+  try {
+    return create(drape::read_problem_files(dir), options, device, out);
+  } catch (const std::exception& e) {
+    return fail(nullptr, e.what(), DRAPE_E_IO);
+  }
+}
+
+drape_status drape_create_sheet(int32_t columns, uint64_t seed, double radius, double young, int32_t plane,
+                                const drape_options* options, int32_t device, drape_ctx** out) {
+  if (columns < 3 || !(radius > 0) || !(young > 0)) return fail(nullptr, "invalid sheet parameters", DRAPE_E_ARG);
+  try {
+    return create(drape::sheet_problem(columns, seed, radius, young, plane != 0), options, device, out);
+  } catch (const std::exception& e) {
+    return fail(nullptr, e.what(), DRAPE_E_ARG);
+  }
+}
+
+drape_status drape_create_reference(int32_t columns, const char* edit, const drape_options* options, int32_t device,
+                                    drape_ctx** out) {
+  if (columns < 3) return fail(nullptr, "invalid column count", DRAPE_E_ARG);
+  try {
+    return create(drape::reference_problem(columns, edit ? edit : "base"), options, device, out);
+  } catch (const std::exception& e) {
+    return fail(nullptr, e.what(), DRAPE_E_ARG);
+  }
+}
+
+drape_status drape_write_sheet_problem(int32_t columns, uint64_t seed, double radius, double young, int32_t plane,
+                                       const char* dir) {
+  if (!dir || columns < 3 || !(radius > 0) || !(young > 0)) return fail(nullptr, "invalid arguments", DRAPE_E_ARG);
+  try {
+    drape::write_problem_files(drape::sheet_problem(columns, seed, radius, young, plane != 0), dir);
+    return DRAPE_OK;
+  } catch (const std::exception& e) {
+    return fail(nullptr, e.what(), DRAPE_E_IO);
+  }
+}
+
+drape_status drape_write_reference_problem(int32_t columns, const char* edit, const char* dir) {
+  if (!dir || columns < 3) return fail(nullptr, "invalid arguments", DRAPE_E_ARG);
+  try {
+    drape::write_problem_files(drape::reference_problem(columns, edit ? edit : "base"), dir);
+    return DRAPE_OK;
+  } catch (const std::exception& e) {
+    return fail(nullptr, e.what(), DRAPE_E_IO);
+  }
+}
+
+drape_status drape_inspect_problem(const char* dir, int64_t* out) {
+  if (!dir || !out) return fail(nullptr, "invalid arguments", DRAPE_E_ARG);
+  try {
+    drape::HostProblem p = drape::read_problem_files(dir);
+    out[0] = p.V;
+    out[1] = p.T;
+    out[2] = p.H;
+    out[3] = p.R;
+    out[4] = p.B;
+    out[5] = p.collider_count();
+    return DRAPE_OK;
+  } catch (const std::exception& e) {
+    return fail(nullptr, e.what(), DRAPE_E_IO);
+  }
+}
+
+void drape_destroy(drape_ctx* ctx) { delete ctx; }
+
+const char* drape_last_error(const drape_ctx* ctx) {
+  if (ctx && ctx->impl) return ctx->impl->last_error.c_str();
+  return g_create_error.c_str();
+}
+
+drape_status drape_sizes(const drape_ctx* ctx, int64_t* out) {
+  if (!ctx || !ctx->impl || !out) return DRAPE_E_ARG;
+  const auto& p = ctx->impl->problem();
+  out[0] = p.V;
+  out[1] = p.T;
+  out[2] = p.H;
+  out[3] = p.R;
+  out[4] = p.B;
+  out[5] = p.collider_count();
+  return DRAPE_OK;
+}
+
+drape_status drape_set_options(drape_ctx* ctx, const drape_options* options) {
+  return guarded(ctx, [&](drape::Context& c) {
+    if (!options) return fail(ctx, "options is null", DRAPE_E_ARG);
+    c.options() = *options;
+    return DRAPE_OK;
+  });
+}
+
+drape_status drape_set_state(drape_ctx* ctx, const double* xyz) {
+  return guarded(ctx, [&](drape::Context& c) {
+    if (!xyz) return fail(ctx, "xyz is null", DRAPE_E_ARG);
+    c.set_positions(xyz);
+    return DRAPE_OK;
+  });
+}
+
+drape_status drape_get_state(const drape_ctx* cctx, double* xyz, double* final_h) {
+  auto* ctx = const_cast<drape_ctx*>(cctx);
+  return guarded(ctx, [&](drape::Context& c) {
+    if (xyz) c.get_positions(xyz);
+    if (final_h) *final_h = c.final_h();
+    return DRAPE_OK;
+  });
+}
+
+drape_status drape_solve_equilibrium(drape_ctx* ctx, const double* start, double h0, drape_run_log* log) {
+  return guarded(ctx, [&](drape::Context& c) {
+    int reason = c.solve_equilibrium(start, h0, log);
+    if (reason == 2) return fail(ctx, "the solve stalled: no PTC step could be taken", DRAPE_E_DIVERGED);
+    if (reason == 3) return fail(ctx, "time budget exhausted", DRAPE_E_TIMEOUT);
+    return DRAPE_OK;
+  });
+}
+
+drape_status drape_step_records(const drape_ctx* cctx, drape_step_record* out, int32_t capacity, int32_t* count) {
+  auto* ctx = const_cast<drape_ctx*>(cctx);
+  return guarded(ctx, [&](drape::Context& c) {
+    const auto& s = c.steps();
+    if (count) *count = int32_t(s.size());
+    for (int32_t i = 0; out && i < capacity && i < int32_t(s.size()); ++i) out[i] = s[size_t(i)];
+    return DRAPE_OK;
+  });
+}
+
+drape_status drape_assemble(drape_ctx* ctx, const double* x, const double* x_hat, double h, double mu, int32_t mode,
+                            int32_t curvature, double* grad, float* blocks) {
+  return guarded(ctx, [&](drape::Context& c) {
+    if (!x || (mode == 0 && (!x_hat || !(h > 0))) || (mode != 0 && mode != 1))
+      return fail(ctx, "assemble needs x, and x_hat with h > 0 in mode 0", DRAPE_E_ARG);
+    c.assemble_host(x, x_hat, h, mu, mode, curvature, grad, blocks);
+    return DRAPE_OK;
+  });
+}
+
+drape_status drape_pcg(drape_ctx* ctx, const float* blocks, const double* rhs, double rtol, int32_t max_iterations,
+                       double* solution, int32_t* info, double* relative) {
+  return guarded(ctx, [&](drape::Context& c) {
+    if (!rhs || !solution || !(rtol > 0) || max_iterations < 1) return fail(ctx, "invalid PCG arguments", DRAPE_E_ARG);
+    drape::PcgResult r = c.pcg_host(blocks, rhs, rtol, max_iterations, solution);
+    if (info) {
+      info[0] = r.iterations;
+      info[1] = r.status;
+      info[2] = r.replacements;
+    }
+    if (relative) *relative = r.relative;
+    return DRAPE_OK;
+  });
+}
+
+drape_status drape_energy_change(drape_ctx* ctx, const double* x, const double* x_hat, double h, const double* d,
+                                 double alpha, int32_t mode, double* out) {
+  return guarded(ctx, [&](drape::Context& c) {
+    if (!x || !d || !out || (mode == 0 && (!x_hat || !(h > 0)))) return fail(ctx, "invalid arguments", DRAPE_E_ARG);
+    *out = c.energy_change_host(x, x_hat, h, d, alpha, mode);
+    return DRAPE_OK;
+  });
+}
+
+drape_status drape_max_step(drape_ctx* ctx, const double* x, const double* d, double* out) {
+  return guarded(ctx, [&](drape::Context& c) {
+    if (!x || !d || !out) return fail(ctx, "invalid arguments", DRAPE_E_ARG);
+    *out = c.max_step_host(x, d);
+    return DRAPE_OK;
+  });
+}
+
+drape_status drape_static_residual(drape_ctx* ctx, const double* x, double* out) {
+  return guarded(ctx, [&](drape::Context& c) {
+    if (!out) return fail(ctx, "out is null", DRAPE_E_ARG);
+    if (x) c.set_positions(x);
+    *out = c.static_residual();
+    return DRAPE_OK;
+  });
+}
+
+drape_status drape_static_energy(drape_ctx* ctx, const double* x, double* out) {
+  return guarded(ctx, [&](drape::Context& c) {
+    if (!out) return fail(ctx, "out is null", DRAPE_E_ARG);
+    *out = x ? c.static_energy_host(x) : c.static_energy();
+    return DRAPE_OK;
+  });
+}
+
+drape_status drape_time_spmv(drape_ctx* ctx, int32_t launches, int32_t lanes_per_row, int32_t threads, float* ms) {
+  return guarded(ctx, [&](drape::Context& c) {
+    if (launches < 1 || !ms || threads < 32 || threads % 32 || threads > 1024) return fail(ctx, "invalid arguments", DRAPE_E_ARG);
+    *ms = c.time_spmv(launches, lanes_per_row, threads);
+    return DRAPE_OK;
+  });
+}
+
+drape_status drape_time_assembly(drape_ctx* ctx, int32_t launches, float* ms) {
+  return guarded(ctx, [&](drape::Context& c) {
+    if (launches < 1 || !ms) return fail(ctx, "invalid arguments", DRAPE_E_ARG);
+    *ms = c.time_assembly(launches);
+    return DRAPE_OK;
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,633 @@
+// The drape GPU stage on one device: problem upload, Newton-step operations and the PTC driver.
+// Host-side rules follow the reference's GPU host loop and oracle:
+//   PTC step / attempts / rejection   drape-e7.ts:97-180, e7_ptc.rs:129-189
+//   regularised inexact Newton        robust-newton.ts:312-441 (mu schedule newton.rs:113-125, forcing
+//                                     e4_rules.rs:15-22), Armijo from the CCD bound newton.rs:158-167
+//   controller                        e7_ptc.rs:30-35 (inner-count) or x2 per accepted step (doubling)
+#include "context.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+namespace drape {
+
+// Energy, minimum-distance kernels live in elem.cu.
+cudaError_t launch_static_energy(const DevProblem& p, const double* x, double* partial, int grid, cudaStream_t s);
+cudaError_t launch_min_distance(const DevProblem& p, const double* x, double* partial, int grid, cudaStream_t s);
+
+void check(cudaError_t e, const char* where) {
+  if (e != cudaSuccess) throw CudaError(e, where);
+}
+
+template <class T> void DeviceArray<T>::alloc(size_t count) {
+  release();
+  n = count;
+  if (count) check(cudaMalloc(&ptr, count * sizeof(T)), "cudaMalloc");
+}
+template <class T> void DeviceArray<T>::upload(const T* host, size_t count, cudaStream_t s) {
+  if (count > n) throw std::runtime_error("upload larger than the device array");
+  if (count) check(cudaMemcpyAsync(ptr, host, count * sizeof(T), cudaMemcpyHostToDevice, s), "upload");
+}
+template <class T> void DeviceArray<T>::download(T* host, size_t count, cudaStream_t s) const {
+  if (count > n) throw std::runtime_error("download larger than the device array");
+  if (count) check(cudaMemcpyAsync(host, ptr, count * sizeof(T), cudaMemcpyDeviceToHost, s), "download");
+}
+
+namespace {
+
+constexpr int kReduceGrid = 296;
+enum Slot { kNorm = 0, kSlope, kAlpha, kDelta, kEnergy, kMinDist, kRefine, kInf, kSlots = 16 };
+enum Phase { kAssembly = 0, kPcg, kLineSearch, kCcd, kOther };
+
+double raise_mu(double mu) { return std::min(std::max(10.0 * mu, 1e-3), 1e3); }
+double relax_mu(double mu) { return mu / 10.0 < 1e-3 ? 0.0 : mu / 10.0; }
+
+// Eisenstat-Walker choice 2 (e4_rules.rs:15-22).
+double next_forcing(double previous, double ratio) {
+  double eta = 0.9 * ratio * ratio, safeguard = 0.9 * previous * previous;
+  double guarded = safeguard > 0.1 ? std::max(eta, safeguard) : eta;
+  return std::min(std::max(guarded, 1e-7), 1e-2);
+}
+
+}  // namespace
+
+Context::Context(const HostProblem& problem, const drape_options& options, int device)
+    : host_(problem), opt_(options), device_(device) {
+  std::string err = validate(host_);
+  if (!err.empty()) throw std::invalid_argument("inconsistent problem: " + err);
+  check(cudaSetDevice(device_), "cudaSetDevice");
+  check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  for (auto& e : ev_) check(cudaEventCreate(&e), "cudaEventCreate");
+  check(cudaMallocHost(&pinned_, kSlots * sizeof(double)), "cudaMallocHost");
+  check(cudaMallocHost(&pinned_state_, sizeof(PcgState)), "cudaMallocHost");
+  upload_problem();
+}
+
+Context::~Context() {
+  if (stream_) cudaStreamSynchronize(stream_);
+  for (auto& e : ev_)
+    if (e) cudaEventDestroy(e);
+  if (pinned_) cudaFreeHost(pinned_);
+  if (pinned_state_) cudaFreeHost(pinned_state_);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Context::upload_problem() {
+  const HostProblem& p = host_;
+  const int V = p.V, T = p.T, H = p.H, R = p.R, B = p.B;
+  // Row-centric element maps: for every row, its incident triangles and hinges in element order, each with the
+  // block slot (within the row) of every element vertex.
+  std::vector<int> vertex_row(V, -1);
+  for (int r = 0; r < R; ++r) vertex_row[p.row_vertex[r]] = r;
+  auto slot_of = [&](int r, int c) -> int {
+    if (c < 0) return -1;
+    auto b = p.col_idx.begin() + p.row_ptr[r], e = p.col_idx.begin() + p.row_ptr[r + 1];
+    auto it = std::lower_bound(b, e, c);
+    if (it == e || *it != c) throw std::invalid_argument("element coupling outside the BSR pattern");
+    return int(it - b);
+  };
+  std::vector<std::vector<int>> rt(R), rh(R);
+  for (int t = 0; t < T; ++t)
+    for (int k = 0; k < 3; ++k) {
+      int r = vertex_row[p.tri[3 * t + k]];
+      if (r >= 0) rt[r].push_back(t << 2 | k);
+    }
+  for (int h = 0; h < H; ++h)
+    for (int k = 0; k < 4; ++k) {
+      int r = vertex_row[p.hinge[4 * h + k]];
+      if (r >= 0) rh[r].push_back(h << 2 | k);
+    }
+  std::vector<int> rt_ptr{0}, rt_ent, rt_pos, rh_ptr{0}, rh_ent, rh_pos, diag_slot(R), diag_pos(R);
+  int max_entries = 0, max_blocks = 0;
+  for (int r = 0; r < R; ++r) {
+    for (int ent : rt[r]) {
+      rt_ent.push_back(ent);
+      for (int l = 0; l < 3; ++l) rt_pos.push_back(slot_of(r, vertex_row[p.tri[3 * (ent >> 2) + l]]));
+    }
+    for (int ent : rh[r]) {
+      rh_ent.push_back(ent);
+      for (int l = 0; l < 4; ++l) rh_pos.push_back(slot_of(r, vertex_row[p.hinge[4 * (ent >> 2) + l]]));
+    }
+    rt_ptr.push_back(int(rt_ent.size()));
+    rh_ptr.push_back(int(rh_ent.size()));
+    max_entries = std::max(max_entries, int(rt[r].size() + rh[r].size()));
+    max_blocks = std::max(max_blocks, p.row_ptr[r + 1] - p.row_ptr[r]);
+    diag_slot[r] = slot_of(r, r);
+    diag_pos[r] = p.row_ptr[r] + diag_slot[r];
+  }
+  if (max_entries > kMaxRowEntries)
+    throw std::invalid_argument("a row has " + std::to_string(max_entries) + " incident elements (limit " +
+                                std::to_string(kMaxRowEntries) + ")");
+  if (max_blocks > kMaxRowBlocks)
+    throw std::invalid_argument("a row has " + std::to_string(max_blocks) + " blocks (limit " +
+                                std::to_string(kMaxRowBlocks) + ")");
+
+  geom_.alloc(7 * size_t(T));
+  geom_.upload(p.tri_geom.data(), geom_.n, stream_);
+  tri_.alloc(3 * size_t(T));
+  tri_.upload(p.tri.data(), tri_.n, stream_);
+  hinge_.alloc(4 * size_t(H));
+  hinge_.upload(p.hinge.data(), hinge_.n, stream_);
+  hinge_k_.alloc(H);
+  hinge_k_.upload(p.hinge_k.data(), H, stream_);
+  row_vertex_.alloc(R);
+  row_vertex_.upload(p.row_vertex.data(), R, stream_);
+  unit_mass_.alloc(R);
+  unit_mass_.upload(p.unit_mass.data(), R, stream_);
+  row_ptr_.alloc(R + 1);
+  row_ptr_.upload(p.row_ptr.data(), R + 1, stream_);
+  col_idx_.alloc(B);
+  col_idx_.upload(p.col_idx.data(), B, stream_);
+  diag_slot_.alloc(R);
+  diag_slot_.upload(diag_slot.data(), R, stream_);
+  diag_pos_.alloc(R);
+  diag_pos_.upload(diag_pos.data(), R, stream_);
+  auto up = [&](DeviceArray<int>& d, const std::vector<int>& h) {
+    d.alloc(std::max<size_t>(h.size(), 1));
+    d.upload(h.data(), h.size(), stream_);
+  };
+  up(rt_ptr_, rt_ptr);
+  up(rt_ent_, rt_ent);
+  up(rt_pos_, rt_pos);
+  up(rh_ptr_, rh_ptr);
+  up(rh_ent_, rh_ent);
+  up(rh_pos_, rh_pos);
+  colliders_.alloc(std::max<size_t>(p.colliders.size(), 8));
+  colliders_.upload(p.colliders.data(), p.colliders.size(), stream_);
+
+  const size_t nv = 3 * size_t(V);
+  for (auto* a : {&x_, &xn_, &xhat_, &xt_, &d_, &towards_}) a->alloc(nv);
+  x_.upload(p.start.data(), nv, stream_);
+  g_.alloc(3 * size_t(R));
+  partial_grid_ = std::max(assemble_grid(R), kReduceGrid);
+  partial_.alloc(partial_grid_);
+  scalars_.alloc(kSlots);
+  a0_.alloc(B);
+  a1_.alloc(B);
+  a2_.alloc(B);
+  for (auto* a : {&b_, &px_, &pr_, &pz_, &pp0_, &pp1_, &pq_, &sol_, &corr_}) a->alloc(R);
+  dinv_.alloc(3 * size_t(R));
+  pcg_state_.alloc(1);
+  for (auto* a : {&b_, &px_, &pr_, &pz_, &pp0_, &pp1_, &pq_, &sol_, &corr_})
+    check(cudaMemsetAsync(a->ptr, 0, sizeof(float4) * a->n, stream_), "memset");
+
+  dp_ = DevProblem{};
+  dp_.V = V;
+  dp_.T = T;
+  dp_.H = H;
+  dp_.R = R;
+  dp_.B = B;
+  dp_.ncol = p.collider_count();
+  dp_.max_row_blocks = max_blocks;
+  dp_.max_row_entries = max_entries;
+  dp_.geom = geom_.ptr;
+  dp_.tri = tri_.ptr;
+  dp_.hinge = hinge_.ptr;
+  dp_.hinge_k = hinge_k_.ptr;
+  dp_.row_vertex = row_vertex_.ptr;
+  dp_.unit_mass = unit_mass_.ptr;
+  dp_.row_ptr = row_ptr_.ptr;
+  dp_.col_idx = col_idx_.ptr;
+  dp_.diag_slot = diag_slot_.ptr;
+  dp_.rt_ptr = rt_ptr_.ptr;
+  dp_.rt_ent = rt_ent_.ptr;
+  dp_.rt_pos = rt_pos_.ptr;
+  dp_.rh_ptr = rh_ptr_.ptr;
+  dp_.rh_ent = rh_ent_.ptr;
+  dp_.rh_pos = rh_pos_.ptr;
+  dp_.colliders = colliders_.ptr;
+  dp_.wale = p.wale;
+  dp_.course = p.course;
+  dp_.coupling = p.coupling;
+  dp_.shear = p.shear;
+  for (int k = 0; k < 3; ++k) dp_.gravity[k] = p.gravity[k];
+  dp_.dhat = p.dhat;
+  dp_.kappa = p.kappa;
+
+  double gn = std::sqrt(p.gravity[0] * p.gravity[0] + p.gravity[1] * p.gravity[1] + p.gravity[2] * p.gravity[2]);
+  double s = 0;
+  for (double m : p.unit_mass) s += (m * gn) * (m * gn);
+  gravity_load_ = std::sqrt(s);
+
+  // PCG launch shape: one CTA per ~64 rows up to one per SM (fewer CTAs = cheaper grid barriers).
+  pcg_cfg_.lanes_per_row = opt_.pcg_lanes > 0 ? opt_.pcg_lanes : 8;
+  pcg_cfg_.threads = opt_.pcg_threads > 0 ? opt_.pcg_threads : 256;
+  int sms = 0;
+  check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_), "attribute");
+  int cap = pcg_max_grid(pcg_cfg_.threads, pcg_cfg_.lanes_per_row);
+  if (cap <= 0) throw std::invalid_argument("unsupported PCG launch shape");
+  int want = opt_.pcg_grid > 0 ? opt_.pcg_grid : std::min(sms, (R + 63) / 64);
+  pcg_cfg_.grid = std::max(1, std::min(want, cap));
+  sync();
+}
+
+void Context::sync() { check(cudaStreamSynchronize(stream_), "stream synchronize"); }
+
+double Context::read_scalar(int slot) {
+  check(cudaMemcpyAsync(pinned_ + slot, scalars_.ptr + slot, sizeof(double), cudaMemcpyDeviceToHost, stream_), "read");
+  sync();
+  return pinned_[slot];
+}
+
+double Context::reduce_partials(int n, int op, int slot) {
+  check(launch_reduce(partial_.ptr, n, op, scalars_.ptr, slot, stream_), "reduce");
+  return read_scalar(slot);
+}
+
+void Context::set_positions(const double* xyz) {
+  x_.upload(xyz, 3 * size_t(host_.V), stream_);
+  sync();
+}
+
+void Context::get_positions(double* xyz) const {
+  x_.download(xyz, 3 * size_t(host_.V), stream_);
+  check(cudaStreamSynchronize(stream_), "stream synchronize");
+}
+
+double Context::assemble(const double* x, double inv_h2, double mu, int mode, bool hessian) {
+  AssembleArgs a{};
+  a.p = dp_;
+  a.x = x;
+  a.x_hat = xhat_.ptr;
+  a.inv_h2 = inv_h2;
+  a.mu = mu;
+  a.mode = mode;
+  a.curvature = opt_.curvature;
+  a.grad = g_.ptr;
+  a.bsr = hessian ? DevBsr{a0_.ptr, a1_.ptr, a2_.ptr} : DevBsr{nullptr, nullptr, nullptr};
+  a.partial = partial_.ptr;
+  check(launch_assemble(a, stream_), "assemble");
+  return std::sqrt(reduce_partials(assemble_grid(host_.R), 0, kNorm));
+}
+
+PcgResult Context::pcg(double rtol, int max_iterations) {
+  PcgArgs a{};
+  a.R = host_.R;
+  a.row_ptr = row_ptr_.ptr;
+  a.col_idx = col_idx_.ptr;
+  a.diag_pos = diag_pos_.ptr;
+  a.A = DevBsr{a0_.ptr, a1_.ptr, a2_.ptr};
+  a.b = b_.ptr;
+  a.x = px_.ptr;
+  a.r = pr_.ptr;
+  a.z = pz_.ptr;
+  a.p0 = pp0_.ptr;
+  a.p1 = pp1_.ptr;
+  a.q = pq_.ptr;
+  a.dinv = dinv_.ptr;
+  a.state = pcg_state_.ptr;
+  a.tol2 = float(rtol * rtol);
+  a.max_iterations = max_iterations;
+  a.replace_every = opt_.replace_every;
+  a.replace_above2 = float(opt_.replace_above * opt_.replace_above);
+  a.spin_limit = 4000000000LL;  // ~2 s of SM clock per barrier wait
+  if (pcg_partial_.n < 3 * size_t(pcg_cfg_.grid)) pcg_partial_.alloc(3 * size_t(pcg_cfg_.grid));
+  a.partial = pcg_partial_.ptr;
+  check(cudaMemsetAsync(pcg_state_.ptr, 0, sizeof(PcgState), stream_), "memset");
+  check(cudaEventRecord(ev_[0], stream_), "event");
+  check(launch_pcg(a, pcg_cfg_, stream_), "pcg launch");
+  check(cudaEventRecord(ev_[1], stream_), "event");
+  check(cudaMemcpyAsync(pinned_state_, pcg_state_.ptr, sizeof(PcgState), cudaMemcpyDeviceToHost, stream_), "read");
+  sync();
+  PcgResult r;
+  cudaEventElapsedTime(&r.ms, ev_[0], ev_[1]);
+  phase_ms_[kPcg] += r.ms;
+  const PcgState& s = *pinned_state_;
+  if (s.error) throw CudaError(cudaErrorLaunchTimeout, "PCG grid barrier gave up waiting");
+  r.iterations = s.iterations;
+  r.status = s.status;
+  r.replacements = s.replacements;
+  r.relative = s.rr0 > 0 ? std::sqrt(double(s.rr) / double(s.rr0)) : 0.0;
+  return r;
+}
+
+double Context::max_step(const double* x, const double* d) {
+  check(launch_max_step(dp_, x, d, partial_.ptr, kReduceGrid, stream_), "max_step");
+  return reduce_partials(kReduceGrid, 1, kAlpha);
+}
+
+double Context::energy_change(const double* x, const double* d, double alpha, double inv_h2, int mode) {
+  EnergyArgs a{dp_, x, xhat_.ptr, d, alpha, inv_h2, mode, partial_.ptr};
+  check(launch_energy_change(a, kReduceGrid, stream_), "energy_change");
+  return reduce_partials(kReduceGrid, 0, kDelta);
+}
+
+double Context::static_residual() { return assemble(x_.ptr, 0.0, 0.0, 1, false); }
+
+double Context::static_energy() {
+  check(launch_static_energy(dp_, x_.ptr, partial_.ptr, kReduceGrid, stream_), "static_energy");
+  return reduce_partials(kReduceGrid, 0, kEnergy);
+}
+
+// One attempt at step size h from xn_ (into x_): feasible start, then the regularised inexact Newton.
+AttemptResult Context::attempt(double h, double scale) {
+  AttemptResult res;
+  const double inv_h2 = 1.0 / (h * h);
+  const size_t nv = 3 * size_t(host_.V);
+  auto t_phase = [&](int phase, auto&& fn) {
+    auto t0 = std::chrono::steady_clock::now();
+    auto out = fn();
+    phase_ms_[phase] += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return out;
+  };
+  check(launch_predict(dp_, xn_.ptr, h * h, xhat_.ptr, stream_), "predict");
+  check(launch_sub(int(nv), xhat_.ptr, xn_.ptr, towards_.ptr, stream_), "towards");
+  double a0 = t_phase(kCcd, [&] { return max_step(xn_.ptr, towards_.ptr); });
+  check(launch_axpy(int(nv), xn_.ptr, a0, towards_.ptr, x_.ptr, stream_), "start");
+  double mu = 0.0, eta = opt_.forcing ? 1e-2 : opt_.pcg_rtol, prev_norm = 0.0;
+  for (int it = 0;; ++it) {
+    double norm = t_phase(kAssembly, [&] { return assemble(x_.ptr, inv_h2, mu, 0, true); });
+    double rel = norm / scale;
+    if (!std::isfinite(rel)) {
+      res.non_finite = true;
+      return res;
+    }
+    if (rel <= opt_.inner_tolerance) {
+      res.status = 0;
+      return res;
+    }
+    if (it == opt_.inner_max) {
+      res.status = 1;
+      return res;
+    }
+    if (opt_.forcing) eta = it == 0 ? 1e-2 : next_forcing(eta, norm / prev_norm);
+    prev_norm = norm;
+    double slope = 0.0;
+    for (;;) {
+      res.max_mu = std::max(res.max_mu, mu);
+      check(launch_rhs(host_.R, g_.ptr, b_.ptr, stream_), "rhs");
+      PcgResult pr = pcg(eta, opt_.pcg_max_iterations);
+      res.pcg_iterations += pr.iterations;
+      check(cudaMemcpyAsync(sol_.ptr, px_.ptr, sizeof(float4) * host_.R, cudaMemcpyDeviceToDevice, stream_), "copy");
+      if (opt_.refine && pr.status != kPcgBreakdown) {
+        check(launch_refine_residual(host_.R, row_ptr_.ptr, col_idx_.ptr, DevBsr{a0_.ptr, a1_.ptr, a2_.ptr}, g_.ptr,
+                                     sol_.ptr, b_.ptr, partial_.ptr, kReduceGrid, stream_),
+              "refine");
+        PcgResult pc = pcg(opt_.refine_rtol, opt_.pcg_max_iterations);
+        res.pcg_iterations += pc.iterations;
+        if (pc.status != kPcgBreakdown) check(launch_add_rows(host_.R, sol_.ptr, px_.ptr, stream_), "add");
+      }
+      if (host_.R < host_.V)  // fixed vertices keep a zero direction
+        check(cudaMemsetAsync(d_.ptr, 0, nv * sizeof(double), stream_), "memset");
+      check(launch_scatter_direction(dp_, sol_.ptr, d_.ptr, stream_), "scatter");
+      check(launch_slope(dp_, g_.ptr, d_.ptr, partial_.ptr, kReduceGrid, stream_), "slope");
+      slope = reduce_partials(kReduceGrid, 0, kSlope);
+      bool failed = pr.status == kPcgBreakdown || !(slope < 0.0);
+      if (!failed) break;
+      if (mu >= 1e3) {
+        res.status = 3;
+        return res;
+      }
+      mu = raise_mu(mu);
+      res.mu_retries++;
+      t_phase(kAssembly, [&] { return assemble(x_.ptr, inv_h2, mu, 0, true); });
+    }
+    double amax = t_phase(kCcd, [&] { return max_step(x_.ptr, d_.ptr); });
+    int halvings = -1;
+    double alpha = 0.0;
+    t_phase(kLineSearch, [&] {
+      for (int k = 0; k <= opt_.max_halvings; ++k) {
+        double a = amax * std::ldexp(1.0, -k);
+        double delta = energy_change(x_.ptr, d_.ptr, a, inv_h2, 0);
+        if (delta <= opt_.armijo * a * slope) {
+          halvings = k;
+          alpha = a;
+          break;
+        }
+      }
+      return 0;
+    });
+    if (halvings < 0) {
+      res.status = 2;
+      return res;
+    }
+    check(launch_axpy(int(nv), x_.ptr, alpha, d_.ptr, x_.ptr, stream_), "advance");
+    res.updates++;
+    res.halvings += halvings;
+    mu = halvings == 0 ? relax_mu(mu) : mu;
+  }
+}
+
+int Context::solve_equilibrium(const double* start, double h0, drape_run_log* log) {
+  if (start) set_positions(start);
+  const size_t nv = 3 * size_t(host_.V);
+  const double L = gravity_load_;
+  double h = h0 > 0 ? h0 : opt_.h0;
+  const double h_floor = opt_.h0 * opt_.h_min_factor;
+  std::memset(phase_ms_, 0, sizeof phase_ms_);
+  steps_.clear();
+  drape_run_log out{};
+  out.gravity_load = L;
+  auto t_start = std::chrono::steady_clock::now();
+  auto elapsed = [&] { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count(); };
+  int reason = 1;
+  double r = 0.0;
+  for (;;) {
+    r = static_residual();
+    if ((opt_.equilibrium_absolute > 0 && r <= opt_.equilibrium_absolute) ||
+        (opt_.equilibrium_relative > 0 && r / L <= opt_.equilibrium_relative)) {
+      reason = 0;
+      break;
+    }
+    if (!std::isfinite(r)) {
+      reason = 2;
+      break;
+    }
+    if (int(steps_.size()) >= opt_.max_steps) {
+      reason = 1;
+      break;
+    }
+    if (opt_.time_budget_s > 0 && elapsed() > opt_.time_budget_s) {
+      reason = 3;
+      break;
+    }
+    check(cudaMemcpyAsync(xn_.ptr, x_.ptr, nv * sizeof(double), cudaMemcpyDeviceToDevice, stream_), "save");
+    bool accepted = false;
+    AttemptResult res;
+    double h_try = h;
+    int rejected = 0;
+    for (; rejected <= opt_.max_rejections; ++rejected) {
+      h_try = std::max(h * std::pow(opt_.shrink, rejected), h_floor);
+      res = attempt(h_try, r);
+      bool failed = res.non_finite || (res.updates == 0 && (res.status == 2 || res.status == 3));
+      if (!failed && opt_.curvature && res.status == 3 && res.updates > 0) {
+        // mu-cap trigger: solve again without the b' d2d barrier term (drape-e7.ts:113-123).
+        opt_.curvature = 0;
+        AttemptResult again = attempt(h_try, r);
+        opt_.curvature = 1;
+        res = again;
+        failed = res.non_finite || (res.updates == 0 && (res.status == 2 || res.status == 3));
+      }
+      if (!failed) {
+        accepted = true;
+        break;
+      }
+      check(cudaMemcpyAsync(x_.ptr, xn_.ptr, nv * sizeof(double), cudaMemcpyDeviceToDevice, stream_), "restore");
+      out.rejected_attempts++;
+    }
+    if (!accepted) {
+      reason = 2;
+      break;
+    }
+    drape_step_record rec{};
+    rec.step = int(steps_.size()) + 1;
+    rec.h = h_try;
+    rec.residual = r;
+    rec.inner = res.updates;
+    rec.rejected = rejected;
+    rec.pcg_iterations = res.pcg_iterations;
+    check(launch_min_distance(dp_, x_.ptr, partial_.ptr, kReduceGrid, stream_), "min_distance");
+    rec.min_distance = reduce_partials(kReduceGrid, 1, kMinDist);
+    steps_.push_back(rec);
+    out.newton_iterations += res.updates;
+    out.pcg_iterations += res.pcg_iterations;
+    out.mu_retries += res.mu_retries;
+    if (opt_.progress)
+      std::fprintf(stderr, "step %d h %.3e r/L %.3e inner %d rej %d pcg %d %.2f s\n", rec.step, h_try, r / L,
+                   res.updates, rejected, res.pcg_iterations, elapsed());
+    double factor = opt_.controller == 1 ? opt_.growth : (res.updates < opt_.inner_max ? opt_.growth : opt_.shrink);
+    h = std::min(std::max(h_try * factor, h_floor), opt_.h_max);
+  }
+  final_h_ = h;
+  out.ptc_steps = int(steps_.size());
+  out.reason = reason;
+  out.final_residual = r;
+  out.final_relative_residual = r / L;
+  out.final_h = h;
+  out.seconds = elapsed();
+  out.static_energy = static_energy();
+  out.ms_assembly = phase_ms_[kAssembly];
+  out.ms_pcg = phase_ms_[kPcg];
+  out.ms_line_search = phase_ms_[kLineSearch];
+  out.ms_ccd = phase_ms_[kCcd];
+  out.ms_other = out.seconds * 1e3 - out.ms_assembly - out.ms_pcg - out.ms_line_search - out.ms_ccd;
+  if (log) *log = out;
+  return reason;
+}
+
+// ---------------------------------------------------------------- host-buffer entry points
+double Context::assemble_host(const double* x, const double* x_hat, double h, double mu, int mode, int curvature,
+                              double* grad, float* blocks) {
+  const size_t nv = 3 * size_t(host_.V);
+  xt_.upload(x, nv, stream_);
+  if (x_hat) xhat_.upload(x_hat, nv, stream_);
+  int saved = opt_.curvature;
+  opt_.curvature = curvature;
+  double norm = assemble(xt_.ptr, h > 0 ? 1.0 / (h * h) : 0.0, mu, mode, blocks != nullptr);
+  opt_.curvature = saved;
+  if (grad) g_.download(grad, 3 * size_t(host_.R), stream_);
+  if (blocks) {
+    std::vector<float4> h0(host_.B), h1(host_.B);
+    std::vector<float> h2(host_.B);
+    a0_.download(h0.data(), host_.B, stream_);
+    a1_.download(h1.data(), host_.B, stream_);
+    a2_.download(h2.data(), host_.B, stream_);
+    sync();
+    for (int k = 0; k < host_.B; ++k) {
+      float* o = blocks + 9 * size_t(k);
+      o[0] = h0[k].x;
+      o[1] = h0[k].y;
+      o[2] = h0[k].z;
+      o[3] = h0[k].w;
+      o[4] = h1[k].x;
+      o[5] = h1[k].y;
+      o[6] = h1[k].z;
+      o[7] = h1[k].w;
+      o[8] = h2[k];
+    }
+  }
+  sync();
+  return norm;
+}
+
+PcgResult Context::pcg_host(const float* blocks, const double* rhs, double rtol, int max_iterations, double* solution) {
+  const int R = host_.R, B = host_.B;
+  if (blocks) {
+    std::vector<float4> h0(B), h1(B);
+    std::vector<float> h2(B);
+    for (int k = 0; k < B; ++k) {
+      const float* v = blocks + 9 * size_t(k);
+      h0[k] = make_float4(v[0], v[1], v[2], v[3]);
+      h1[k] = make_float4(v[4], v[5], v[6], v[7]);
+      h2[k] = v[8];
+    }
+    a0_.upload(h0.data(), B, stream_);
+    a1_.upload(h1.data(), B, stream_);
+    a2_.upload(h2.data(), B, stream_);
+  }
+  std::vector<float4> b(R);
+  for (int r = 0; r < R; ++r)
+    b[r] = make_float4(float(rhs[3 * r]), float(rhs[3 * r + 1]), float(rhs[3 * r + 2]), 0.0f);
+  b_.upload(b.data(), R, stream_);
+  PcgResult res = pcg(rtol, max_iterations);
+  std::vector<float4> x(R);
+  px_.download(x.data(), R, stream_);
+  sync();
+  for (int r = 0; r < R; ++r) {
+    solution[3 * r] = x[r].x;
+    solution[3 * r + 1] = x[r].y;
+    solution[3 * r + 2] = x[r].z;
+  }
+  return res;
+}
+
+double Context::energy_change_host(const double* x, const double* x_hat, double h, const double* d, double alpha,
+                                   int mode) {
+  const size_t nv = 3 * size_t(host_.V);
+  xt_.upload(x, nv, stream_);
+  if (x_hat) xhat_.upload(x_hat, nv, stream_);
+  d_.upload(d, nv, stream_);
+  return energy_change(xt_.ptr, d_.ptr, alpha, h > 0 ? 1.0 / (h * h) : 0.0, mode);
+}
+
+double Context::max_step_host(const double* x, const double* d) {
+  const size_t nv = 3 * size_t(host_.V);
+  xt_.upload(x, nv, stream_);
+  d_.upload(d, nv, stream_);
+  return max_step(xt_.ptr, d_.ptr);
+}
+
+double Context::static_energy_host(const double* x) {
+  xt_.upload(x, 3 * size_t(host_.V), stream_);
+  check(launch_static_energy(dp_, xt_.ptr, partial_.ptr, kReduceGrid, stream_), "static_energy");
+  return reduce_partials(kReduceGrid, 0, kEnergy);
+}
+
+float Context::time_spmv(int launches, int lanes_per_row, int threads) {
+  DevBsr A{a0_.ptr, a1_.ptr, a2_.ptr};
+  for (int i = 0; i < 3; ++i)
+    check(launch_spmv(host_.R, row_ptr_.ptr, col_idx_.ptr, A, pp0_.ptr, pq_.ptr, lanes_per_row, threads, stream_), "spmv");
+  check(cudaEventRecord(ev_[2], stream_), "event");
+  for (int i = 0; i < launches; ++i)
+    check(launch_spmv(host_.R, row_ptr_.ptr, col_idx_.ptr, A, pp0_.ptr, pq_.ptr, lanes_per_row, threads, stream_), "spmv");
+  check(cudaEventRecord(ev_[3], stream_), "event");
+  sync();
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ev_[2], ev_[3]);
+  return ms / launches;
+}
+
+float Context::time_assembly(int launches) {
+  AssembleArgs a{};
+  a.p = dp_;
+  a.x = x_.ptr;
+  a.x_hat = x_.ptr;
+  a.inv_h2 = 1.0;
+  a.mode = 0;
+  a.grad = g_.ptr;
+  a.bsr = DevBsr{a0_.ptr, a1_.ptr, a2_.ptr};
+  a.partial = partial_.ptr;
+  for (int i = 0; i < 3; ++i) check(launch_assemble(a, stream_), "assemble");
+  check(cudaEventRecord(ev_[2], stream_), "event");
+  for (int i = 0; i < launches; ++i) check(launch_assemble(a, stream_), "assemble");
+  check(cudaEventRecord(ev_[3], stream_), "event");
+  sync();
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ev_[2], ev_[3]);
+  return ms / launches;
+}
+
+}  // namespace drape

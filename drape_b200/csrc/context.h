@@ -1,0 +1,135 @@
+// One drape on one GPU: device buffers, the Newton step operations (assembly, PCG direction, CCD bound, line
+// search) and the pseudo-transient continuation driver. The host makes every decision from a few scalars read
+// back per operation; all vectors stay resident in HBM.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/drape_b200.h"
+#include "kernels.h"
+#include "problem.h"
+
+namespace drape {
+
+struct CudaError : std::runtime_error {
+  cudaError_t code;
+  CudaError(cudaError_t c, const std::string& where)
+      : std::runtime_error(where + ": " + cudaGetErrorString(c)), code(c) {}
+};
+
+template <class T> struct DeviceArray {
+  T* ptr = nullptr;
+  size_t n = 0;
+  DeviceArray() = default;
+  DeviceArray(const DeviceArray&) = delete;
+  DeviceArray& operator=(const DeviceArray&) = delete;
+  ~DeviceArray() { release(); }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count);
+  void upload(const T* host, size_t count, cudaStream_t s);
+  void download(T* host, size_t count, cudaStream_t s) const;
+};
+
+struct PcgResult {
+  int iterations = 0, status = 0, replacements = 0;
+  double relative = 0.0;  // recursive sqrt(rr / rr0)
+  float ms = 0.0f;
+};
+
+struct AttemptResult {
+  int updates = 0, pcg_iterations = 0, mu_retries = 0, halvings = 0;
+  int status = 0;  // 0 converged, 1 iteration limit, 2 line search failed, 3 regularisation cap
+  bool non_finite = false;
+  double max_mu = 0.0;
+};
+
+class Context {
+ public:
+  Context(const HostProblem& problem, const drape_options& options, int device);
+  ~Context();
+
+  const HostProblem& problem() const { return host_; }
+  const drape_options& options() const { return opt_; }
+  drape_options& options() { return opt_; }
+
+  // ---- state
+  void set_positions(const double* xyz);           // host -> current state x
+  void get_positions(double* xyz) const;           // current state -> host
+  double final_h() const { return final_h_; }
+
+  // ---- kernel-level operations on host buffers (parity entry points)
+  // g = grad Phi at x with x_hat and step h (mode 0) or grad E_s (mode 1); optional f32 blocks (9B row-major).
+  double assemble_host(const double* x, const double* x_hat, double h, double mu, int mode, int curvature,
+                       double* grad, float* blocks);
+  PcgResult pcg_host(const float* blocks, const double* rhs, double rtol, int max_iterations, double* solution);
+  double energy_change_host(const double* x, const double* x_hat, double h, const double* d, double alpha, int mode);
+  double max_step_host(const double* x, const double* d);
+  double static_energy_host(const double* x);
+
+  // ---- device-resident operations
+  double gravity_load() const { return gravity_load_; }
+  double static_residual();                        // |grad E_s(x)| at the current state
+  double static_energy();                          // E_s(x) at the current state
+  int solve_equilibrium(const double* start, double h0, drape_run_log* log);
+  const std::vector<drape_step_record>& steps() const { return steps_; }
+
+  // Stand-alone timed SpMV of the assembled matrix (roofline measurement): average ms per launch.
+  float time_spmv(int launches, int lanes_per_row, int threads);
+  // Stand-alone timed assembly at the current state (ms per launch).
+  float time_assembly(int launches);
+
+  std::string last_error;
+
+ private:
+  void upload_problem();
+  void sync();
+  double read_scalar(int slot);
+  double assemble(const double* x, double inv_h2, double mu, int mode, bool hessian);
+  double reduce_partials(int n, int op, int slot);
+  PcgResult pcg(double rtol, int max_iterations);
+  double direction_slope();
+  double max_step(const double* x, const double* d);
+  double energy_change(const double* x, const double* d, double alpha, double inv_h2, int mode);
+  AttemptResult attempt(double h, double scale);
+  void record_phase(int phase, cudaEvent_t a, cudaEvent_t b);
+
+  HostProblem host_;
+  drape_options opt_;
+  int device_ = 0;
+  cudaStream_t stream_ = nullptr;
+  DevProblem dp_{};
+  double gravity_load_ = 0.0, final_h_ = 0.0;
+  PcgLaunch pcg_cfg_;
+
+  // static problem arrays
+  DeviceArray<double> geom_, hinge_k_, unit_mass_, colliders_;
+  DeviceArray<int> tri_, hinge_, row_vertex_, row_ptr_, col_idx_, diag_slot_, diag_pos_;
+  DeviceArray<int> rt_ptr_, rt_ent_, rt_pos_, rh_ptr_, rh_ent_, rh_pos_;
+  // state and work (vertex layout f64)
+  DeviceArray<double> x_, xn_, xhat_, xt_, d_, towards_;
+  DeviceArray<double> g_, partial_, scalars_;
+  // BSR f32 planes and PCG vectors (float4 rows)
+  DeviceArray<float4> a0_, a1_;
+  DeviceArray<float> a2_;
+  DeviceArray<float4> b_, px_, pr_, pz_, pp0_, pp1_, pq_, dinv_, sol_, corr_;
+  DeviceArray<float> pcg_partial_;
+  DeviceArray<PcgState> pcg_state_;
+  double* pinned_ = nullptr;
+  PcgState* pinned_state_ = nullptr;
+  cudaEvent_t ev_[8] = {};
+  std::vector<drape_step_record> steps_;
+  double phase_ms_[6] = {};
+  int partial_grid_ = 0;
+};
+
+void check(cudaError_t e, const char* where);
+
+}  // namespace drape

@@ -1,0 +1,107 @@
+// Kernel argument blocks and launchers of the drape GPU stage (elem.cu, pcg.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "device_problem.h"
+
+namespace drape {
+
+// Incident elements (triangles + hinges) one warp evaluates per BSR row; the context rejects meshes above it.
+constexpr int kMaxRowEntries = 32;
+// Blocks per BSR row one warp writes (one lane per block).
+constexpr int kMaxRowBlocks = 32;
+
+struct AssembleArgs {
+  DevProblem p;
+  const double* x;
+  const double* x_hat;
+  double inv_h2;    // 1/h^2 (mode 0)
+  double mu;        // the diagonal carries (1 + mu) m/h^2 (mode 0)
+  int mode;         // 0: grad Phi = m/h^2 (x - x_hat) + grad Pi;  1: grad E_s = grad Pi - m g (no inertia block)
+  int curvature;    // 1 keeps the barrier's b' (I - n n^T)/|x - c| term (negative semidefinite: off by default)
+  double* grad;     // f64 [3R]
+  DevBsr bsr;       // f32 blocks; a0 == nullptr computes the gradient only
+  double* partial;  // f64 [assemble_grid(R)]: per-CTA sum of |grad_row|^2 (may be null)
+};
+
+struct EnergyArgs {
+  DevProblem p;
+  const double* x;
+  const double* x_hat;
+  const double* d;
+  double alpha, inv_h2;
+  int mode;         // 0: Phi (inertia term), 1: E_s (gravity potential)
+  double* partial;  // f64 [grid]
+};
+
+int assemble_grid(int R);
+cudaError_t launch_assemble(const AssembleArgs& a, cudaStream_t s);
+cudaError_t launch_energy_change(const EnergyArgs& a, int grid, cudaStream_t s);
+cudaError_t launch_max_step(const DevProblem& p, const double* x, const double* d, double* partial, int grid,
+                            cudaStream_t s);
+cudaError_t launch_slope(const DevProblem& p, const double* g, const double* d, double* partial, int grid,
+                         cudaStream_t s);
+cudaError_t launch_inf_norm(const DevProblem& p, const double* d, double* partial, int grid, cudaStream_t s);
+// out[slot] = sum (op 0) or min (op 1) of n partials.
+cudaError_t launch_reduce(const double* partial, int n, int op, double* out, int slot, cudaStream_t s);
+cudaError_t launch_predict(const DevProblem& p, const double* x, double h2, double* x_hat, cudaStream_t s);
+cudaError_t launch_axpy(int n, const double* x, double alpha, const double* d, double* out, cudaStream_t s);
+cudaError_t launch_sub(int n, const double* a, const double* b, double* out, cudaStream_t s);
+cudaError_t launch_scatter_direction(const DevProblem& p, const float4* sol, double* d, cudaStream_t s);
+cudaError_t launch_rhs(int R, const double* g, float4* b, cudaStream_t s);
+
+// ---------------------------------------------------------------- PCG
+enum PcgStatus { kPcgRunning = 0, kPcgConverged = 1, kPcgIterationLimit = 2, kPcgBreakdown = 3, kPcgTimeout = 4 };
+
+// Device-resident solver state (the reference's 16-word State, state.wgsl:4-9, plus the grid barrier).
+struct PcgState {
+  float rz, rr, rr0, pq, alpha, beta;
+  int iterations, status;
+  unsigned barrier_count, barrier_gen;
+  int error;  // a grid barrier gave up waiting (the kernel returned early)
+  int replacements;
+};
+
+struct PcgArgs {
+  int R;
+  const int* row_ptr;
+  const int* col_idx;
+  const int* diag_pos;  // absolute block index of each row's diagonal
+  DevBsr A;
+  const float4* b;
+  float4* x;
+  float4* r;
+  float4* z;
+  float4* p0;
+  float4* p1;
+  float4* q;
+  float4* dinv;         // 3 float4 per row: rows of the inverted diagonal block
+  float* partial;       // [3 * grid]
+  PcgState* state;
+  float tol2;           // tolerance^2 on rr / rr0
+  int max_iterations;
+  int replace_every;    // residual replacement period (0 = never)
+  float replace_above2; // only while rr > replace_above^2 rr0
+  long long spin_limit; // clock cycles a grid barrier waits before giving up
+};
+
+struct PcgLaunch {
+  int grid = 0, threads = 256, lanes_per_row = 8;
+};
+
+// Cooperative launch of the whole PCG solve; `cfg.grid` <= co-resident CTAs (see pcg_max_grid).
+cudaError_t launch_pcg(const PcgArgs& a, const PcgLaunch& cfg, cudaStream_t s);
+int pcg_max_grid(int threads, int lanes_per_row);
+
+// y = A p (f32 BSR times float4-per-row vector): the stand-alone SpMV of the roofline measurement.
+cudaError_t launch_spmv(int R, const int* row_ptr, const int* col_idx, DevBsr A, const float4* p, float4* y,
+                        int lanes_per_row, int threads, cudaStream_t s);
+
+// r = b64 - A d in f64 (A the f32 blocks, d float4 rows), written as the f32 right-hand side of a refinement
+// solve; partial gets per-CTA |r|^2 (f64).
+cudaError_t launch_refine_residual(int R, const int* row_ptr, const int* col_idx, DevBsr A, const double* b64_neg_g,
+                                   const float4* d, float4* r_out, double* partial, int grid, cudaStream_t s);
+// d += e (float4 rows).
+cudaError_t launch_add_rows(int R, float4* d, const float4* e, cudaStream_t s);
+
+}  // namespace drape

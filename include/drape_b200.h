@@ -1,0 +1,174 @@
+/* drape_b200: the GPU stage of the quasi-static drape solve (pseudo-transient continuation, regularised inexact
+ * Newton, block-Jacobi PCG, IPC contact with a CCD-bounded Armijo line search) on one NVIDIA B200.
+ *
+ * C ABI: plain pointers and sizes, status codes, no exceptions across the boundary. A context is used from one
+ * host thread; its work is ordered on one CUDA stream. Host arrays passed in are copied; the caller keeps them.
+ *
+ * The reference runs this stage as a process (engine/gpu/src/node/run-e7.ts:116-138) over problem.json /
+ * problem.bin written by `oracle e7-generate` (engine/oracle/src/e7_run.rs:41-50), and in-process through the
+ * TypeScript functions cited beside each entry point below.
+ */
+#ifndef DRAPE_B200_H
+#define DRAPE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct drape_ctx drape_ctx;
+
+typedef enum {
+  DRAPE_OK = 0,
+  DRAPE_E_ARG = 1,      /* invalid argument or inconsistent problem arrays */
+  DRAPE_E_CUDA = 2,     /* a CUDA call failed (message in drape_last_error) */
+  DRAPE_E_DIVERGED = 3, /* the solve stalled (no PTC step could be taken) or produced a non-finite state */
+  DRAPE_E_TIMEOUT = 4,  /* a device-side wait gave up (bounded grid barrier) or the time budget ran out */
+  DRAPE_E_IO = 5,       /* problem or state file could not be read or written */
+  DRAPE_E_STATE = 6     /* called in the wrong state (e.g. no context) */
+} drape_status;
+
+/* One drape, borrowed arrays in the problem.bin layout (e3_generate.rs:84-104, e5_checks.rs:80-86):
+ *   start_xyz       [3V]  cold-start vertex positions (rest_positions)
+ *   elem_vertices   [3T]  triangle vertex ids                       elem_geom [7T] dN_k/dX (k=0..2) and rest area
+ *   hinge_vertices  [4H]  [left opposite, right opposite, edge a, edge b]   hinge_stiffness [H]
+ *   row_vertex      [R]   vertex of each unknown row                row_unit_mass [R] lumped masses (kg)
+ *   row_ptr [R+1], col_idx [B]  BSR(3x3) pattern over rows (sorted columns, diagonal present)
+ *   collider_data   [8 * colliders]  kind (1 plane n.x = w, 2 sphere |x - c| = w), a, b, c, w, 0, 0, 0 */
+typedef struct {
+  int32_t columns, vertices, triangles, hinges, rows, blocks;
+  const double* start_xyz;
+  const uint32_t* elem_vertices;
+  const double* elem_geom;
+  const uint32_t* hinge_vertices;
+  const double* hinge_stiffness;
+  const uint32_t* row_vertex;
+  const double* row_unit_mass;
+  const uint32_t* row_ptr;
+  const uint32_t* col_idx;
+  double wale, course, coupling, shear; /* membrane law, N/m (material.rs:28-45) */
+  double gravity[3];                    /* m/s^2 */
+  int32_t colliders;
+  const double* collider_data;
+  double dhat, kappa; /* IPC barrier activation distance (m) and stiffness */
+} drape_problem_view;
+
+/* Solver rules (the problem.json "ptc", "newton", "pcg", "robust" blocks: e7_run.rs:28-33, e3_generate.rs:199-226). */
+typedef struct {
+  int32_t controller;          /* 0: x2 below the inner cap, x0.5 at it (e7_ptc.rs:30-35); 1: x2 after every step */
+  double h0, h_max, h_min_factor, growth, shrink;
+  double inner_tolerance;      /* inner Newton stop: |g| / |g(x_n)| <= this */
+  int32_t inner_max, max_rejections, max_steps;
+  double equilibrium_relative; /* stop at |grad E_s| / |m g| <= this (0: off) */
+  double equilibrium_absolute; /* stop at |grad E_s| <= this, N (0: off) */
+  double pcg_rtol;             /* PCG relative tolerance (forcing 0) */
+  int32_t pcg_max_iterations;
+  int32_t forcing;             /* 0: fixed pcg_rtol; 1: Eisenstat-Walker (e4_rules.rs:15-22) */
+  int32_t replace_every;       /* PCG residual replacement period (0: never) */
+  double replace_above;
+  int32_t refine;              /* 1: one f64 residual refinement of every Newton direction */
+  double refine_rtol;          /* relative tolerance of the refinement solve */
+  int32_t curvature;           /* 1: keep the barrier's b'(I - nn^T)/|x - c| Hessian term (not SPD) */
+  int32_t preconditioner;      /* 0: block Jacobi */
+  double armijo;
+  int32_t max_halvings;
+  double time_budget_s;        /* 0: none */
+  int32_t pcg_grid, pcg_threads, pcg_lanes; /* 0: automatic */
+  int32_t progress;            /* 1: one stderr line per accepted PTC step */
+} drape_options;
+
+/* Outcome of drape_solve_equilibrium (gpu-result.json fields, run-e7.ts:100-106). */
+typedef struct {
+  int32_t ptc_steps, newton_iterations, pcg_iterations, rejected_attempts, mu_retries;
+  int32_t reason; /* 0 tolerance, 1 step cap, 2 stalled, 3 time budget */
+  double final_residual, final_relative_residual, final_h, gravity_load, static_energy, seconds;
+  double ms_assembly, ms_pcg, ms_line_search, ms_ccd, ms_other;
+} drape_run_log;
+
+/* One accepted PTC step (gpu-ptc.bin columns, run-e7.ts:96). */
+typedef struct {
+  int32_t step, inner, rejected, pcg_iterations;
+  double h, residual, min_distance;
+} drape_step_record;
+
+/* Library version string. */
+const char* drape_version(void);
+
+/* Fills the sheet-over-sphere rules: doubling controller from h0 = 1e-3 s, |grad E_s| <= 1e-6 N, PCG rtol 1e-6,
+ * at most 2000 PCG iterations, inner Newton tol 0.1 and 10 updates (replaces parsePtcRules/parseRobustRules,
+ * ptc.ts:28-32, robust-newton.ts:208-214). */
+void drape_default_options(drape_options* out);
+
+/* Creates a context on `device` from borrowed arrays (replaces prepareDrapeGpu, drape-gpu.ts:141-162). */
+drape_status drape_create(const drape_problem_view* problem, const drape_options* options, int32_t device,
+                          drape_ctx** out);
+/* Builds the problem from a problem.json / problem.bin directory (replaces load + parseDrapeProblem,
+ * run-e7.ts:51-57, drape.ts:44-63). */
+drape_status drape_create_from_files(const char* dir, const drape_options* options, int32_t device, drape_ctx** out);
+/* Builds the 1 m sheet over a sphere (optional ground plane at y = -0.25) with the product's scene builder. */
+drape_status drape_create_sheet(int32_t columns, uint64_t seed, double radius, double young, int32_t plane,
+                                const drape_options* options, int32_t device, drape_ctx** out);
+/* Builds the reference's 0.5 m knit sphere-on-floor scene, edit "base" | "w1" | "w2" | "w3" (e7_run.rs:18-26). */
+drape_status drape_create_reference(int32_t columns, const char* edit, const drape_options* options, int32_t device,
+                                    drape_ctx** out);
+void drape_destroy(drape_ctx* ctx);
+
+/* Host-only (no GPU needed): write the problem.json / problem.bin pair of the product's scene builders (replaces
+ * `oracle e7-generate`, e7_run.rs:41-50, for the GPU stage's inputs), and read + validate a pair, returning
+ * [V, T, H, R, B, colliders]. */
+drape_status drape_write_sheet_problem(int32_t columns, uint64_t seed, double radius, double young, int32_t plane,
+                                       const char* dir);
+drape_status drape_write_reference_problem(int32_t columns, const char* edit, const char* dir);
+drape_status drape_inspect_problem(const char* dir, int64_t* sizes6);
+
+/* Last error message of a context, or of the last failed create when ctx is NULL. */
+const char* drape_last_error(const drape_ctx* ctx);
+
+/* [V, T, H, R, B, colliders] */
+drape_status drape_sizes(const drape_ctx* ctx, int64_t* out6);
+drape_status drape_set_options(drape_ctx* ctx, const drape_options* options);
+
+/* Current state (f64 master positions, 3V) and the step size the last solve ended with (e7_state.rs:9-40). */
+drape_status drape_set_state(drape_ctx* ctx, const double* xyz);
+drape_status drape_get_state(const drape_ctx* ctx, double* xyz, double* final_h);
+
+/* PTC to equilibrium from `start_xyz` (NULL: the current state) with first step `h0` (<= 0: options.h0)
+ * (replaces solveEquilibrium, drape-e7.ts:156-180; oracle ptc_solve, e7_ptc.rs:170-189). */
+drape_status drape_solve_equilibrium(drape_ctx* ctx, const double* start_xyz, double h0, drape_run_log* log);
+/* Copies up to `capacity` accepted-step records of the last solve; returns their total count in *count. */
+drape_status drape_step_records(const drape_ctx* ctx, drape_step_record* out, int32_t capacity, int32_t* count);
+
+/* Kernel-level entry points on host buffers (the parity checks of run-e7.ts:140-145 --checks):
+ * g = grad Phi(x) with x_hat and step h (mode 0; Phi = (1/2h^2)(x - x_hat)^T M (x - x_hat) + Pi) or
+ * grad E_s (mode 1), 3R f64; blocks = K + mu M/h^2 (mode 0) as 9B f32 row-major blocks, NULL to skip
+ * (replaces evaluateKernelsWithInertia, drape-e4.ts; oracle DrapeStep::residual/tangent, drape.rs:304-322). */
+drape_status drape_assemble(drape_ctx* ctx, const double* x, const double* x_hat, double h, double mu, int32_t mode,
+                            int32_t curvature, double* grad, float* blocks);
+/* Block-Jacobi PCG from 0 on the given f32 blocks (NULL: the last assembled matrix) and f64 rhs (3R, rounded to
+ * f32); info = [iterations, status (1 converged, 2 iteration limit, 3 breakdown, 4 timeout), replacements],
+ * relative = recursive sqrt(rr/rr0) (replaces solveOnce, solver.ts:179-191; oracle pcg::solve, pcg.rs:271-291). */
+drape_status drape_pcg(drape_ctx* ctx, const float* blocks, const double* rhs, double rtol, int32_t max_iterations,
+                       double* solution, int32_t* info, double* relative);
+/* Phi(x + alpha d) - Phi(x) (mode 0) or E_s(x + alpha d) - E_s(x) (mode 1), f64 sum of per-element changes
+ * (replaces gpuEnergy, newton-ops.ts:360-365; oracle DrapeStep::energy_change, drape.rs:325-335). */
+drape_status drape_energy_change(drape_ctx* ctx, const double* x, const double* x_hat, double h, const double* d,
+                                 double alpha, int32_t mode, double* out);
+/* Largest alpha <= 1 keeping every vertex at >= 0.1 of its collider distances (replaces maxStepOnGpu,
+ * contact-host.ts:36-41; oracle DrapeStep::max_step, drape.rs:344-346). */
+drape_status drape_max_step(drape_ctx* ctx, const double* x, const double* d, double* out);
+/* |grad E_s| and E_s at x (NULL: the current state), f64 (oracle static_gradient / static_energy,
+ * e7_ptc.rs:43-51). */
+drape_status drape_static_residual(drape_ctx* ctx, const double* x, double* out);
+drape_status drape_static_energy(drape_ctx* ctx, const double* x, double* out);
+
+/* Timed stand-alone launches for the roofline: average device ms per launch of the BSR SpMV on the last
+ * assembled matrix (lanes per row 4/8/16/32) and of the row assembly at the current state. */
+drape_status drape_time_spmv(drape_ctx* ctx, int32_t launches, int32_t lanes_per_row, int32_t threads, float* ms);
+drape_status drape_time_assembly(drape_ctx* ctx, int32_t launches, float* ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DRAPE_B200_H */

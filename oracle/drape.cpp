@@ -521,15 +521,23 @@ PtcRun ptc_solve(const Drape& d, std::vector<Vec3> start, double h_start, const 
 }
 
 // ---------------------------------------------------------------- kernel-check states
+// e3_checks.rs:40-44's fold plus noise, applied on top of the scene's start state with the fold along the up
+// axis (-gravity): the reference evaluated it on the contact-free pinned sheet lying at z = 0; placing it over the
+// start state keeps every vertex of a contact scene outside its colliders (the barrier is checked separately at
+// contact_state). The noise draws keep the reference's order (x, y, z per vertex).
 std::vector<Vec3> bent_state(const Drape& d, Lcg& rng) {
   double w = d.mesh.width, h = d.mesh.height, s = d.mesh.width / (d.mesh.columns - 1);
+  double gn = d.g_norm();
+  Vec3 up{-d.gravity[0] / gn, -d.gravity[1] / gn, -d.gravity[2] / gn};
   std::vector<Vec3> x;
-  for (auto& p : d.mesh.rest) {
-    double a = p[0] + 0.1 * s * rng.uniform();
-    double b = p[1] + 0.1 * s * rng.uniform();
+  for (size_t v = 0; v < d.mesh.rest.size(); ++v) {
+    auto& p = d.mesh.rest[v];
+    double a = 0.1 * s * rng.uniform();
+    double b = 0.1 * s * rng.uniform();
     double fold = 0.05 * std::sin(M_PI * p[0] / w) * std::cos(2.0 * M_PI * p[1] / h);
-    double c = fold + 0.1 * s * rng.uniform();
-    x.push_back({a, b, c});
+    double c = 0.1 * s * rng.uniform();
+    Vec3 base = d.start[v];
+    x.push_back({base[0] + a + fold * up[0], base[1] + b + fold * up[1], base[2] + c + fold * up[2]});
   }
   return x;
 }

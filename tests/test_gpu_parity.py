@@ -1,0 +1,149 @@
+"""CUDA path against the f64 oracle, through the C ABI (needs a B200).
+
+Tolerances: gradients are f64 on both sides (relative L2 <= 1e-10); the f32 BSR blocks carry one f32 rounding
+of an f64 sum (relative L2 <= 1e-6 per matrix); line-search energy changes and the CCD bound are f64 (relative
+<= 1e-9). Full solves are compared on the converged state: max vertex error <= 1e-4 m (the sheet scene's
+acceptance bound) and relative static-energy error <= 1e-6.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from drape_b200 import api
+from tests import oracle_py
+
+pytestmark = pytest.mark.gpu
+GOLDEN = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_values.json")))
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def scenes(n=17):
+    return [
+        ("sheet", oracle_py.Scene("sheet", n, seed=1, radius=0.25, young=5e5, plane=True, projected=True),
+         lambda o: api.Drape.sheet(n, seed=1, radius=0.25, young=5e5, plane=True, options=o)),
+        ("reference", oracle_py.Scene("reference", n, edit="base", projected=True),
+         lambda o: api.Drape.reference(n, "base", options=o)),
+    ]
+
+
+@pytest.mark.parametrize("which", [0, 1])
+@pytest.mark.parametrize("state", ["kernel", "contact"])
+def test_assembly_matches_the_oracle(which, state):
+    name, oracle, make = scenes()[which]
+    gpu = make(api.default_options())
+    x = oracle.kernel_state() if state == "kernel" else oracle.contact_state()
+    rng = np.random.default_rng(7)
+    x_hat = x + 1e-4 * rng.standard_normal(x.shape)
+    for mu, h in [(0.0, 1.0 / 240.0), (0.37, 0.1)]:
+        g_o, k_o = oracle.assemble(x, x_hat, h, mu=mu, curvature=False)
+        g_g, k_g = gpu.assemble(x, x_hat, h, mu=mu, mode=0)
+        assert rel(g_g, g_o) <= 1e-10, (name, state, mu)
+        assert rel(k_g, k_o) <= 1e-6, (name, state, mu)
+    # Static gradient (mode 1) against the oracle's grad E_s.
+    g1, _ = gpu.assemble(x, mode=1, blocks=False)
+    assert rel(g1, oracle.static_gradient(x)) <= 1e-10
+
+
+@pytest.mark.parametrize("which", [0, 1])
+def test_energy_change_max_step_and_energy_match_the_oracle(which):
+    name, oracle, make = scenes()[which]
+    gpu = make(api.default_options())
+    x = oracle.contact_state()
+    rng = np.random.default_rng(3)
+    d = 1e-4 * rng.standard_normal(x.shape)
+    x_hat = x + 1e-4 * rng.standard_normal(x.shape)
+    for alpha in [1.0, 0.25, 1e-3]:
+        e_o = oracle.energy_change(x, x_hat, 0.05, d, alpha)
+        e_g = gpu.energy_change(x, d, alpha, x_hat=x_hat, h=0.05, mode=0)
+        assert abs(e_g - e_o) <= 1e-9 * abs(e_o) + 1e-18, (name, alpha, e_g, e_o)
+    a_o, a_g = oracle.max_step(x, d), gpu.max_step(x, d)
+    assert abs(a_g - a_o) <= 1e-12 * a_o, (a_g, a_o)
+    assert a_o < 1.0
+    e_o, e_g = oracle.static_energy(x), gpu.static_energy(x)
+    assert abs(e_g - e_o) <= 1e-12 * abs(e_o)
+
+
+@pytest.mark.parametrize("case", ["tension-n33", "dynamic-n33", "tension-n65", "dynamic-n65"])
+def test_pcg_on_the_reference_linear_cases(case):
+    """The E1 systems (experiments/cases/*): the persistent PCG converges to rtol 1e-7 with residual replacement
+    every 50 iterations, within 10% of the reference's stored f32 iteration count, and its solution agrees with
+    the f64 solution to the f32 storage error of the system."""
+    kind, n = case.split("-n")
+    rp, ci, vals, rhs = oracle_py.linear_case(kind, int(n))
+    R = len(rp) - 1
+    opts = api.default_options(replace_every=50, replace_above=1e-2)
+    gpu = api.Drape.from_arrays(np.zeros(3 * R), np.arange(R), np.ones(R), rp, ci, options=opts)
+    sol, info = gpu.pcg(rhs, 1e-7, 20000, blocks=vals.astype(np.float32))
+    ref = GOLDEN["e1"][case]["pcg_f32_cpu"]["iterations"]
+    assert info["status"] == "converged"
+    assert abs(info["iterations"] - ref) <= 0.1 * ref, (info, ref)
+    x64, _ = oracle_py.pcg(rp, ci, vals, rhs, 1e-12, 20000)
+    assert rel(sol, x64) <= 1e-3, rel(sol, x64)
+
+
+def test_pcg_reports_breakdown_on_an_indefinite_matrix():
+    rp, ci, vals, rhs = oracle_py.linear_case("tension", 9)
+    R = len(rp) - 1
+    gpu = api.Drape.from_arrays(np.zeros(3 * R), np.arange(R), np.ones(R), rp, ci)
+    _, info = gpu.pcg(rhs, 1e-7, 500, blocks=(-vals).astype(np.float32) + np.float32(0))
+    # -A is negative definite: p.q < 0 at the first iteration.
+    assert info["status"] == "breakdown"
+    sol, info = gpu.pcg(rhs, 1e-7, 3, blocks=vals.astype(np.float32))
+    assert info["status"] == "iteration_limit" and info["iterations"] == 3
+
+
+def test_solve_is_deterministic():
+    o = api.default_options(max_steps=4)
+    a = api.Drape.sheet(17, options=o)
+    b = api.Drape.sheet(17, options=o)
+    la, lb = a.solve_equilibrium(check=False), b.solve_equilibrium(check=False)
+    assert np.array_equal(a.state, b.state)
+    assert la["pcg_iterations"] == lb["pcg_iterations"]
+
+
+@pytest.mark.parametrize("n", [17, 33])
+def test_sheet_solve_reaches_the_oracle_equilibrium(n):
+    """Sheet over sphere + plane, doubling PTC from 1e-3 s to |grad E_s| <= 1e-6 N on both sides."""
+    o = api.default_options()
+    gpu = api.Drape.sheet(n, seed=0, plane=True, options=o)
+    log = gpu.solve_equilibrium()
+    assert log["reason"] == "tolerance" and log["final_residual"] <= 1e-6, log
+    oracle = oracle_py.Scene("sheet", n, seed=0, plane=True)
+    x_o, st = oracle.ptc(h0=1e-3, doubling=True, absolute=1e-6, pcg=True, rtol=1e-6, maxit=2000)
+    assert st["converged"] == 1.0
+    x_g = gpu.state
+    err = np.abs(x_g - x_o).reshape(-1, 3).max()
+    assert err <= 1e-4, err
+    e_o, e_g = oracle.static_energy(x_o), gpu.static_energy()
+    assert abs(e_g - e_o) <= 1e-6 * abs(e_o), (e_g, e_o)
+    # The GPU's final state satisfies the oracle's f64 residual test too.
+    assert np.linalg.norm(oracle.static_gradient(x_g)) <= 1.01e-6
+
+
+def test_reference_scene_reaches_the_stored_equilibrium():
+    """The reference's n17 base scene (knit sheet on a sphere on a floor) solved by the GPU stage reaches the
+    reference oracle's stored converged static energy (experiments/drape7/drape-n17/base/reference-cold.json)."""
+    gold = GOLDEN["drape7"]["drape-n17/base"]["references"]["cold"]
+    o = api.default_options(controller=0, h0=1.0 / 240.0, equilibrium_absolute=0.0, equilibrium_relative=1e-7)
+    gpu = api.Drape.reference(17, "base", options=o)
+    log = gpu.solve_equilibrium()
+    assert log["reason"] == "tolerance", log
+    e = gpu.static_energy()
+    assert abs(e - gold["static_energy"]) <= 1e-7 * gold["static_energy"], (e, gold["static_energy"])
+
+
+def test_problem_files_round_trip_through_the_gpu_stage(tmp_path):
+    d = str(tmp_path / "p")
+    api.write_sheet_problem(d, 17, seed=2, plane=True)
+    a = api.Drape.from_files(d)
+    b = api.Drape.sheet(17, seed=2, plane=True)
+    x = b.state
+    assert np.array_equal(a.state, x)
+    ga, _ = a.assemble(x, mode=1, blocks=False)
+    gb, _ = b.assemble(x, mode=1, blocks=False)
+    assert np.array_equal(ga, gb)

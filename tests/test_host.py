@@ -1,0 +1,119 @@
+"""Host-side checks of libdrape_b200.so that need no GPU: the C ABI exports, the product's scene builders
+against the oracle's scenes, and the problem-file reader on files in the reference's format."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from drape_b200 import api
+from tests import oracle_py
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from drape_b200 import build
+
+    build.build()
+    return api.load()
+
+
+def declared_functions():
+    text = open(os.path.join(ROOT, "include", "drape_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(drape_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_every_declared_symbol_is_exported(lib):
+    out = subprocess.run(["nm", "-D", "--defined-only", api.LIB_PATH], capture_output=True, text=True, check=True).stdout
+    exported = set(re.findall(r" T (drape_[a-z0-9_]+)$", out, flags=re.M))
+    names = declared_functions()
+    assert len(names) >= 20
+    missing = [n for n in names if n not in exported]
+    assert not missing, missing
+    for n in names:
+        assert hasattr(lib, n)
+
+
+def test_options_struct_matches_the_header(lib):
+    o = api.default_options()
+    assert o.controller == 1 and o.h0 == 1e-3 and o.equilibrium_absolute == 1e-6
+    assert o.pcg_rtol == 1e-6 and o.pcg_max_iterations == 2000 and o.inner_max == 10 and o.max_halvings == 30
+
+
+def _oracle_topology(scene):
+    tris = np.zeros(3 * scene.T, np.int32)
+    hinges = np.zeros(4 * scene.H, np.int32)
+    k = np.zeros(scene.H)
+    scene.lib.oracle_scene_topology(oracle_py.P(scene.h), oracle_py.ptr(tris), oracle_py.ptr(hinges), oracle_py.ptr(k))
+    return tris, hinges, k
+
+
+def _compare(tmp_path, arrays, meta, scene):
+    tris, hinges, k = _oracle_topology(scene)
+    assert np.array_equal(arrays["elem_vertices"].astype(np.int32), tris)
+    assert np.array_equal(arrays["hinge_vertices"].astype(np.int32), hinges)
+    assert np.allclose(arrays["hinge_stiffness_f64"], k, rtol=1e-14, atol=0)
+    rp, ci = scene.pattern()
+    assert np.array_equal(arrays["row_ptr"].astype(np.int32), rp)
+    assert np.array_equal(arrays["col_idx"].astype(np.int32), ci)
+    assert np.allclose(arrays["row_unit_mass_f64"], scene.mass(), rtol=1e-14, atol=0)
+    assert np.array_equal(arrays["rest_positions_f64"], scene.start())
+    assert meta["contact"]["dhat_m"] == scene.dhat
+    assert abs(meta["contact"]["kappa"] - scene.kappa) <= 1e-15 * scene.kappa
+    assert np.allclose(meta["gravity_vector"], scene.gravity)
+
+
+@pytest.mark.parametrize("n,seed,plane", [(9, 0, False), (17, 3, True), (33, 0, True)])
+def test_sheet_builder_matches_the_oracle(lib, tmp_path, n, seed, plane):
+    d = str(tmp_path / "sheet")
+    api.write_sheet_problem(d, n, seed=seed, radius=0.2, young=8e5, plane=plane)
+    meta, arrays = api.read_problem_arrays(d)
+    scene = oracle_py.Scene("sheet", n, seed=seed, radius=0.2, young=8e5, plane=plane)
+    _compare(tmp_path, arrays, meta, scene)
+    assert api.inspect_problem(d) == (scene.V, scene.T, scene.H, scene.R, scene.B, scene.colliders)
+
+
+@pytest.mark.parametrize("edit", ["base", "w1", "w2", "w3"])
+def test_reference_builder_matches_the_oracle(lib, tmp_path, edit):
+    d = str(tmp_path / edit)
+    api.write_reference_problem(d, 17, edit)
+    meta, arrays = api.read_problem_arrays(d)
+    _compare(tmp_path, arrays, meta, oracle_py.Scene("reference", 17, edit=edit))
+
+
+def test_reads_problem_files_in_the_reference_format(lib, tmp_path):
+    """`oracle e7-generate` writes the reference's problem.json / problem.bin layout (e3_generate.rs:84-229); the
+    GPU stage's reader accepts it."""
+    oracle_py.build()
+    d = str(tmp_path / "n17")
+    subprocess.run([oracle_py.CLI, "e7-generate", "--n", "17", "--edit", "base", "--out", d], check=True)
+    s = oracle_py.Scene("reference", 17, edit="base")
+    assert api.inspect_problem(d) == (s.V, s.T, s.H, s.R, s.B, 2)
+
+
+def test_problem_reader_rejects_bad_input(lib, tmp_path):
+    with pytest.raises(api.DrapeError) as e:
+        api.inspect_problem(str(tmp_path / "missing"))
+    assert e.value.status == 5
+    d = str(tmp_path / "trunc")
+    api.write_sheet_problem(d, 9)
+    raw = open(os.path.join(d, "problem.bin"), "rb").read()
+    open(os.path.join(d, "problem.bin"), "wb").write(raw[: len(raw) // 2])
+    with pytest.raises(api.DrapeError):
+        api.inspect_problem(d)
+    with pytest.raises(api.DrapeError) as e:
+        api.write_sheet_problem(str(tmp_path / "x"), 2)
+    assert e.value.status == 1
+
+
+def test_creating_a_context_without_a_device_fails_loudly(lib):
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(api.DrapeError):
+        api.Drape.sheet(9)
