@@ -60,7 +60,8 @@ const char* drape_version(void) { return "drape_b200 0.1 (sm_100a)"; }
 void drape_default_options(drape_options* o) {
   if (!o) return;
   std::memset(o, 0, sizeof *o);
-  o->controller = 1;
+  o->controller = 0;
+  o->newton_start = 0;
   o->h0 = 1e-3;
   o->h_max = 1.0;
   o->h_min_factor = 0.1;

@@ -334,9 +334,14 @@ AttemptResult Context::attempt(double h, double scale) {
     return out;
   };
   check(launch_predict(dp_, xn_.ptr, h * h, xhat_.ptr, stream_), "predict");
-  check(launch_sub(int(nv), xhat_.ptr, xn_.ptr, towards_.ptr, stream_), "towards");
-  double a0 = t_phase(kCcd, [&] { return max_step(xn_.ptr, towards_.ptr); });
-  check(launch_axpy(int(nv), xn_.ptr, a0, towards_.ptr, x_.ptr, stream_), "start");
+  if (opt_.newton_start == 1) {
+    // The reference's start: x_n + alpha_max (x_hat - x_n).
+    check(launch_sub(int(nv), xhat_.ptr, xn_.ptr, towards_.ptr, stream_), "towards");
+    double a0 = t_phase(kCcd, [&] { return max_step(xn_.ptr, towards_.ptr); });
+    check(launch_axpy(int(nv), xn_.ptr, a0, towards_.ptr, x_.ptr, stream_), "start");
+  } else {
+    check(cudaMemcpyAsync(x_.ptr, xn_.ptr, nv * sizeof(double), cudaMemcpyDeviceToDevice, stream_), "start");
+  }
   double mu = 0.0, eta = opt_.forcing ? 1e-2 : opt_.pcg_rtol, prev_norm = 0.0;
   for (int it = 0;; ++it) {
     double norm = t_phase(kAssembly, [&] { return assemble(x_.ptr, inv_h2, mu, 0, true); });

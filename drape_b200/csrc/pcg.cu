@@ -164,9 +164,12 @@ __global__ void __launch_bounds__(256) pcg_kernel(PcgArgs a) {
     float4* pold = cur ? a.p1 : a.p0;
     float4* pnew = cur ? a.p0 : a.p1;
     float pq_l = 0.0f;
-    for (int row = r_begin + group; row < r_end; row += groups) {
+    // Uniform trip count across the CTA: every lane reaches the group shuffles in every pass.
+    for (int row0 = r_begin; row0 < r_end; row0 += groups) {
+      const int row = row0 + group;
+      const bool active = row < r_end;
       float y0 = 0.f, y1 = 0.f, y2 = 0.f;
-      const int kb = a.row_ptr[row], ke = a.row_ptr[row + 1];
+      const int kb = active ? a.row_ptr[row] : 0, ke = active ? a.row_ptr[row + 1] : 0;
       for (int k = kb + gl; k < ke; k += LPR) {
         const int c = __ldg(a.col_idx + k);
         float4 pc = __ldcg(pold + c);
@@ -177,7 +180,7 @@ __global__ void __launch_bounds__(256) pcg_kernel(PcgArgs a) {
         block_apply(a.A, k, pc.x, pc.y, pc.z, y0, y1, y2);
       }
       group_reduce<LPR>(y0, y1, y2);
-      if (gl == 0) {
+      if (active && gl == 0) {
         float4 p = pold[row];
         if (fused) {
           const float4 z = a.z[row];
@@ -243,14 +246,17 @@ __global__ void __launch_bounds__(256) pcg_kernel(PcgArgs a) {
       // (grid_total above) before any CTA rewrites them below.
       if (!grid_barrier(st, G, a.spin_limit)) return;
       rz_l = rr_l = 0.0f;
-      for (int row = r_begin + group; row < r_end; row += groups) {
+      for (int row0 = r_begin; row0 < r_end; row0 += groups) {
+        const int row = row0 + group;
+        const bool active = row < r_end;
         float y0 = 0.f, y1 = 0.f, y2 = 0.f;
-        for (int k = a.row_ptr[row] + gl; k < a.row_ptr[row + 1]; k += LPR) {
+        const int kb = active ? a.row_ptr[row] : 0, ke = active ? a.row_ptr[row + 1] : 0;
+        for (int k = kb + gl; k < ke; k += LPR) {
           const float4 xc = __ldcg(a.x + __ldg(a.col_idx + k));
           block_apply(a.A, k, xc.x, xc.y, xc.z, y0, y1, y2);
         }
         group_reduce<LPR>(y0, y1, y2);
-        if (gl == 0) {
+        if (active && gl == 0) {
           const float4 b = a.b[row];
           const float4 r = f4(b.x - y0, b.y - y1, b.z - y2);
           const float4 z = f4(dot3(a.dinv[3 * row], r), dot3(a.dinv[3 * row + 1], r), dot3(a.dinv[3 * row + 2], r));
@@ -285,14 +291,18 @@ __global__ void __launch_bounds__(256) spmv_kernel(int R, const int* __restrict_
                                                    DevBsr A, const float4* __restrict__ p, float4* __restrict__ y) {
   const int groups = blockDim.x / LPR;
   const int gl = threadIdx.x % LPR;
-  for (int row = blockIdx.x * groups + threadIdx.x / LPR; row < R; row += gridDim.x * groups) {
+  // Uniform trip count across the grid so every lane reaches the group shuffles.
+  for (int row0 = blockIdx.x * groups; row0 < R; row0 += gridDim.x * groups) {
+    const int row = row0 + threadIdx.x / LPR;
+    const bool active = row < R;
     float y0 = 0.f, y1 = 0.f, y2 = 0.f;
-    for (int k = row_ptr[row] + gl; k < row_ptr[row + 1]; k += LPR) {
+    const int kb = active ? row_ptr[row] : 0, ke = active ? row_ptr[row + 1] : 0;
+    for (int k = kb + gl; k < ke; k += LPR) {
       const float4 pc = __ldg(p + __ldg(col_idx + k));
       block_apply(A, k, pc.x, pc.y, pc.z, y0, y1, y2);
     }
     group_reduce<LPR>(y0, y1, y2);
-    if (gl == 0) y[row] = f4(y0, y1, y2);
+    if (active && gl == 0) y[row] = f4(y0, y1, y2);
   }
 }
 
@@ -303,9 +313,14 @@ __global__ void __launch_bounds__(256) refine_residual_kernel(int R, const int* 
   __shared__ double red[32];
   const int gl = threadIdx.x & 7;
   double s = 0.0;
-  for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 3; row < R; row += (gridDim.x * blockDim.x) >> 3) {
+  const int groups = blockDim.x >> 3;
+  // Uniform trip count across the grid so every lane reaches the group shuffles.
+  for (int row0 = blockIdx.x * groups; row0 < R; row0 += gridDim.x * groups) {
+    const int row = row0 + (threadIdx.x >> 3);
+    const bool active = row < R;
     double y0 = 0.0, y1 = 0.0, y2 = 0.0;
-    for (int k = row_ptr[row] + gl; k < row_ptr[row + 1]; k += 8) {
+    const int kb = active ? row_ptr[row] : 0, ke = active ? row_ptr[row + 1] : 0;
+    for (int k = kb + gl; k < ke; k += 8) {
       const float4 dc = d[col_idx[k]];
       const float4 m0 = A.a0[k], m1 = A.a1[k];
       const float m8 = A.a2[k];
@@ -319,7 +334,7 @@ __global__ void __launch_bounds__(256) refine_residual_kernel(int R, const int* 
       y1 += __shfl_xor_sync(0xffffffffu, y1, o, 8);
       y2 += __shfl_xor_sync(0xffffffffu, y2, o, 8);
     }
-    if (gl == 0) {
+    if (active && gl == 0) {
       // neg_g holds the f64 gradient g; the right-hand side is -g.
       const double r0 = -neg_g[3 * row] - y0, r1 = -neg_g[3 * row + 1] - y1, r2 = -neg_g[3 * row + 2] - y2;
       r_out[row] = f4(float(r0), float(r1), float(r2));

@@ -76,6 +76,9 @@ typedef struct {
   double time_budget_s;        /* 0: none */
   int32_t pcg_grid, pcg_threads, pcg_lanes; /* 0: automatic */
   int32_t progress;            /* 1: one stderr line per accepted PTC step */
+  int32_t newton_start;        /* inner Newton start: 0 the current state x_k (feasible; grad Phi(x_k) = grad E_s);
+                                  1 the reference's prediction x_k + h^2 g cut back by the CCD bound
+                                  (drape-e4.ts:55-62, e7_ptc.rs:129-133) */
 } drape_options;
 
 /* Outcome of drape_solve_equilibrium (gpu-result.json fields, run-e7.ts:100-106). */
@@ -95,9 +98,10 @@ typedef struct {
 /* Library version string. */
 const char* drape_version(void);
 
-/* Fills the sheet-over-sphere rules: doubling controller from h0 = 1e-3 s, |grad E_s| <= 1e-6 N, PCG rtol 1e-6,
- * at most 2000 PCG iterations, inner Newton tol 0.1 and 10 updates (replaces parsePtcRules/parseRobustRules,
- * ptc.ts:28-32, robust-newton.ts:208-214). */
+/* Fills the sheet-over-sphere rules: h0 = 1e-3 s doubled after each accepted step whose inner Newton stayed below
+ * its cap (halved at the cap), |grad E_s| <= 1e-6 N, PCG rtol 1e-6 with at most 2000 iterations, inner Newton
+ * tol 0.1 and 10 updates from the current state (replaces parsePtcRules/parseRobustRules, ptc.ts:28-32,
+ * robust-newton.ts:208-214). */
 void drape_default_options(drape_options* out);
 
 /* Creates a context on `device` from borrowed arrays (replaces prepareDrapeGpu, drape-gpu.ts:141-162). */

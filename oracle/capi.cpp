@@ -153,11 +153,13 @@ double oracle_static_energy(void* p, const double* x) {
 }
 
 // PTC to equilibrium from `start` (null: the scene's cold start). controller 0 inner-count (reference), 1 doubling.
-// direction 0 band Cholesky, 1 f64 block-Jacobi PCG (rtol, maxit). Stops at r/L <= equilibrium, r <= absolute
+// direction 0 band Cholesky, 1 f64 block-Jacobi PCG (rtol, maxit). predicted_start 1: the reference's CCD-cut
+// prediction as the inner Newton start, 0: the current state. Stops at r/L <= equilibrium, r <= absolute
 // (when > 0), the floor rule (floor != 0), max_steps, or a stall. stats: [steps, newton, rejected, pcg, final_r,
 // final_h, seconds, converged, reason code (0 tolerance 1 floor 2 cap 3 stalled)].
 int oracle_ptc(void* p, const double* start, double h0, int controller, double equilibrium, double absolute, int floor,
-               int max_steps, int direction, double rtol, int maxit, int progress, double* x_out, double* stats) {
+               int max_steps, int direction, double rtol, int maxit, int progress, int predicted_start, double* x_out,
+               double* stats) {
   try {
     auto& d = *static_cast<Handle*>(p)->drape;
     PtcRules r = PtcRules::reference();
@@ -166,6 +168,7 @@ int oracle_ptc(void* p, const double* start, double h0, int controller, double e
     r.equilibrium = equilibrium;
     r.absolute = absolute;
     r.floor_rule = floor != 0;
+    r.predicted_start = predicted_start != 0;
     r.max_steps = max_steps;
     DirectionSolver dir{direction != 0, rtol, maxit};
     auto x0 = start ? to_vec3(start, d.mesh.rest.size()) : d.start;

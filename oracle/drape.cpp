@@ -443,7 +443,7 @@ static StepSolution inner_solve(const Drape& d, const std::vector<Vec3>& x, doub
   d.time_step = h;
   DrapeStep sys{&d, ptc_prediction(d, x, h)};
   NewtonSettings set{rules.inner_tolerance, rules.inner_max, 1e-4, 30};
-  return solve_step_regularized(sys, feasible_start(sys, x), residual, set, dir);
+  return solve_step_regularized(sys, rules.predicted_start ? feasible_start(sys, x) : x, residual, set, dir);
 }
 
 static bool attempt(const Drape& d, const std::vector<Vec3>& x, double h, double residual, const PtcRules& rules,

@@ -40,7 +40,7 @@ def test_every_declared_symbol_is_exported(lib):
 
 def test_options_struct_matches_the_header(lib):
     o = api.default_options()
-    assert o.controller == 1 and o.h0 == 1e-3 and o.equilibrium_absolute == 1e-6
+    assert o.controller == 0 and o.newton_start == 0 and o.h0 == 1e-3 and o.equilibrium_absolute == 1e-6
     assert o.pcg_rtol == 1e-6 and o.pcg_max_iterations == 2000 and o.inner_max == 10 and o.max_halvings == 30
 
 

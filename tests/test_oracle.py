@@ -93,7 +93,8 @@ def test_cold_ptc_reaches_the_reference_equilibrium_n17(edit):
     different path (32 vs 51 steps); like the reference's own n33 w1 branch it is not a parity target."""
     gold = GOLDEN["drape7"][f"drape-n17/{edit}"]["references"]["cold"]
     s = oracle_py.Scene("reference", 17, edit=edit)
-    x, st = s.ptc(h0=1.0 / 240.0, doubling=False, equilibrium=1e-8, absolute=0.0, floor=True, pcg=False)
+    x, st = s.ptc(h0=1.0 / 240.0, doubling=False, equilibrium=1e-8, absolute=0.0, floor=True, pcg=False,
+                  predicted_start=True)
     assert st["converged"] == 1.0
     e = s.static_energy(x)
     assert abs(e - gold["static_energy"]) <= 1e-10 * gold["static_energy"], (e, gold["static_energy"])
@@ -105,7 +106,8 @@ def test_cold_ptc_reaches_the_reference_equilibrium_n17(edit):
 def test_cold_ptc_reaches_the_reference_equilibrium_n33():
     gold = GOLDEN["drape7"]["drape-n33/base"]["references"]["cold"]
     s = oracle_py.Scene("reference", 33, edit="base")
-    x, st = s.ptc(h0=1.0 / 240.0, doubling=False, equilibrium=1e-8, absolute=0.0, floor=True, pcg=False)
+    x, st = s.ptc(h0=1.0 / 240.0, doubling=False, equilibrium=1e-8, absolute=0.0, floor=True, pcg=False,
+                  predicted_start=True)
     assert st["converged"] == 1.0
     e = s.static_energy(x)
     assert abs(e - gold["static_energy"]) <= 1e-10 * gold["static_energy"], (e, gold["static_energy"])
