@@ -1,0 +1,292 @@
+"""Benchmark of the quasi-static drape GPU stage (one JSON line on rank 0).
+
+Workload: the 1.0 m sheet of n x n vertices (default n = 129: 16641 vertices, 32768 triangles, 48896 hinges,
+180993 BSR blocks) over a sphere of radius 0.25 m and a ground plane at y = -0.25 m, isotropic StVK E = 5e5 Pa,
+nu = 0.3, t = 5e-4 m, k_b = 1e-5 N m, IPC d_hat = 2e-3 m, kappa = 1e3; PTC from dt0 = 1e-3 s to
+|grad E_s| <= 1e-6 N with block-Jacobi PCG (rtol 1e-6, <= 2000 iterations). One step = one full cold solve to
+the converged state. Synthetic scene (the reference ships no dataset; seeded jitter, seed 0).
+
+value: seconds per converged solve with the problem resident in HBM (CUDA-event-timed solve, max over ranks).
+e2e:   the same through the C ABI from host arrays: drape_create (host->device copies) + solve + drape_get_state
+       (device->host), wall clock on the host.
+--impl reference: the reference's CPU implementation of this path (the f64 oracle restatement; the Rust crate
+       cannot be built here), single-threaded like the reference, on a bounded sample of the same solve.
+Multi-GPU: replicas only (one independent drape per rank, no collective on the data path).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "n129 drape wall-time to converged state"
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "_fallback": True}
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.proc or not os.path.exists(self.path):
+            return None
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [v.strip() for v in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.remove(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def flush_l2(torch, device):
+    """Writes 512 MiB (> the 126 MB L2) so every timed solve starts cold."""
+    buf = torch.empty(128 * 1024 * 1024, dtype=torch.float32, device=device)
+    buf.fill_(1.0)
+    torch.cuda.synchronize(device)
+    del buf
+
+
+def run_gpu(args):
+    import numpy as np
+    import torch
+
+    from drape_b200 import api
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    opts = api.default_options(pcg_max_iterations=args.pcg_max, max_steps=args.max_steps)
+    # Host arrays for the end-to-end leg (built outside every timed region).
+    pdir = tempfile.mkdtemp(prefix="drape_bench_")
+    api.write_sheet_problem(pdir, args.n, seed=args.seed, plane=bool(args.plane))
+    meta, arr = api.read_problem_arrays(pdir)
+    host = dict(start=arr["rest_positions_f64"], row_vertex=arr["row_vertex"], unit_mass=arr["row_unit_mass_f64"],
+                row_ptr=arr["row_ptr"], col_idx=arr["col_idx"], tri=arr["elem_vertices"], geom=arr["elem_geom_f64"],
+                hinge=arr["hinge_vertices"], hinge_k=arr["hinge_stiffness_f64"],
+                material=(meta["material"]["wale_N_per_m"], meta["material"]["course_N_per_m"],
+                          meta["material"]["coupling_N_per_m"], meta["material"]["shear_N_per_m"]),
+                gravity=tuple(meta["gravity_vector"]), colliders=arr["colliders"][4:].astype(np.float64),
+                dhat=meta["contact"]["dhat_m"], kappa=meta["contact"]["kappa"], columns=args.n)
+    h2d = sum(v.nbytes for v in host.values() if hasattr(v, "nbytes"))
+    drape = api.Drape.from_arrays(**host, options=opts, device=local)
+    start = drape.state.copy()
+    d2h = start.nbytes
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+
+    def one_solve():
+        drape.state = start
+        flush_l2(torch, local)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        ev0.record()
+        log = drape.solve_equilibrium(check=False)
+        ev1.record()
+        barrier()
+        return log, ev0.elapsed_time(ev1) / 1e3
+
+    for _ in range(args.warmup):
+        one_solve()
+    logs, secs = [], []
+    with ClockSampler(local) as clock:
+        for _ in range(args.steps):
+            log, s = one_solve()
+            logs.append(log)
+            secs.append(s)
+    clocks = clock.summary()
+    # End-to-end through the public C ABI from host buffers.
+    e2e = []
+    for _ in range(max(1, min(args.steps, 2))):
+        flush_l2(torch, local)
+        barrier()
+        t0 = time.perf_counter()
+        d2 = api.Drape.from_arrays(**host, options=opts, device=local)
+        d2.solve_equilibrium(check=False)
+        _ = d2.state
+        torch.cuda.synchronize()
+        e2e.append(time.perf_counter() - t0)
+        d2.close()
+    t = sum(secs) / len(secs)
+    t_e2e = sum(e2e) / len(e2e)
+    if dist:
+        v = torch.tensor([t, t_e2e], device=f"cuda:{local}")
+        dist.all_reduce(v, op=dist.ReduceOp.MAX)
+        t, t_e2e = v.tolist()
+    last = logs[-1]
+    R, B = drape.R, drape.B
+    bytes_per_iter = 40 * B + 196 * R
+    pk = peaks()
+    achieved = (bytes_per_iter * last["pcg_iterations"]) / (last["ms_pcg"] / 1e3) / 1e9 if last["ms_pcg"] > 0 else 0.0
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "pcg_traffic.json")
+    if os.path.exists(tpath):
+        tr = json.load(open(tpath))
+        if tr.get("columns") == args.n:
+            traffic = tr["dram_bytes_per_iteration"] * last["pcg_iterations"] / max(1, last.get("pcg_launches", 1))
+    out = {
+        "metric": METRIC, "value": t, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"sheet n{args.n} over sphere r=0.25 + ground plane y=-0.25, block-Jacobi PCG, "
+                               f"PTC dt0=1e-3 s to |grad E_s|<=1e-6 N", "columns": args.n, "rows": R, "blocks": B,
+                   "seed": args.seed, "preconditioner": "block-jacobi", "parallelism": f"replicas{world}",
+                   "l2": "flushed (512 MiB write) before every timed solve"},
+        "solve": {"converged": last["reason"] == "tolerance", "reason": last["reason"],
+                  "final_residual_N": last["final_residual"], "ptc_steps": last["ptc_steps"],
+                  "newton_iterations": last["newton_iterations"], "pcg_iterations": last["pcg_iterations"],
+                  "pcg_per_newton": last["pcg_iterations"] / max(1, last["newton_iterations"]),
+                  "rejected_attempts": last["rejected_attempts"], "static_energy_J": last["static_energy"],
+                  "phase_ms": {k: last[k] for k in ("ms_assembly", "ms_pcg", "ms_line_search", "ms_ccd", "ms_other")}},
+        "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": None,
+        "roofline": {"bound": "hbm", "kernel": "pcg_kernel (persistent block-Jacobi PCG)", "achieved": achieved,
+                     "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
+                     "traffic": traffic, "peak_source": "fallback" if pk.get("_fallback") else "measured",
+                     "algorithmic_bytes_per_pcg_iteration": bytes_per_iter},
+        "clocks": clocks,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(args, last)
+    if dist:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def cpu_baseline(args, gpu_log=None, budget_s=None):
+    """The f64 oracle (port of the reference crate's method: exact tangent, LM, f64 block-Jacobi PCG rtol 1e-6
+    <= 2000 iterations, inner-count PTC from dt0 = 1e-3 s) on a bounded sample of the same solve: it runs PTC
+    steps until `budget_s` of CPU time has passed, and the full-solve time is its seconds per Newton iteration
+    times the Newton iterations of the full solve (the GPU's, when given, else the sample's rate over the
+    oracle's own PTC step cap is not extrapolated)."""
+    from tests import oracle_py
+
+    budget = budget_s if budget_s is not None else args.cpu_budget
+    s = oracle_py.Scene("sheet", args.n, seed=args.seed, plane=bool(args.plane))
+    # The cold solve, stopped at the first PTC step that ends past the CPU budget.
+    _, st = s.ptc(h0=1e-3, doubling=False, absolute=1e-6, pcg=True, rtol=1e-6, maxit=2000, budget_s=budget)
+    steps, elapsed, newton = int(st["steps"]), st["seconds"], int(st["newton"])
+    per_newton = elapsed / max(1, newton)
+    full_newton = gpu_log["newton_iterations"] if gpu_log else newton
+    return {"value": per_newton * full_newton, "unit": "s", "cores": 1, "kind": "port",
+            "sample": f"{steps} PTC steps ({newton} Newton iterations) of the n{args.n} solve in {elapsed:.1f} s on 1 "
+                      f"host core; value = {per_newton:.3f} s per Newton iteration x {full_newton} Newton iterations "
+                      f"of the full solve",
+            "host_cpu": _cpu_model()}
+
+
+def _cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from tests import oracle_py
+
+    oracle_py.build()
+    results = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(args, None, budget_s=args.cpu_budget)
+        if i >= args.warmup:
+            results.append(r)
+    v = sum(r["value"] for r in results) / len(results)
+    out = {"metric": METRIC, "value": v, "unit": "s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+           "config": {"workload": f"sheet n{args.n} over sphere r=0.25 + ground plane y=-0.25, f64 oracle port "
+                                  f"(exact tangent, LM, block-Jacobi PCG rtol 1e-6 <= 2000)", "columns": args.n},
+           "cpu_baseline": {"value": v, "unit": "s", "cores": 1, "kind": "port", "sample": results[-1]["sample"]},
+           "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="drape_b200", choices=["drape_b200", "reference"])
+    ap.add_argument("--n", type=int, default=129)
+    ap.add_argument("--plane", type=int, default=1)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--pcg-max", type=int, default=2000)
+    ap.add_argument("--max-steps", type=int, default=1000)
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

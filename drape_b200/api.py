@@ -37,7 +37,7 @@ class Options(ctypes.Structure):
         ("curvature", ctypes.c_int32), ("preconditioner", ctypes.c_int32), ("armijo", ctypes.c_double),
         ("max_halvings", ctypes.c_int32), ("time_budget_s", ctypes.c_double), ("pcg_grid", ctypes.c_int32),
         ("pcg_threads", ctypes.c_int32), ("pcg_lanes", ctypes.c_int32), ("progress", ctypes.c_int32),
-        ("newton_start", ctypes.c_int32),
+        ("newton_start", ctypes.c_int32), ("tangent", ctypes.c_int32),
     ]
 
 

@@ -80,7 +80,8 @@ void drape_default_options(drape_options* o) {
   o->replace_above = 1e-2;
   o->refine = 1;
   o->refine_rtol = 0.1;
-  o->curvature = 0;
+  o->curvature = 1;
+  o->tangent = 0;
   o->preconditioner = 0;
   o->armijo = 1e-4;
   o->max_halvings = 30;

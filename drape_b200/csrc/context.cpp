@@ -256,6 +256,7 @@ double Context::assemble(const double* x, double inv_h2, double mu, int mode, bo
   a.mu = mu;
   a.mode = mode;
   a.curvature = opt_.curvature;
+  a.exact = opt_.tangent == 0;
   a.grad = g_.ptr;
   a.bsr = hessian ? DevBsr{a0_.ptr, a1_.ptr, a2_.ptr} : DevBsr{nullptr, nullptr, nullptr};
   a.partial = partial_.ptr;
@@ -622,6 +623,8 @@ float Context::time_assembly(int launches) {
   a.x_hat = x_.ptr;
   a.inv_h2 = 1.0;
   a.mode = 0;
+  a.exact = opt_.tangent == 0;
+  a.curvature = opt_.curvature;
   a.grad = g_.ptr;
   a.bsr = DevBsr{a0_.ptr, a1_.ptr, a2_.ptr};
   a.partial = partial_.ptr;

@@ -100,12 +100,13 @@ __device__ __forceinline__ V3 membrane_gradient_row(const Membrane& m, const Tri
   return (pw * G.g[k][0] + pc * G.g[k][1]) * G.area;
 }
 
-// Row k of the stress-clamped membrane Hessian: blocks (k, l) for l = 0..2, row-major 3x3 each.
+// Row k of the membrane Hessian: blocks (k, l) for l = 0..2, row-major 3x3 each. `clamp` projects the stress
+// onto its positive part (PSD, membrane.rs:54-57); otherwise this is the exact tangent (membrane.rs:59-62).
 __device__ __forceinline__ void membrane_hessian_row(const Membrane& m, const TriGeom& G, V3 fw, V3 fc, int k,
-                                                     double out[3][9]) {
+                                                     double out[3][9], bool clamp) {
   double s[3];
   stress_of(m, fw, fc, s);
-  clamp_stress(s);
+  if (clamp) clamp_stress(s);
   V3 bw[3], bc[3], bs[3];
 #pragma unroll
   for (int l = 0; l < 3; ++l) {
@@ -166,6 +167,64 @@ __device__ __forceinline__ void hinge_angle_gradient(V3 x1, V3 x2, V3 x3, V3 x4,
   g[1] = a2 * (-len);
   g[2] = (a1 * (dot(x1 - x4, e) / len) + a2 * (dot(x2 - x4, e) / len)) * -1.0;
   g[3] = (a1 * (dot(x1 - x3, e) / len) + a2 * (dot(x2 - x3, e) / len));
+}
+
+// Forward-mode dual numbers (value, derivative along one seed direction): differentiating the analytic
+// gradient with them gives the exact Hessian column without new formulas (dual.rs:6-90, hinge.rs:66-82).
+struct Dual {
+  double v, t;
+};
+__device__ __forceinline__ Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.t + b.t}; }
+__device__ __forceinline__ Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.t - b.t}; }
+__device__ __forceinline__ Dual operator*(Dual a, Dual b) { return {a.v * b.v, a.t * b.v + a.v * b.t}; }
+__device__ __forceinline__ Dual operator/(Dual a, Dual b) { return {a.v / b.v, (a.t * b.v - a.v * b.t) / (b.v * b.v)}; }
+__device__ __forceinline__ Dual dsqrt(Dual a) {
+  const double s = sqrt(a.v);
+  return {s, a.t / (2.0 * s)};
+}
+struct DV3 {
+  Dual x, y, z;
+};
+__device__ __forceinline__ DV3 operator-(DV3 a, DV3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ DV3 operator+(DV3 a, DV3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ DV3 operator*(DV3 a, Dual s) { return {a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ Dual ddot(DV3 a, DV3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ DV3 dcross(DV3 a, DV3 b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+
+// Component k of d theta / dx in dual arithmetic (the same formula as hinge_angle_gradient).
+__device__ __forceinline__ DV3 hinge_angle_gradient_dual(DV3 x1, DV3 x2, DV3 x3, DV3 x4, int k) {
+  const DV3 e = x4 - x3;
+  const Dual len = dsqrt(ddot(e, e));
+  const DV3 n1 = dcross(x1 - x3, x1 - x4), n2 = dcross(x2 - x4, x2 - x3);
+  const Dual one{1.0, 0.0}, mone{-1.0, 0.0};
+  const DV3 a1 = n1 * (one / ddot(n1, n1)), a2 = n2 * (one / ddot(n2, n2));
+  if (k == 0) return a1 * (mone * len);
+  if (k == 1) return a2 * (mone * len);
+  if (k == 2) return (a1 * (ddot(x1 - x4, e) / len) + a2 * (ddot(x2 - x4, e) / len)) * mone;
+  return a1 * (ddot(x1 - x3, e) / len) + a2 * (ddot(x2 - x3, e) / len);
+}
+
+// Row k of the exact hinge Hessian 2c (grad theta grad theta^T + theta d2 theta): blocks (k, l), l = 0..3.
+__device__ __forceinline__ void hinge_exact_hessian_row(const V3 x[4], const V3 dg[4], double theta, double c2, int k,
+                                                        double out[4][9]) {
+#pragma unroll 1
+  for (int l = 0; l < 4; ++l)
+#pragma unroll 1
+    for (int c = 0; c < 3; ++c) {
+      DV3 p[4];
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        const double sx = (m == l && c == 0) ? 1.0 : 0.0, sy = (m == l && c == 1) ? 1.0 : 0.0,
+                     sz = (m == l && c == 2) ? 1.0 : 0.0;
+        p[m] = {{x[m].x, sx}, {x[m].y, sy}, {x[m].z, sz}};
+      }
+      const DV3 col = hinge_angle_gradient_dual(p[0], p[1], p[2], p[3], k);
+      const double h[3] = {col.x.t, col.y.t, col.z.t};
+#pragma unroll
+      for (int r = 0; r < 3; ++r) out[l][3 * r + c] = c2 * (comp(dg[k], r) * comp(dg[l], c) + theta * h[r]);
+    }
 }
 
 // Barrier b(d) = -kappa (d - dhat)^2 ln(d / dhat) on 0 < d < dhat, and its first two derivatives.

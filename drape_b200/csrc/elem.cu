@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(32 * WARPS_PER_CTA) assemble_rows(AssembleArgs
         V3 fw, fc;
         columns(G, load3(a.x, tv[0]), load3(a.x, tv[1]), load3(a.x, tv[2]), fw, fc);
         g = membrane_gradient_row(mat, G, fw, fc, k);
-        if (hess) membrane_hessian_row(mat, G, fw, fc, k, blk);
+        if (hess) membrane_hessian_row(mat, G, fw, fc, k, blk, !a.exact);
         nslot = 3;
         if (hess)
           for (int l = 0; l < 3; ++l) slots[warp][lane][l] = p.rt_pos[3 * (size_t)(t0 + lane) + l];
@@ -82,11 +82,16 @@ __global__ void __launch_bounds__(32 * WARPS_PER_CTA) assemble_rows(AssembleArgs
         V3 dg[4];
         hinge_angle_gradient(x1, x2, x3, x4, dg);
         const double c2 = 2.0 * p.hinge_k[h];
-        g = dg[k] * (c2 * hinge_angle(x1, x2, x3, x4));
-        if (hess)
+        const double theta = hinge_angle(x1, x2, x3, x4);
+        g = dg[k] * (c2 * theta);
+        if (hess && a.exact) {
+          const V3 xs[4] = {x1, x2, x3, x4};
+          hinge_exact_hessian_row(xs, dg, theta, c2, k, blk);
+        } else if (hess) {
           for (int l = 0; l < 4; ++l)
             for (int r = 0; r < 3; ++r)
               for (int c = 0; c < 3; ++c) blk[l][3 * r + c] = c2 * comp(dg[k], r) * comp(dg[l], c);
+        }
         nslot = 4;
         if (hess)
           for (int l = 0; l < 4; ++l) slots[warp][lane][l] = p.rh_pos[4 * (size_t)(h0 + eh) + l];

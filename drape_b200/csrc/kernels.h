@@ -18,7 +18,8 @@ struct AssembleArgs {
   double inv_h2;    // 1/h^2 (mode 0)
   double mu;        // the diagonal carries (1 + mu) m/h^2 (mode 0)
   int mode;         // 0: grad Phi = m/h^2 (x - x_hat) + grad Pi;  1: grad E_s = grad Pi - m g (no inertia block)
-  int curvature;    // 1 keeps the barrier's b' (I - n n^T)/|x - c| term (negative semidefinite: off by default)
+  int curvature;    // 1 keeps the barrier's b' (I - n n^T)/|x - c| term (negative semidefinite)
+  int exact;        // 1: exact tangent (StVK stress, 2c(grad grad^T + theta d2 theta)); 0: clamped stress + Gauss-Newton
   double* grad;     // f64 [3R]
   DevBsr bsr;       // f32 blocks; a0 == nullptr computes the gradient only
   double* partial;  // f64 [assemble_grid(R)]: per-CTA sum of |grad_row|^2 (may be null)

@@ -79,6 +79,8 @@ typedef struct {
   int32_t newton_start;        /* inner Newton start: 0 the current state x_k (feasible; grad Phi(x_k) = grad E_s);
                                   1 the reference's prediction x_k + h^2 g cut back by the CCD bound
                                   (drape-e4.ts:55-62, e7_ptc.rs:129-133) */
+  int32_t tangent;             /* 0: exact tangent (drape.rs:15-21 TangentKind::Exact) with Levenberg-Marquardt mu;
+                                  1: projected (clamped membrane stress, Gauss-Newton hinge): SPD up to the barrier */
 } drape_options;
 
 /* Outcome of drape_solve_equilibrium (gpu-result.json fields, run-e7.ts:100-106). */

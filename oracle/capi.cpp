@@ -158,8 +158,8 @@ double oracle_static_energy(void* p, const double* x) {
 // (when > 0), the floor rule (floor != 0), max_steps, or a stall. stats: [steps, newton, rejected, pcg, final_r,
 // final_h, seconds, converged, reason code (0 tolerance 1 floor 2 cap 3 stalled)].
 int oracle_ptc(void* p, const double* start, double h0, int controller, double equilibrium, double absolute, int floor,
-               int max_steps, int direction, double rtol, int maxit, int progress, int predicted_start, double* x_out,
-               double* stats) {
+               int max_steps, int direction, double rtol, int maxit, int progress, int predicted_start, double budget_s,
+               double* x_out, double* stats) {
   try {
     auto& d = *static_cast<Handle*>(p)->drape;
     PtcRules r = PtcRules::reference();
@@ -170,6 +170,7 @@ int oracle_ptc(void* p, const double* start, double h0, int controller, double e
     r.floor_rule = floor != 0;
     r.predicted_start = predicted_start != 0;
     r.max_steps = max_steps;
+    r.time_budget_s = budget_s;
     DirectionSolver dir{direction != 0, rtol, maxit};
     auto x0 = start ? to_vec3(start, d.mesh.rest.size()) : d.start;
     auto t0 = std::chrono::steady_clock::now();

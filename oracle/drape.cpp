@@ -1,6 +1,7 @@
 // Test infrastructure only (see core.h). Implementation of drape.h.
 #include "drape.h"
 
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 
@@ -492,8 +493,14 @@ PtcRun ptc_solve(const Drape& d, std::vector<Vec3> start, double h_start, const 
   run.final_h = h_start;
   run.states.push_back(std::move(start));
   std::vector<Vec3> x = run.states.back();
+  auto t0 = std::chrono::steady_clock::now();
   for (;;) {
     run.final_residual = vector_norm(static_gradient(d, x));
+    if (rules.time_budget_s > 0 &&
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > rules.time_budget_s) {
+      run.reason = "time_budget";
+      break;
+    }
     if (const char* reason = equilibrium_reason(d, x, run.final_residual, rules)) {
       run.reason = reason;
       break;

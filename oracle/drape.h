@@ -155,6 +155,7 @@ struct PtcRules {
   // Inner Newton start: the reference's prediction x_k + h^2 g cut back by the CCD bound (e7_ptc.rs:129-133),
   // or the current state x_k (feasible, and grad Phi(x_k) = grad E_s(x_k)).
   bool predicted_start = true;
+  double time_budget_s = 0.0;  // > 0: stop ("time_budget") once a step ends past this wall time
   static PtcRules reference() { return PtcRules{}; }
   // The sheet-over-sphere solve: dt0 = 1e-3 s, doubled after each accepted step, ||grad E_s|| <= 1e-6 N.
   static PtcRules doubling(double h0, double absolute) {

@@ -46,7 +46,7 @@ def load():
         lib.oracle_assemble.argtypes = [P, P, P, ctypes.c_double, ctypes.c_double, ctypes.c_int, P, P]
         lib.oracle_ptc.argtypes = [P, P, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                    ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
-                                   ctypes.c_int, ctypes.c_int, P, P]
+                                   ctypes.c_int, ctypes.c_int, ctypes.c_double, P, P]
         lib.oracle_pcg.argtypes = [ctypes.c_int, P, P, P, P, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                    ctypes.c_double, ctypes.c_int, ctypes.c_int, P, P]
         _lib = lib
@@ -128,12 +128,13 @@ class Scene:
         return self.lib.oracle_static_energy(P(self.h), ptr(x))
 
     def ptc(self, start=None, h0=1e-3, doubling=True, equilibrium=0.0, absolute=1e-6, floor=False,
-            max_steps=1000, pcg=True, rtol=1e-6, maxit=2000, progress=False, predicted_start=False):
+            max_steps=1000, pcg=True, rtol=1e-6, maxit=2000, progress=False, predicted_start=False, budget_s=0.0):
         x = np.zeros(3 * self.V)
         stats = np.zeros(9)
         s = None if start is None else ptr(np.ascontiguousarray(start, dtype=np.float64))
         if self.lib.oracle_ptc(P(self.h), s, h0, int(doubling), equilibrium, absolute, int(floor), max_steps,
-                               int(pcg), rtol, maxit, int(progress), int(predicted_start), ptr(x), ptr(stats)):
+                               int(pcg), rtol, maxit, int(progress), int(predicted_start), budget_s, ptr(x),
+                               ptr(stats)):
             raise RuntimeError(self.lib.oracle_last_error().decode())
         keys = ["steps", "newton", "rejected", "pcg", "final_residual", "final_h", "seconds", "converged", "reason"]
         return x, dict(zip(keys, stats.tolist()))
