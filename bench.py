@@ -182,7 +182,7 @@ def run_gpu(args):
     if os.path.exists(tpath):
         tr = json.load(open(tpath))
         if tr.get("columns") == args.n:
-            traffic = tr["dram_bytes_per_iteration"] * last["pcg_iterations"] / max(1, last.get("pcg_launches", 1))
+            traffic = tr["dram_bytes_per_iteration"] * last["pcg_iterations"] / max(1, last["pcg_launches"])
     out = {
         "metric": METRIC, "value": t, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",

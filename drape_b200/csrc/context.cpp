@@ -62,7 +62,7 @@ Context::Context(const HostProblem& problem, const drape_options& options, int d
   check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
   for (auto& e : ev_) check(cudaEventCreate(&e), "cudaEventCreate");
   check(cudaMallocHost(&pinned_, kSlots * sizeof(double)), "cudaMallocHost");
-  check(cudaMallocHost(&pinned_state_, sizeof(PcgState)), "cudaMallocHost");
+  check(cudaMallocHost(&pinned_state_, sizeof(PcgSyncHeader)), "cudaMallocHost");
   upload_problem();
 }
 
@@ -168,10 +168,8 @@ void Context::upload_problem() {
   a0_.alloc(B);
   a1_.alloc(B);
   a2_.alloc(B);
-  for (auto* a : {&b_, &px_, &pr_, &pz_, &pp0_, &pp1_, &pq_, &sol_, &corr_}) a->alloc(R);
-  dinv_.alloc(3 * size_t(R));
-  pcg_state_.alloc(1);
-  for (auto* a : {&b_, &px_, &pr_, &pz_, &pp0_, &pp1_, &pq_, &sol_, &corr_})
+  for (auto* a : {&b_, &px_, &pz_, &pp0_, &pp1_, &pq_, &sol_, &corr_}) a->alloc(R);
+  for (auto* a : {&b_, &px_, &pz_, &pp0_, &pp1_, &pq_, &sol_, &corr_})
     check(cudaMemsetAsync(a->ptr, 0, sizeof(float4) * a->n, stream_), "memset");
 
   dp_ = DevProblem{};
@@ -212,16 +210,45 @@ void Context::upload_problem() {
   for (double m : p.unit_mass) s += (m * gn) * (m * gn);
   gravity_load_ = std::sqrt(s);
 
-  // PCG launch shape: one CTA per ~64 rows up to one per SM (fewer CTAs = cheaper grid barriers).
-  pcg_cfg_.lanes_per_row = opt_.pcg_lanes > 0 ? opt_.pcg_lanes : 8;
-  pcg_cfg_.threads = opt_.pcg_threads > 0 ? opt_.pcg_threads : 256;
+  configure_pcg();
+  sync();
+}
+
+// PCG launch shape: 1024-thread CTAs whose lane groups cover each CTA's rows in one pass where possible, at most
+// one CTA per SM (fewer CTAs = fewer barrier words), and each CTA's matrix rows in shared memory when they fit.
+void Context::configure_pcg() {
+  const int R = host_.R;
+  PcgLaunch c;
+  c.lanes_per_row = opt_.pcg_lanes > 0 ? opt_.pcg_lanes : 8;
+  c.threads = opt_.pcg_threads > 0 ? opt_.pcg_threads : 1024;
+  if (c.threads % 32 || c.threads > 1024 || c.threads < c.lanes_per_row)
+    throw std::invalid_argument("unsupported PCG thread count");
   int sms = 0;
   check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_), "attribute");
-  int cap = pcg_max_grid(pcg_cfg_.threads, pcg_cfg_.lanes_per_row);
-  if (cap <= 0) throw std::invalid_argument("unsupported PCG launch shape");
-  int want = opt_.pcg_grid > 0 ? opt_.pcg_grid : std::min(sms, (R + 63) / 64);
-  pcg_cfg_.grid = std::max(1, std::min(want, cap));
-  sync();
+  const int groups = c.threads / c.lanes_per_row;
+  int grid = opt_.pcg_grid > 0 ? opt_.pcg_grid : std::min(sms, (R + groups - 1) / groups);
+  grid = std::max(1, std::min(grid, R));
+  for (;;) {
+    int cap_rows = 0, cap_blocks = 0;
+    for (int b = 0; b < grid; ++b) {
+      const int r0 = int((long long)R * b / grid), r1 = int((long long)R * (b + 1) / grid);
+      cap_rows = std::max(cap_rows, r1 - r0);
+      cap_blocks = std::max(cap_blocks, host_.row_ptr[r1] - host_.row_ptr[r0]);
+    }
+    c.matrix_in_smem = pcg_smem_bytes(cap_rows, cap_blocks, true) <= 200 * 1024;
+    c.smem = pcg_smem_bytes(cap_rows, cap_blocks, c.matrix_in_smem);
+    const int fit = pcg_max_grid(c.threads, c.lanes_per_row, c.smem, c.matrix_in_smem);
+    if (fit <= 0) throw std::invalid_argument("the PCG rows of one CTA do not fit in shared memory");
+    if (grid <= fit) {
+      c.grid = grid;
+      pcg_caps_[0] = cap_rows;
+      pcg_caps_[1] = cap_blocks;
+      break;
+    }
+    grid = fit;
+  }
+  pcg_cfg_ = c;
+  pcg_sync_.alloc((sizeof(PcgSyncHeader) + 16 * size_t(c.grid) + 7) / 8);
 }
 
 void Context::sync() { check(cudaStreamSynchronize(stream_), "stream synchronize"); }
@@ -273,31 +300,33 @@ PcgResult Context::pcg(double rtol, int max_iterations) {
   a.A = DevBsr{a0_.ptr, a1_.ptr, a2_.ptr};
   a.b = b_.ptr;
   a.x = px_.ptr;
-  a.r = pr_.ptr;
   a.z = pz_.ptr;
   a.p0 = pp0_.ptr;
   a.p1 = pp1_.ptr;
-  a.q = pq_.ptr;
-  a.dinv = dinv_.ptr;
-  a.state = pcg_state_.ptr;
+  auto* head = reinterpret_cast<PcgSyncHeader*>(pcg_sync_.ptr);
+  a.state = &head->state;
+  a.error = &head->error;
+  a.bcast = head->bcast;
+  a.slots = reinterpret_cast<unsigned long long*>(head + 1);
+  a.cap_rows = pcg_caps_[0];
+  a.cap_blocks = pcg_caps_[1];
   a.tol2 = float(rtol * rtol);
   a.max_iterations = max_iterations;
   a.replace_every = opt_.replace_every;
   a.replace_above2 = float(opt_.replace_above * opt_.replace_above);
-  a.spin_limit = 4000000000LL;  // ~2 s of SM clock per barrier wait
-  if (pcg_partial_.n < 3 * size_t(pcg_cfg_.grid)) pcg_partial_.alloc(3 * size_t(pcg_cfg_.grid));
-  a.partial = pcg_partial_.ptr;
-  check(cudaMemsetAsync(pcg_state_.ptr, 0, sizeof(PcgState), stream_), "memset");
+  a.spin_limit = 4000000000LL;  // ~2 s of SM clock per wait
+  check(cudaMemsetAsync(pcg_sync_.ptr, 0, pcg_sync_.n * sizeof(unsigned long long), stream_), "memset");
   check(cudaEventRecord(ev_[0], stream_), "event");
   check(launch_pcg(a, pcg_cfg_, stream_), "pcg launch");
   check(cudaEventRecord(ev_[1], stream_), "event");
-  check(cudaMemcpyAsync(pinned_state_, pcg_state_.ptr, sizeof(PcgState), cudaMemcpyDeviceToHost, stream_), "read");
+  check(cudaMemcpyAsync(pinned_state_, pcg_sync_.ptr, sizeof(PcgSyncHeader), cudaMemcpyDeviceToHost, stream_), "read");
   sync();
   PcgResult r;
   cudaEventElapsedTime(&r.ms, ev_[0], ev_[1]);
   phase_ms_[kPcg] += r.ms;
-  const PcgState& s = *pinned_state_;
-  if (s.error) throw CudaError(cudaErrorLaunchTimeout, "PCG grid barrier gave up waiting");
+  pcg_launches_++;
+  const PcgState& s = pinned_state_->state;
+  if (pinned_state_->error) throw CudaError(cudaErrorLaunchTimeout, "PCG grid wait gave up");
   r.iterations = s.iterations;
   r.status = s.status;
   r.replacements = s.replacements;
@@ -424,6 +453,7 @@ int Context::solve_equilibrium(const double* start, double h0, drape_run_log* lo
   double h = h0 > 0 ? h0 : opt_.h0;
   const double h_floor = opt_.h0 * opt_.h_min_factor;
   std::memset(phase_ms_, 0, sizeof phase_ms_);
+  pcg_launches_ = 0;
   steps_.clear();
   drape_run_log out{};
   out.gravity_load = L;
@@ -510,6 +540,8 @@ int Context::solve_equilibrium(const double* start, double h0, drape_run_log* lo
   out.ms_line_search = phase_ms_[kLineSearch];
   out.ms_ccd = phase_ms_[kCcd];
   out.ms_other = out.seconds * 1e3 - out.ms_assembly - out.ms_pcg - out.ms_line_search - out.ms_ccd;
+  out.pcg_launches = int(pcg_launches_);
+  out.pcg_grid = pcg_cfg_.grid;
   if (log) *log = out;
   return reason;
 }

@@ -108,6 +108,15 @@ class Context {
   DevProblem dp_{};
   double gravity_load_ = 0.0, final_h_ = 0.0;
   PcgLaunch pcg_cfg_;
+  int pcg_caps_[2] = {0, 0};
+  long long pcg_launches_ = 0;
+
+ public:
+  const PcgLaunch& pcg_launch() const { return pcg_cfg_; }
+  long long pcg_launches() const { return pcg_launches_; }
+
+ private:
+  void configure_pcg();
 
   // static problem arrays
   DeviceArray<double> geom_, hinge_k_, unit_mass_, colliders_;
@@ -119,11 +128,10 @@ class Context {
   // BSR f32 planes and PCG vectors (float4 rows)
   DeviceArray<float4> a0_, a1_;
   DeviceArray<float> a2_;
-  DeviceArray<float4> b_, px_, pr_, pz_, pp0_, pp1_, pq_, dinv_, sol_, corr_;
-  DeviceArray<float> pcg_partial_;
-  DeviceArray<PcgState> pcg_state_;
+  DeviceArray<float4> b_, px_, pz_, pp0_, pp1_, pq_, sol_, corr_;
+  DeviceArray<unsigned long long> pcg_sync_;  // PcgSyncHeader + 2 * grid partial words
   double* pinned_ = nullptr;
-  PcgState* pinned_state_ = nullptr;
+  PcgSyncHeader* pinned_state_ = nullptr;
   cudaEvent_t ev_[8] = {};
   std::vector<drape_step_record> steps_;
   double phase_ms_[6] = {};

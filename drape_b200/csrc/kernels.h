@@ -54,13 +54,11 @@ cudaError_t launch_rhs(int R, const double* g, float4* b, cudaStream_t s);
 // ---------------------------------------------------------------- PCG
 enum PcgStatus { kPcgRunning = 0, kPcgConverged = 1, kPcgIterationLimit = 2, kPcgBreakdown = 3, kPcgTimeout = 4 };
 
-// Device-resident solver state (the reference's 16-word State, state.wgsl:4-9, plus the grid barrier).
+// Device-resident solver result (the reference's 16-word State, state.wgsl:4-9).
 struct PcgState {
   float rz, rr, rr0, pq, alpha, beta;
   int iterations, status;
-  unsigned barrier_count, barrier_gen;
-  int error;  // a grid barrier gave up waiting (the kernel returned early)
-  int replacements;
+  int replacements, pad;
 };
 
 struct PcgArgs {
@@ -70,29 +68,41 @@ struct PcgArgs {
   const int* diag_pos;  // absolute block index of each row's diagonal
   DevBsr A;
   const float4* b;
-  float4* x;
-  float4* r;
-  float4* z;
-  float4* p0;
+  float4* x;            // solution (and the published x of a residual replacement)
+  float4* z;            // published z (gathered by the fused direction update)
+  float4* p0;           // published p, double-buffered
   float4* p1;
-  float4* q;
-  float4* dinv;         // 3 float4 per row: rows of the inverted diagonal block
-  float* partial;       // [3 * grid]
+  unsigned long long* slots;  // [2 * grid] per-CTA (generation, partial) words
+  unsigned long long* bcast;  // [2] (generation, total) words
+  int* error;           // set when a wait gave up (the kernel returned early)
   PcgState* state;
+  int cap_rows, cap_blocks;   // shared-memory capacity per CTA
   float tol2;           // tolerance^2 on rr / rr0
   int max_iterations;
   int replace_every;    // residual replacement period (0 = never)
   float replace_above2; // only while rr > replace_above^2 rr0
-  long long spin_limit; // clock cycles a grid barrier waits before giving up
+  long long spin_limit; // clock cycles a wait lasts before giving up
+};
+
+// One allocation per context, cleared before every launch: the result, the error flag, the broadcast words,
+// then the per-CTA partial words (2 * grid).
+struct PcgSyncHeader {
+  PcgState state;
+  int error;
+  int pad[3];
+  unsigned long long bcast[2];
 };
 
 struct PcgLaunch {
-  int grid = 0, threads = 256, lanes_per_row = 8;
+  int grid = 0, threads = 1024, lanes_per_row = 8;
+  bool matrix_in_smem = true;
+  size_t smem = 0;
 };
 
 // Cooperative launch of the whole PCG solve; `cfg.grid` <= co-resident CTAs (see pcg_max_grid).
 cudaError_t launch_pcg(const PcgArgs& a, const PcgLaunch& cfg, cudaStream_t s);
-int pcg_max_grid(int threads, int lanes_per_row);
+size_t pcg_smem_bytes(int cap_rows, int cap_blocks, bool matrix_in_smem);
+int pcg_max_grid(int threads, int lanes_per_row, size_t smem, bool matrix_in_smem);
 
 // y = A p (f32 BSR times float4-per-row vector): the stand-alone SpMV of the roofline measurement.
 cudaError_t launch_spmv(int R, const int* row_ptr, const int* col_idx, DevBsr A, const float4* p, float4* y,

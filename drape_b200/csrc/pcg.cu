@@ -1,21 +1,23 @@
 // Block-Jacobi PCG on the f32 BSR(3x3) Newton matrix as ONE persistent cooperative kernel (sm_100a).
 //
-// Each CTA owns a contiguous range of block rows for the whole solve. One iteration is two phases separated by
-// grid barriers:
-//   A  q = A p and p.q, where the direction update p = z + beta p_old is fused into the SpMV's column gathers
-//      (p is double-buffered: the owner writes p for its rows into the other buffer while every CTA forms the
-//      gathered columns from z and the previous buffer, which nobody writes in this phase);
-//   B  alpha = rz / pq, x += alpha p, r -= alpha q, z = D^-1 r, and the partial sums of r.z and r.r.
-// The CTA partials of each dot product are summed by every CTA in the same fixed order, so all CTAs take the
-// same alpha, beta and stop decision, and the solve is deterministic. Residual replacement (r = b - A x every
-// `replace_every` iterations while rr > replace_above^2 rr0, keeping p) follows pcg.rs:213-223.
-// Block rows are processed by groups of `LPR` lanes; a group's lanes stride over the row's blocks and reduce
-// with xor shuffles. Blocks are read as one 16-byte load from each of two planes plus one 4-byte load.
-// Every grid barrier gives up after `spin_limit` cycles, sets `state->error` and the kernel returns (status
-// kPcgTimeout), so a stalled launch cannot hang the GPU.
+// Each CTA owns a contiguous range of block rows for the whole solve and keeps, in shared memory, the rows'
+// BSR blocks and column indices (when they fit), the inverted diagonal blocks and the row vectors x, r, z, p, q
+// and b. Only the vectors other CTAs gather (p and z) are published to global memory (L2). One iteration:
+//   A  q = A p and the partial p.q. The direction update p = z + beta p_old is fused into the column gathers
+//      (every CTA forms the gathered p from the published z and previous p; the owner publishes its new p into
+//      the other of two buffers, which nobody reads in this phase);
+//   B  alpha = rz / pq, x += alpha p, r -= alpha q, z = D^-1 r (all from shared memory), publish z, and the
+//      partials of r.z and r.r.
+// Each phase ends in a reduce-and-broadcast barrier: every CTA publishes its partials as 64-bit words
+// (generation << 32 | float bits); a master warp in CTA 0 waits for all words of the generation, sums them in a
+// fixed order and publishes (generation, total) words that every CTA waits for. No atomics, so every CTA takes
+// the same alpha, beta and stop decision and the solve is deterministic; every wait gives up after `spin_limit`
+// cycles, sets `*error` and the kernel returns, so a stalled launch cannot hang the GPU.
+// Residual replacement (r = b - A x every `replace_every` iterations while rr > replace_above^2 rr0, keeping p)
+// follows pcg.rs:213-223. Block rows are processed by groups of LPR lanes with xor-shuffle reductions; every row
+// loop has a CTA-uniform trip count so all lanes reach the shuffles.
 // Reference semantics: pcg.rs:271-296 (solve), 389-439 (State), 479-492 (invert3); WGSL cg_init, spmv_dot,
 // update_dot, direction, reduce, residual.
-#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include "kernels.h"
@@ -25,85 +27,107 @@ namespace {
 
 __device__ __forceinline__ float4 f4(float a, float b, float c) { return make_float4(a, b, c, 0.0f); }
 __device__ __forceinline__ float dot3(float4 a, float4 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ unsigned long long pack(unsigned gen, float v) {
+  return (static_cast<unsigned long long>(gen) << 32) | __float_as_uint(v);
+}
+__device__ __forceinline__ unsigned long long load_volatile(const unsigned long long* p) {
+  return *reinterpret_cast<const volatile unsigned long long*>(p);
+}
+__device__ __forceinline__ void store_volatile(unsigned long long* p, unsigned long long v) {
+  *reinterpret_cast<volatile unsigned long long*>(p) = v;
+}
 
-// Sense-free generation barrier over all CTAs of the cooperative grid, bounded by `limit` cycles.
-__device__ __forceinline__ bool grid_barrier(PcgState* st, unsigned ctas, long long limit) {
-  __shared__ int ok;
+// CTA sum of NV per-thread floats into out[] (valid in thread 0 after the call).
+template <int NV> __device__ __forceinline__ void cta_sum(float (&v)[NV], float* out) {
+  __shared__ float red[NV][32];
+#pragma unroll
+  for (int k = 0; k < NV; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  if ((threadIdx.x & 31) == 0)
+#pragma unroll
+    for (int k = 0; k < NV; ++k) red[k][threadIdx.x >> 5] = v[k];
   __syncthreads();
+  if (threadIdx.x == 0)
+    for (int k = 0; k < NV; ++k) {
+      float s = 0.0f;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[k][w];
+      out[k] = s;
+    }
+  __syncthreads();
+}
+
+// Publishes this CTA's NV partials for generation `gen` and returns (in vals, all threads) the grid totals.
+template <int NV> __device__ __forceinline__ bool reduce_barrier(const PcgArgs& a, unsigned gen, float* vals) {
+  __shared__ float totals[2];
+  __shared__ int ok;
+  const unsigned G = gridDim.x;
   if (threadIdx.x == 0) {
-    volatile unsigned* gen = &st->barrier_gen;
-    const unsigned g0 = *gen;
-    __threadfence();
-    const unsigned arrived = atomicAdd(&st->barrier_count, 1u);
-    if (arrived == ctas - 1) {
-      atomicExch(&st->barrier_count, 0u);
-      __threadfence();
-      atomicAdd(&st->barrier_gen, 1u);
-    } else {
-      const long long t0 = clock64();
-      while (*gen == g0) {
-        if (clock64() - t0 > limit) {
-          atomicExch(&st->error, 1);
-          break;
+    __threadfence();  // this CTA's published vectors before its partial words
+#pragma unroll
+    for (int k = 0; k < NV; ++k) store_volatile(a.slots + k * G + blockIdx.x, pack(gen, vals[k]));
+  }
+  if (blockIdx.x == 0 && threadIdx.x < 32) {
+    // Master warp: wait for every CTA's word of this generation, sum in a fixed order, broadcast.
+    float sum[NV];
+    bool good = true;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) sum[k] = 0.0f;
+    const long long t0 = clock64();
+    for (unsigned i = threadIdx.x; i < G && good; i += 32)
+#pragma unroll
+      for (int k = 0; k < NV; ++k) {
+        unsigned long long w = load_volatile(a.slots + k * G + i);
+        while (static_cast<unsigned>(w >> 32) != gen) {
+          if (clock64() - t0 > a.spin_limit) {
+            good = false;
+            break;
+          }
+          w = load_volatile(a.slots + k * G + i);
         }
-        __nanosleep(32);
+        sum[k] += __uint_as_float(static_cast<unsigned>(w));
+      }
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) sum[k] += __shfl_xor_sync(0xffffffffu, sum[k], o);
+    good = __all_sync(0xffffffffu, good);
+    if (threadIdx.x == 0) {
+      __threadfence();
+      if (good) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) store_volatile(a.bcast + k, pack(gen, sum[k]));
+      } else {
+        atomicExch(a.error, 1);
       }
     }
-    __threadfence();
-    ok = *(volatile int*)&st->error == 0;
   }
-  __syncthreads();
-  return ok;
-}
-
-// Sum of two per-thread floats over the CTA, written to partial[slot_a * grid + cta], partial[slot_b * ...].
-__device__ __forceinline__ void cta_sum2(float a, float b, float* partial, int slot_a, int slot_b) {
-  __shared__ float ra[32], rb[32];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    a += __shfl_xor_sync(0xffffffffu, a, o);
-    b += __shfl_xor_sync(0xffffffffu, b, o);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    ra[threadIdx.x >> 5] = a;
-    rb[threadIdx.x >> 5] = b;
-  }
-  __syncthreads();
   if (threadIdx.x == 0) {
-    float sa = 0.0f, sb = 0.0f;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-      sa += ra[w];
-      sb += rb[w];
-    }
-    partial[slot_a * gridDim.x + blockIdx.x] = sa;
-    if (slot_b >= 0) partial[slot_b * gridDim.x + blockIdx.x] = sb;
-  }
-}
-
-// The grid-wide sum of one partial slot, computed identically (same order) by every CTA.
-__device__ __forceinline__ float grid_total(const float* partial, int slot) {
-  __shared__ float total;
-  if (threadIdx.x < 32) {
-    float s = 0.0f;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += 32) s += __ldcg(partial + slot * gridDim.x + i);
+    bool good = true;
+    const long long t0 = clock64();
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (threadIdx.x == 0) total = s;
+    for (int k = 0; k < NV && good; ++k) {
+      unsigned long long w = load_volatile(a.bcast + k);
+      while (static_cast<unsigned>(w >> 32) != gen) {
+        if (clock64() - t0 > a.spin_limit || *reinterpret_cast<volatile int*>(a.error)) {
+          good = false;
+          atomicExch(a.error, 1);
+          break;
+        }
+        __nanosleep(16);
+        w = load_volatile(a.bcast + k);
+      }
+      totals[k] = __uint_as_float(static_cast<unsigned>(w));
+    }
+    __threadfence();  // acquire: other CTAs' published vectors after their words
+    ok = good;
   }
   __syncthreads();
-  float t = total;
+#pragma unroll
+  for (int k = 0; k < NV; ++k) vals[k] = totals[k];
+  const bool r = ok;
   __syncthreads();
-  return t;
-}
-
-// Row r of block k applied to v.
-__device__ __forceinline__ void block_apply(const DevBsr& A, int k, float px, float py, float pz, float& y0, float& y1,
-                                            float& y2) {
-  const float4 m0 = __ldg(A.a0 + k), m1 = __ldg(A.a1 + k);
-  const float m8 = __ldg(A.a2 + k);
-  y0 += m0.x * px + m0.y * py + m0.z * pz;
-  y1 += m0.w * px + m1.x * py + m1.y * pz;
-  y2 += m1.z * px + m1.w * py + m8 * pz;
+  return r;
 }
 
 template <int LPR>
@@ -116,21 +140,49 @@ __device__ __forceinline__ void group_reduce(float& y0, float& y1, float& y2) {
   }
 }
 
-template <int LPR>
-__global__ void __launch_bounds__(256) pcg_kernel(PcgArgs a) {
-  const unsigned G = gridDim.x;
-  const int cta = blockIdx.x;
-  const int r_begin = (int)((long long)a.R * cta / G), r_end = (int)((long long)a.R * (cta + 1) / G);
-  const int groups = blockDim.x / LPR, group = threadIdx.x / LPR, gl = threadIdx.x % LPR;
-  PcgState* st = a.state;
+__device__ __forceinline__ void apply(float4 m0, float4 m1, float m8, float4 p, float& y0, float& y1, float& y2) {
+  y0 += m0.x * p.x + m0.y * p.y + m0.z * p.z;
+  y1 += m0.w * p.x + m1.x * p.y + m1.y * p.z;
+  y2 += m1.z * p.x + m1.w * p.y + m8 * p.z;
+}
 
-  // ---- setup: D^-1, x = 0, r = b, z = D^-1 r, p = z; partial r.z, r.r
-  float rz_l = 0.0f, rr_l = 0.0f;
-  for (int row = r_begin + threadIdx.x; row < r_end; row += blockDim.x) {
-    const int k = a.diag_pos[row];
+template <int LPR, bool MSMEM>
+__global__ void __launch_bounds__(1024) pcg_kernel(PcgArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int G = gridDim.x, cta = blockIdx.x;
+  const int r0 = (int)((long long)a.R * cta / G), r1 = (int)((long long)a.R * (cta + 1) / G), n = r1 - r0;
+  const int kb0 = a.row_ptr[r0], nb = a.row_ptr[r1] - kb0;
+  const int groups = blockDim.x / LPR, group = threadIdx.x / LPR, gl = threadIdx.x % LPR;
+  const int cap = a.cap_rows;
+  float4* xs = reinterpret_cast<float4*>(smem);
+  float4* rs = xs + cap;
+  float4* zs = rs + cap;
+  float4* ps = zs + cap;
+  float4* qs = ps + cap;
+  float4* bs = qs + cap;
+  float4* dv = bs + cap;  // 3 per row
+  float4* m0s = dv + 3 * cap;
+  float4* m1s = m0s + (MSMEM ? a.cap_blocks : 0);
+  float* m8s = reinterpret_cast<float*>(m1s + (MSMEM ? a.cap_blocks : 0));
+  int* cols = reinterpret_cast<int*>(m8s + (MSMEM ? a.cap_blocks : 0));
+  int* rp = cols + (MSMEM ? a.cap_blocks : 0);  // n + 1 local row offsets
+
+  // ---- stage the CTA's rows
+  for (int i = threadIdx.x; i <= n; i += blockDim.x) rp[i] = a.row_ptr[r0 + i] - kb0;
+  if (MSMEM)
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+      m0s[k] = a.A.a0[kb0 + k];
+      m1s[k] = a.A.a1[kb0 + k];
+      m8s[k] = a.A.a2[kb0 + k];
+      cols[k] = a.col_idx[kb0 + k];
+    }
+  __syncthreads();
+  // ---- setup: D^-1 (adjugate, pcg.rs:479-492), x = 0, r = b, z = D^-1 r, p = z; partial r.z, r.r
+  float acc[2] = {0.0f, 0.0f};
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int k = a.diag_pos[r0 + i];
     const float4 m0 = a.A.a0[k], m1 = a.A.a1[k];
     const float m8 = a.A.a2[k];
-    // Adjugate inverse in the reference's operation order (pcg.rs:479-492).
     const float A_ = m0.x, B_ = m0.y, C_ = m0.z, D_ = m0.w, E_ = m1.x, F_ = m1.y, G_ = m1.z, H_ = m1.w, I_ = m8;
     const float c00 = E_ * I_ - F_ * H_, c01 = C_ * H_ - B_ * I_, c02 = B_ * F_ - C_ * E_;
     const float c10 = F_ * G_ - D_ * I_, c11 = A_ * I_ - C_ * G_, c12 = C_ * D_ - A_ * F_;
@@ -138,88 +190,97 @@ __global__ void __launch_bounds__(256) pcg_kernel(PcgArgs a) {
     const float det = A_ * c00 + B_ * c10 + C_ * c20;
     const float4 d0 = f4(c00 / det, c01 / det, c02 / det), d1 = f4(c10 / det, c11 / det, c12 / det),
                  d2 = f4(c20 / det, c21 / det, c22 / det);
-    a.dinv[3 * row] = d0;
-    a.dinv[3 * row + 1] = d1;
-    a.dinv[3 * row + 2] = d2;
-    const float4 b = a.b[row];
+    dv[3 * i] = d0;
+    dv[3 * i + 1] = d1;
+    dv[3 * i + 2] = d2;
+    const float4 b = a.b[r0 + i];
     const float4 z = f4(dot3(d0, b), dot3(d1, b), dot3(d2, b));
-    a.x[row] = f4(0.f, 0.f, 0.f);
-    a.r[row] = b;
-    a.z[row] = z;
-    a.p0[row] = z;
-    rz_l += dot3(b, z);
-    rr_l += dot3(b, b);
+    bs[i] = b;
+    xs[i] = f4(0.f, 0.f, 0.f);
+    rs[i] = b;
+    zs[i] = z;
+    ps[i] = z;
+    a.p0[r0 + i] = z;
+    acc[0] += dot3(b, z);
+    acc[1] += dot3(b, b);
   }
-  cta_sum2(rz_l, rr_l, a.partial, 1, 2);
-  if (!grid_barrier(st, G, a.spin_limit)) return;
-  float rz = grid_total(a.partial, 1), rr = grid_total(a.partial, 2);
+  float tot[2];
+  cta_sum<2>(acc, tot);
+  unsigned gen = 1;
+  if (!reduce_barrier<2>(a, gen++, tot)) return;
+  float rz = tot[0], rr = tot[1];
   const float rr0 = rr;
   int status = rr <= 0.0f ? kPcgConverged : kPcgRunning;
   int it = 0, cur = 0, replacements = 0;
   bool fused = false;
   float beta = 0.0f, alpha = 0.0f, pq = 0.0f;
+  const int passes = (n + groups - 1) / groups;
 
   while (status == kPcgRunning) {
     // ---- phase A: p (fused update), q = A p, partial p.q
-    float4* pold = cur ? a.p1 : a.p0;
+    const float4* pold = cur ? a.p1 : a.p0;
     float4* pnew = cur ? a.p0 : a.p1;
-    float pq_l = 0.0f;
-    // Uniform trip count across the CTA: every lane reaches the group shuffles in every pass.
-    for (int row0 = r_begin; row0 < r_end; row0 += groups) {
-      const int row = row0 + group;
-      const bool active = row < r_end;
+    float pq_l[1] = {0.0f};
+    for (int pass = 0; pass < passes; ++pass) {
+      const int i = pass * groups + group;
+      const bool active = i < n;
       float y0 = 0.f, y1 = 0.f, y2 = 0.f;
-      const int kb = active ? a.row_ptr[row] : 0, ke = active ? a.row_ptr[row + 1] : 0;
+      const int kb = active ? rp[i] : 0, ke = active ? rp[i + 1] : 0;
       for (int k = kb + gl; k < ke; k += LPR) {
-        const int c = __ldg(a.col_idx + k);
+        const int c = MSMEM ? cols[k] : __ldg(a.col_idx + kb0 + k);
         float4 pc = __ldcg(pold + c);
         if (fused) {
           const float4 zc = __ldcg(a.z + c);
           pc = f4(zc.x + beta * pc.x, zc.y + beta * pc.y, zc.z + beta * pc.z);
         }
-        block_apply(a.A, k, pc.x, pc.y, pc.z, y0, y1, y2);
+        if (MSMEM)
+          apply(m0s[k], m1s[k], m8s[k], pc, y0, y1, y2);
+        else
+          apply(__ldg(a.A.a0 + kb0 + k), __ldg(a.A.a1 + kb0 + k), __ldg(a.A.a2 + kb0 + k), pc, y0, y1, y2);
       }
       group_reduce<LPR>(y0, y1, y2);
       if (active && gl == 0) {
-        float4 p = pold[row];
+        float4 p = ps[i];
         if (fused) {
-          const float4 z = a.z[row];
+          const float4 z = zs[i];
           p = f4(z.x + beta * p.x, z.y + beta * p.y, z.z + beta * p.z);
-          pnew[row] = p;
+          ps[i] = p;
+          pnew[r0 + i] = p;
         }
         const float4 q = f4(y0, y1, y2);
-        a.q[row] = q;
-        pq_l += dot3(p, q);
+        qs[i] = q;
+        pq_l[0] += dot3(p, q);
       }
     }
-    cta_sum2(pq_l, 0.0f, a.partial, 0, -1);
-    if (!grid_barrier(st, G, a.spin_limit)) return;
-    pq = grid_total(a.partial, 0);
+    float t1[1];
+    cta_sum<1>(pq_l, t1);
+    if (!reduce_barrier<1>(a, gen++, t1)) return;
+    pq = t1[0];
     if (!(pq > 0.0f) || !isfinite(pq)) {
       status = kPcgBreakdown;
       break;
     }
-    const float4* p_it = fused ? pnew : pold;
     if (fused) cur ^= 1;
     alpha = rz / pq;
-    // ---- phase B: x, r, z; partial r.z, r.r
-    rz_l = rr_l = 0.0f;
-    for (int row = r_begin + threadIdx.x; row < r_end; row += blockDim.x) {
-      const float4 p = p_it[row], q = a.q[row];
-      float4 x = a.x[row], r = a.r[row];
+    // ---- phase B: x, r, z in shared memory; publish z; partial r.z, r.r
+    acc[0] = acc[1] = 0.0f;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const float4 p = ps[i], q = qs[i];
+      float4 x = xs[i], r = rs[i];
       x = f4(x.x + alpha * p.x, x.y + alpha * p.y, x.z + alpha * p.z);
       r = f4(r.x - alpha * q.x, r.y - alpha * q.y, r.z - alpha * q.z);
-      const float4 z = f4(dot3(a.dinv[3 * row], r), dot3(a.dinv[3 * row + 1], r), dot3(a.dinv[3 * row + 2], r));
-      a.x[row] = x;
-      a.r[row] = r;
-      a.z[row] = z;
-      rz_l += dot3(r, z);
-      rr_l += dot3(r, r);
+      const float4 z = f4(dot3(dv[3 * i], r), dot3(dv[3 * i + 1], r), dot3(dv[3 * i + 2], r));
+      xs[i] = x;
+      rs[i] = r;
+      zs[i] = z;
+      a.z[r0 + i] = z;
+      acc[0] += dot3(r, z);
+      acc[1] += dot3(r, r);
     }
-    cta_sum2(rz_l, rr_l, a.partial, 1, 2);
-    if (!grid_barrier(st, G, a.spin_limit)) return;
-    const float rz_new = grid_total(a.partial, 1);
-    rr = grid_total(a.partial, 2);
+    cta_sum<2>(acc, tot);
+    if (!reduce_barrier<2>(a, gen++, tot)) return;
+    const float rz_new = tot[0];
+    rr = tot[1];
     beta = rz_new / rz;
     rz = rz_new;
     ++it;
@@ -233,47 +294,56 @@ __global__ void __launch_bounds__(256) pcg_kernel(PcgArgs a) {
       break;
     }
     if (a.replace_every > 0 && it % a.replace_every == 0 && rr > a.replace_above2 * rr0) {
-      // Keep the direction: p = z + beta p_old for the own rows now, then r = b - A x, z = D^-1 r.
-      float4* po = cur ? a.p1 : a.p0;
+      // Keep the direction (p = z + beta p_old, published), publish x, then r = b - A x and z = D^-1 r.
       float4* pn = cur ? a.p0 : a.p1;
-      for (int row = r_begin + threadIdx.x; row < r_end; row += blockDim.x) {
-        const float4 z = a.z[row], p = po[row];
-        pn[row] = f4(z.x + beta * p.x, z.y + beta * p.y, z.z + beta * p.z);
+      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const float4 z = zs[i], p = ps[i];
+        const float4 np = f4(z.x + beta * p.x, z.y + beta * p.y, z.z + beta * p.z);
+        ps[i] = np;
+        pn[r0 + i] = np;
+        a.x[r0 + i] = xs[i];
       }
       cur ^= 1;
       fused = false;
-      // A grid barrier, not just a CTA one: every CTA must have read the phase-B totals of slots 1 and 2
-      // (grid_total above) before any CTA rewrites them below.
-      if (!grid_barrier(st, G, a.spin_limit)) return;
-      rz_l = rr_l = 0.0f;
-      for (int row0 = r_begin; row0 < r_end; row0 += groups) {
-        const int row = row0 + group;
-        const bool active = row < r_end;
+      float none[1] = {0.0f};
+      __syncthreads();
+      if (!reduce_barrier<1>(a, gen++, none)) return;
+      acc[0] = acc[1] = 0.0f;
+      for (int pass = 0; pass < passes; ++pass) {
+        const int i = pass * groups + group;
+        const bool active = i < n;
         float y0 = 0.f, y1 = 0.f, y2 = 0.f;
-        const int kb = active ? a.row_ptr[row] : 0, ke = active ? a.row_ptr[row + 1] : 0;
+        const int kb = active ? rp[i] : 0, ke = active ? rp[i + 1] : 0;
         for (int k = kb + gl; k < ke; k += LPR) {
-          const float4 xc = __ldcg(a.x + __ldg(a.col_idx + k));
-          block_apply(a.A, k, xc.x, xc.y, xc.z, y0, y1, y2);
+          const int c = MSMEM ? cols[k] : __ldg(a.col_idx + kb0 + k);
+          const float4 xc = __ldcg(a.x + c);
+          if (MSMEM)
+            apply(m0s[k], m1s[k], m8s[k], xc, y0, y1, y2);
+          else
+            apply(__ldg(a.A.a0 + kb0 + k), __ldg(a.A.a1 + kb0 + k), __ldg(a.A.a2 + kb0 + k), xc, y0, y1, y2);
         }
         group_reduce<LPR>(y0, y1, y2);
         if (active && gl == 0) {
-          const float4 b = a.b[row];
+          const float4 b = bs[i];
           const float4 r = f4(b.x - y0, b.y - y1, b.z - y2);
-          const float4 z = f4(dot3(a.dinv[3 * row], r), dot3(a.dinv[3 * row + 1], r), dot3(a.dinv[3 * row + 2], r));
-          a.r[row] = r;
-          a.z[row] = z;
-          rz_l += dot3(r, z);
-          rr_l += dot3(r, r);
+          const float4 z = f4(dot3(dv[3 * i], r), dot3(dv[3 * i + 1], r), dot3(dv[3 * i + 2], r));
+          rs[i] = r;
+          zs[i] = z;
+          a.z[r0 + i] = z;
+          acc[0] += dot3(r, z);
+          acc[1] += dot3(r, r);
         }
       }
-      cta_sum2(rz_l, rr_l, a.partial, 1, 2);
-      if (!grid_barrier(st, G, a.spin_limit)) return;
-      rz = grid_total(a.partial, 1);
-      rr = grid_total(a.partial, 2);
+      cta_sum<2>(acc, tot);
+      if (!reduce_barrier<2>(a, gen++, tot)) return;
+      rz = tot[0];
+      rr = tot[1];
       ++replacements;
     }
   }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) a.x[r0 + i] = xs[i];
   if (cta == 0 && threadIdx.x == 0) {
+    PcgState* st = a.state;
     st->rz = rz;
     st->rr = rr;
     st->rr0 = rr0;
@@ -284,6 +354,10 @@ __global__ void __launch_bounds__(256) pcg_kernel(PcgArgs a) {
     st->status = status;
     st->replacements = replacements;
   }
+}
+
+__device__ __forceinline__ void block_apply(const DevBsr& A, int k, float4 p, float& y0, float& y1, float& y2) {
+  apply(__ldg(A.a0 + k), __ldg(A.a1 + k), __ldg(A.a2 + k), p, y0, y1, y2);
 }
 
 template <int LPR>
@@ -297,10 +371,7 @@ __global__ void __launch_bounds__(256) spmv_kernel(int R, const int* __restrict_
     const bool active = row < R;
     float y0 = 0.f, y1 = 0.f, y2 = 0.f;
     const int kb = active ? row_ptr[row] : 0, ke = active ? row_ptr[row + 1] : 0;
-    for (int k = kb + gl; k < ke; k += LPR) {
-      const float4 pc = __ldg(p + __ldg(col_idx + k));
-      block_apply(A, k, pc.x, pc.y, pc.z, y0, y1, y2);
-    }
+    for (int k = kb + gl; k < ke; k += LPR) block_apply(A, k, __ldg(p + __ldg(col_idx + k)), y0, y1, y2);
     group_reduce<LPR>(y0, y1, y2);
     if (active && gl == 0) y[row] = f4(y0, y1, y2);
   }
@@ -308,13 +379,12 @@ __global__ void __launch_bounds__(256) spmv_kernel(int R, const int* __restrict_
 
 // r = b64 - A d computed in f64 from the f32 blocks; one 8-lane group per row.
 __global__ void __launch_bounds__(256) refine_residual_kernel(int R, const int* row_ptr, const int* col_idx, DevBsr A,
-                                                              const double* neg_g, const float4* d, float4* r_out,
+                                                              const double* g, const float4* d, float4* r_out,
                                                               double* partial) {
   __shared__ double red[32];
   const int gl = threadIdx.x & 7;
   double s = 0.0;
   const int groups = blockDim.x >> 3;
-  // Uniform trip count across the grid so every lane reaches the group shuffles.
   for (int row0 = blockIdx.x * groups; row0 < R; row0 += gridDim.x * groups) {
     const int row = row0 + (threadIdx.x >> 3);
     const bool active = row < R;
@@ -335,8 +405,8 @@ __global__ void __launch_bounds__(256) refine_residual_kernel(int R, const int* 
       y2 += __shfl_xor_sync(0xffffffffu, y2, o, 8);
     }
     if (active && gl == 0) {
-      // neg_g holds the f64 gradient g; the right-hand side is -g.
-      const double r0 = -neg_g[3 * row] - y0, r1 = -neg_g[3 * row + 1] - y1, r2 = -neg_g[3 * row + 2] - y2;
+      // g is the f64 gradient; the right-hand side is -g.
+      const double r0 = -g[3 * row] - y0, r1 = -g[3 * row + 1] - y1, r2 = -g[3 * row + 2] - y2;
       r_out[row] = f4(float(r0), float(r1), float(r2));
       s += r0 * r0 + r1 * r1 + r2 * r2;
     }
@@ -360,36 +430,45 @@ __global__ void add_rows_kernel(int R, float4* d, const float4* e) {
   }
 }
 
-template <int LPR> const void* pcg_entry() { return reinterpret_cast<const void*>(&pcg_kernel<LPR>); }
-
-const void* pcg_fn(int lpr) {
-  switch (lpr) {
-    case 4: return pcg_entry<4>();
-    case 8: return pcg_entry<8>();
-    case 16: return pcg_entry<16>();
-    case 32: return pcg_entry<32>();
+const void* pcg_fn(int lpr, bool msmem) {
+  if (msmem) {
+    if (lpr == 4) return reinterpret_cast<const void*>(&pcg_kernel<4, true>);
+    if (lpr == 8) return reinterpret_cast<const void*>(&pcg_kernel<8, true>);
+    if (lpr == 16) return reinterpret_cast<const void*>(&pcg_kernel<16, true>);
+  } else {
+    if (lpr == 4) return reinterpret_cast<const void*>(&pcg_kernel<4, false>);
+    if (lpr == 8) return reinterpret_cast<const void*>(&pcg_kernel<8, false>);
+    if (lpr == 16) return reinterpret_cast<const void*>(&pcg_kernel<16, false>);
   }
   return nullptr;
 }
 
 }  // namespace
 
-int pcg_max_grid(int threads, int lanes_per_row) {
-  const void* fn = pcg_fn(lanes_per_row);
+size_t pcg_smem_bytes(int cap_rows, int cap_blocks, bool msmem) {
+  return size_t(cap_rows) * (6 * 16 + 3 * 16) + (msmem ? size_t(cap_blocks) * (16 + 16 + 4 + 4) : 0) +
+         size_t(cap_rows + 1) * 4;
+}
+
+int pcg_max_grid(int threads, int lanes_per_row, size_t smem, bool msmem) {
+  const void* fn = pcg_fn(lanes_per_row, msmem);
   if (!fn) return 0;
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, 0) != cudaSuccess) return 0;
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess) return 0;
   return sms * per_sm;
 }
 
 cudaError_t launch_pcg(const PcgArgs& a, const PcgLaunch& cfg, cudaStream_t s) {
-  const void* fn = pcg_fn(cfg.lanes_per_row);
-  if (!fn || cfg.threads % 32 != 0 || cfg.threads > 256 || cfg.grid < 1) return cudaErrorInvalidValue;
+  const void* fn = pcg_fn(cfg.lanes_per_row, cfg.matrix_in_smem);
+  if (!fn || cfg.threads % 32 != 0 || cfg.threads > 1024 || cfg.grid < 1) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(cfg.smem));
+  if (e != cudaSuccess) return e;
   PcgArgs args = a;
   void* params[] = {&args};
-  return cudaLaunchCooperativeKernel(fn, dim3(cfg.grid), dim3(cfg.threads), params, 0, s);
+  return cudaLaunchCooperativeKernel(fn, dim3(cfg.grid), dim3(cfg.threads), params, cfg.smem, s);
 }
 
 cudaError_t launch_spmv(int R, const int* row_ptr, const int* col_idx, DevBsr A, const float4* p, float4* y,

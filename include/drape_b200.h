@@ -89,6 +89,8 @@ typedef struct {
   int32_t reason; /* 0 tolerance, 1 step cap, 2 stalled, 3 time budget */
   double final_residual, final_relative_residual, final_h, gravity_load, static_energy, seconds;
   double ms_assembly, ms_pcg, ms_line_search, ms_ccd, ms_other;
+  int32_t pcg_launches; /* persistent PCG kernel launches (one per linear solve) */
+  int32_t pcg_grid;     /* CTAs of each PCG launch */
 } drape_run_log;
 
 /* One accepted PTC step (gpu-ptc.bin columns, run-e7.ts:96). */
