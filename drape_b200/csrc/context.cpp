@@ -227,7 +227,7 @@ void Context::configure_pcg() {
   check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_), "attribute");
   const int groups = c.threads / c.lanes_per_row;
   int grid = opt_.pcg_grid > 0 ? opt_.pcg_grid : std::min(sms, (R + groups - 1) / groups);
-  grid = std::max(1, std::min(grid, R));
+  grid = std::max(1, std::min({grid, R, c.threads}));  // the master CTA polls one partial word per thread
   for (;;) {
     int cap_rows = 0, cap_blocks = 0;
     for (int b = 0; b < grid; ++b) {

@@ -67,38 +67,46 @@ template <int NV> __device__ __forceinline__ bool reduce_barrier(const PcgArgs& 
 #pragma unroll
     for (int k = 0; k < NV; ++k) store_volatile(a.slots + k * G + blockIdx.x, pack(gen, vals[k]));
   }
-  if (blockIdx.x == 0 && threadIdx.x < 32) {
-    // Master warp: wait for every CTA's word of this generation, sum in a fixed order, broadcast.
-    float sum[NV];
-    bool good = true;
-#pragma unroll
-    for (int k = 0; k < NV; ++k) sum[k] = 0.0f;
-    const long long t0 = clock64();
-    for (unsigned i = threadIdx.x; i < G && good; i += 32)
+  if (blockIdx.x == 0) {
+    // Master CTA: thread t waits for CTA t's words of this generation (all words polled in parallel), then
+    // warp 0 sums them in a fixed order and broadcasts the totals. blockDim.x >= gridDim.x (host-checked).
+    __shared__ float words[NV][1024];
+    __shared__ int good_all;
+    if (threadIdx.x == 0) good_all = 1;
+    __syncthreads();
+    if (threadIdx.x < G) {
+      const long long t0 = clock64();
 #pragma unroll
       for (int k = 0; k < NV; ++k) {
-        unsigned long long w = load_volatile(a.slots + k * G + i);
+        unsigned long long w = load_volatile(a.slots + k * G + threadIdx.x);
         while (static_cast<unsigned>(w >> 32) != gen) {
           if (clock64() - t0 > a.spin_limit) {
-            good = false;
+            good_all = 0;
             break;
           }
-          w = load_volatile(a.slots + k * G + i);
+          w = load_volatile(a.slots + k * G + threadIdx.x);
         }
-        sum[k] += __uint_as_float(static_cast<unsigned>(w));
+        words[k][threadIdx.x] = __uint_as_float(static_cast<unsigned>(w));
       }
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      float sum[NV];
 #pragma unroll
-    for (int k = 0; k < NV; ++k)
+      for (int k = 0; k < NV; ++k) {
+        sum[k] = 0.0f;
+        for (unsigned i = threadIdx.x; i < G; i += 32) sum[k] += words[k][i];
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) sum[k] += __shfl_xor_sync(0xffffffffu, sum[k], o);
-    good = __all_sync(0xffffffffu, good);
-    if (threadIdx.x == 0) {
-      __threadfence();
-      if (good) {
+        for (int o = 16; o > 0; o >>= 1) sum[k] += __shfl_xor_sync(0xffffffffu, sum[k], o);
+      }
+      if (threadIdx.x == 0) {
+        __threadfence();
+        if (good_all) {
 #pragma unroll
-        for (int k = 0; k < NV; ++k) store_volatile(a.bcast + k, pack(gen, sum[k]));
-      } else {
-        atomicExch(a.error, 1);
+          for (int k = 0; k < NV; ++k) store_volatile(a.bcast + k, pack(gen, sum[k]));
+        } else {
+          atomicExch(a.error, 1);
+        }
       }
     }
   }
