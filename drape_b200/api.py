@@ -108,6 +108,7 @@ def load():
     lib.drape_static_energy.argtypes = [P, P, P]
     lib.drape_time_spmv.argtypes = [P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, P]
     lib.drape_time_assembly.argtypes = [P, ctypes.c_int32, P]
+    lib.drape_pcg_profile.argtypes = [P, P, ctypes.c_int32]
     lib.drape_create.argtypes = [ctypes.POINTER(ProblemView), ctypes.POINTER(Options), ctypes.c_int32, ctypes.POINTER(P)]
     lib.drape_write_sheet_problem.argtypes = [ctypes.c_int32, ctypes.c_uint64, ctypes.c_double, ctypes.c_double,
                                               ctypes.c_int32, ctypes.c_char_p]
@@ -297,6 +298,13 @@ class Drape:
         ms = ctypes.c_float()
         self._check(self.lib.drape_time_spmv(self.h, launches, lanes_per_row, threads, ctypes.byref(ms)))
         return ms.value
+
+    def pcg_profile(self, clear=False):
+        """CTA 0's SM cycles per PCG phase: phase A, sum A, barrier A, phase B, sum B, barrier B, iterations."""
+        out = np.zeros(7, np.int64)
+        self._check(self.lib.drape_pcg_profile(self.h, _ptr(out), int(clear)))
+        keys = ["phase_a", "sum_a", "barrier_a", "phase_b", "sum_b", "barrier_b", "iterations"]
+        return dict(zip(keys, out.tolist()))
 
     def time_assembly(self, launches=50):
         ms = ctypes.c_float()

@@ -329,4 +329,14 @@ drape_status drape_time_assembly(drape_ctx* ctx, int32_t launches, float* ms) {
   });
 }
 
+drape_status drape_pcg_profile(drape_ctx* ctx, int64_t* out, int32_t clear) {
+  return guarded(ctx, [&](drape::Context& c) {
+    if (!out) return fail(ctx, "out is null", DRAPE_E_ARG);
+    long long t[8];
+    c.pcg_profile(t, clear != 0);
+    for (int k = 0; k < 7; ++k) out[k] = t[k];
+    return DRAPE_OK;
+  });
+}
+
 }  // extern "C"

@@ -249,6 +249,8 @@ void Context::configure_pcg() {
   }
   pcg_cfg_ = c;
   pcg_sync_.alloc((sizeof(PcgSyncHeader) + 16 * size_t(c.grid) + 7) / 8);
+  pcg_timing_.alloc(8);
+  check(cudaMemsetAsync(pcg_timing_.ptr, 0, 8 * sizeof(long long), stream_), "memset");
 }
 
 void Context::sync() { check(cudaStreamSynchronize(stream_), "stream synchronize"); }
@@ -315,6 +317,7 @@ PcgResult Context::pcg(double rtol, int max_iterations) {
   a.replace_every = opt_.replace_every;
   a.replace_above2 = float(opt_.replace_above * opt_.replace_above);
   a.spin_limit = 4000000000LL;  // ~2 s of SM clock per wait
+  a.timing = pcg_timing_.ptr;
   check(cudaMemsetAsync(pcg_sync_.ptr, 0, pcg_sync_.n * sizeof(unsigned long long), stream_), "memset");
   check(cudaEventRecord(ev_[0], stream_), "event");
   check(launch_pcg(a, pcg_cfg_, stream_), "pcg launch");

@@ -110,10 +110,18 @@ class Context {
   PcgLaunch pcg_cfg_;
   int pcg_caps_[2] = {0, 0};
   long long pcg_launches_ = 0;
+  DeviceArray<long long> pcg_timing_;
 
  public:
   const PcgLaunch& pcg_launch() const { return pcg_cfg_; }
   long long pcg_launches() const { return pcg_launches_; }
+  // CTA 0's accumulated cycles per PCG phase since the last reset (see PcgArgs::timing); reset when `clear`.
+  void pcg_profile(long long* out8, bool clear) {
+    pcg_timing_.download(out8, 8, stream_);
+    if (clear) check_reset_timing();
+    cudaStreamSynchronize(stream_);
+  }
+  void check_reset_timing() { cudaMemsetAsync(pcg_timing_.ptr, 0, 8 * sizeof(long long), stream_); }
 
  private:
   void configure_pcg();

@@ -82,6 +82,8 @@ struct PcgArgs {
   int replace_every;    // residual replacement period (0 = never)
   float replace_above2; // only while rr > replace_above^2 rr0
   long long spin_limit; // clock cycles a wait lasts before giving up
+  long long* timing;    // optional [8]: CTA 0's cycles in phase A, its CTA sum, barrier A, phase B, CTA sum,
+                        // barrier B, iterations (null: not recorded)
 };
 
 // One allocation per context, cleared before every launch: the result, the error flag, the broadcast words,

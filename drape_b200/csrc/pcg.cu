@@ -223,9 +223,11 @@ __global__ void __launch_bounds__(1024) pcg_kernel(PcgArgs a) {
   bool fused = false;
   float beta = 0.0f, alpha = 0.0f, pq = 0.0f;
   const int passes = (n + groups - 1) / groups;
+  long long tm[7] = {0, 0, 0, 0, 0, 0, 0};
 
   while (status == kPcgRunning) {
     // ---- phase A: p (fused update), q = A p, partial p.q
+    long long t_a0 = clock64();
     const float4* pold = cur ? a.p1 : a.p0;
     float4* pnew = cur ? a.p0 : a.p1;
     float pq_l[1] = {0.0f};
@@ -261,8 +263,11 @@ __global__ void __launch_bounds__(1024) pcg_kernel(PcgArgs a) {
       }
     }
     float t1[1];
+    const long long t_a1 = clock64();
     cta_sum<1>(pq_l, t1);
+    const long long t_a2 = clock64();
     if (!reduce_barrier<1>(a, gen++, t1)) return;
+    const long long t_a3 = clock64();
     pq = t1[0];
     if (!(pq > 0.0f) || !isfinite(pq)) {
       status = kPcgBreakdown;
@@ -285,8 +290,20 @@ __global__ void __launch_bounds__(1024) pcg_kernel(PcgArgs a) {
       acc[0] += dot3(r, z);
       acc[1] += dot3(r, r);
     }
+    const long long t_b1 = clock64();
     cta_sum<2>(acc, tot);
+    const long long t_b2 = clock64();
     if (!reduce_barrier<2>(a, gen++, tot)) return;
+    if (a.timing && cta == 0 && threadIdx.x == 0) {
+      const long long t_b3 = clock64();
+      tm[0] += t_a1 - t_a0;
+      tm[1] += t_a2 - t_a1;
+      tm[2] += t_a3 - t_a2;
+      tm[3] += t_b1 - t_a3;
+      tm[4] += t_b2 - t_b1;
+      tm[5] += t_b3 - t_b2;
+      tm[6] += 1;
+    }
     const float rz_new = tot[0];
     rr = tot[1];
     beta = rz_new / rz;
@@ -350,6 +367,8 @@ __global__ void __launch_bounds__(1024) pcg_kernel(PcgArgs a) {
     }
   }
   for (int i = threadIdx.x; i < n; i += blockDim.x) a.x[r0 + i] = xs[i];
+  if (a.timing && cta == 0 && threadIdx.x == 0)
+    for (int k = 0; k < 7; ++k) a.timing[k] += tm[k];
   if (cta == 0 && threadIdx.x == 0) {
     PcgState* st = a.state;
     st->rz = rz;

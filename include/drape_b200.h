@@ -174,6 +174,10 @@ drape_status drape_static_energy(drape_ctx* ctx, const double* x, double* out);
  * assembled matrix (lanes per row 4/8/16/32) and of the row assembly at the current state. */
 drape_status drape_time_spmv(drape_ctx* ctx, int32_t launches, int32_t lanes_per_row, int32_t threads, float* ms);
 drape_status drape_time_assembly(drape_ctx* ctx, int32_t launches, float* ms);
+/* SM-clock cycles CTA 0 of the PCG kernel spent per phase since the last clear: [phase A (p, q = A p),
+ * its CTA sum, its grid reduction, phase B (x, r, z), its CTA sum, its grid reduction, iterations]; clear != 0
+ * zeroes the counters. */
+drape_status drape_pcg_profile(drape_ctx* ctx, int64_t* out7, int32_t clear);
 
 #ifdef __cplusplus
 }
