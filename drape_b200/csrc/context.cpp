@@ -674,3 +674,12 @@ float Context::time_assembly(int launches) {
 }
 
 }  // namespace drape
+
+namespace drape {
+template struct DeviceArray<double>;
+template struct DeviceArray<int>;
+template struct DeviceArray<float>;
+template struct DeviceArray<float4>;
+template struct DeviceArray<long long>;
+template struct DeviceArray<unsigned long long>;
+}  // namespace drape
