@@ -248,7 +248,7 @@ void Context::configure_pcg() {
     grid = fit;
   }
   pcg_cfg_ = c;
-  pcg_sync_.alloc((sizeof(PcgSyncHeader) + 16 * size_t(c.grid) + 7) / 8);
+  pcg_sync_.alloc((sizeof(PcgSyncHeader) + 32 * size_t(c.grid) + 7) / 8);  // 2 parities x 2 words x grid
   pcg_timing_.alloc(8);
   check(cudaMemsetAsync(pcg_timing_.ptr, 0, 8 * sizeof(long long), stream_), "memset");
 }

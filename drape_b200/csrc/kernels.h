@@ -72,8 +72,8 @@ struct PcgArgs {
   float4* z;            // published z (gathered by the fused direction update)
   float4* p0;           // published p, double-buffered
   float4* p1;
-  unsigned long long* slots;  // [2 * grid] per-CTA (generation, partial) words
-  unsigned long long* bcast;  // [2] (generation, total) words
+  unsigned long long* slots;  // [2 parities][2 values][grid] per-CTA (generation, partial) words
+  unsigned long long* bcast;  // unused (kept for the layout of PcgSyncHeader)
   int* error;           // set when a wait gave up (the kernel returned early)
   PcgState* state;
   int cap_rows, cap_blocks;   // shared-memory capacity per CTA

@@ -57,85 +57,64 @@ template <int NV> __device__ __forceinline__ void cta_sum(float (&v)[NV], float*
   __syncthreads();
 }
 
+__device__ __forceinline__ void store_release(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long load_acquire(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
 // Publishes this CTA's NV partials for generation `gen` and returns (in vals, all threads) the grid totals.
+// All-to-all: thread 0 release-stores the CTA's (gen, partial) words after a CTA barrier (so they order every
+// thread's earlier stores of published vectors); thread t of every CTA acquire-polls CTA t's words (all words in
+// parallel, blockDim.x >= gridDim.x, host-checked); every CTA then sums the words in the same fixed order.
+// Words alternate between two buffers by generation parity: a CTA can only rewrite a buffer after every CTA has
+// published the next generation, i.e. after every CTA has read this one.
 template <int NV> __device__ __forceinline__ bool reduce_barrier(const PcgArgs& a, unsigned gen, float* vals) {
+  __shared__ float words[NV][1024];
   __shared__ float totals[2];
-  __shared__ int ok;
+  __shared__ int bad;
   const unsigned G = gridDim.x;
+  unsigned long long* slots = a.slots + (gen & 1u) * 2u * G;
   if (threadIdx.x == 0) {
-    __threadfence();  // this CTA's published vectors before its partial words
+    bad = 0;
 #pragma unroll
-    for (int k = 0; k < NV; ++k) store_volatile(a.slots + k * G + blockIdx.x, pack(gen, vals[k]));
+    for (int k = 0; k < NV; ++k) store_release(slots + k * G + blockIdx.x, pack(gen, vals[k]));
   }
-  if (blockIdx.x == 0) {
-    // Master CTA: thread t waits for CTA t's words of this generation (all words polled in parallel), then
-    // warp 0 sums them in a fixed order and broadcasts the totals. blockDim.x >= gridDim.x (host-checked).
-    __shared__ float words[NV][1024];
-    __shared__ int good_all;
-    if (threadIdx.x == 0) good_all = 1;
-    __syncthreads();
-    if (threadIdx.x < G) {
-      const long long t0 = clock64();
-#pragma unroll
-      for (int k = 0; k < NV; ++k) {
-        unsigned long long w = load_volatile(a.slots + k * G + threadIdx.x);
-        while (static_cast<unsigned>(w >> 32) != gen) {
-          if (clock64() - t0 > a.spin_limit) {
-            good_all = 0;
-            break;
-          }
-          w = load_volatile(a.slots + k * G + threadIdx.x);
-        }
-        words[k][threadIdx.x] = __uint_as_float(static_cast<unsigned>(w));
-      }
-    }
-    __syncthreads();
-    if (threadIdx.x < 32) {
-      float sum[NV];
-#pragma unroll
-      for (int k = 0; k < NV; ++k) {
-        sum[k] = 0.0f;
-        for (unsigned i = threadIdx.x; i < G; i += 32) sum[k] += words[k][i];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) sum[k] += __shfl_xor_sync(0xffffffffu, sum[k], o);
-      }
-      if (threadIdx.x == 0) {
-        __threadfence();
-        if (good_all) {
-#pragma unroll
-          for (int k = 0; k < NV; ++k) store_volatile(a.bcast + k, pack(gen, sum[k]));
-        } else {
-          atomicExch(a.error, 1);
-        }
-      }
-    }
-  }
-  if (threadIdx.x == 0) {
-    bool good = true;
+  __syncthreads();
+  if (threadIdx.x < G) {
     const long long t0 = clock64();
 #pragma unroll
-    for (int k = 0; k < NV && good; ++k) {
-      unsigned long long w = load_volatile(a.bcast + k);
+    for (int k = 0; k < NV; ++k) {
+      unsigned long long w = load_acquire(slots + k * G + threadIdx.x);
       while (static_cast<unsigned>(w >> 32) != gen) {
-        if (clock64() - t0 > a.spin_limit || *reinterpret_cast<volatile int*>(a.error)) {
-          good = false;
-          atomicExch(a.error, 1);
+        if (clock64() - t0 > a.spin_limit) {
+          bad = 1;
           break;
         }
-        __nanosleep(16);
-        w = load_volatile(a.bcast + k);
+        w = load_acquire(slots + k * G + threadIdx.x);
       }
-      totals[k] = __uint_as_float(static_cast<unsigned>(w));
+      words[k][threadIdx.x] = __uint_as_float(static_cast<unsigned>(w));
     }
-    __threadfence();  // acquire: other CTAs' published vectors after their words
-    ok = good;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      float s = 0.0f;
+      for (unsigned i = threadIdx.x; i < G; i += 32) s += words[k][i];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (threadIdx.x == 0) totals[k] = s;
+    }
+    if (threadIdx.x == 0 && bad) atomicExch(a.error, 1);
   }
   __syncthreads();
 #pragma unroll
   for (int k = 0; k < NV; ++k) vals[k] = totals[k];
-  const bool r = ok;
-  __syncthreads();
-  return r;
+  return !bad;
 }
 
 template <int LPR>
