@@ -48,13 +48,16 @@ template <int NV> __device__ __forceinline__ void cta_sum(float (&v)[NV], float*
 #pragma unroll
     for (int k = 0; k < NV; ++k) red[k][threadIdx.x >> 5] = v[k];
   __syncthreads();
-  if (threadIdx.x == 0)
+  if (threadIdx.x < 32) {
+    const int warps = blockDim.x >> 5;
+#pragma unroll
     for (int k = 0; k < NV; ++k) {
-      float s = 0.0f;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[k][w];
-      out[k] = s;
+      float s = threadIdx.x < warps ? red[k][threadIdx.x] : 0.0f;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (threadIdx.x == 0) out[k] = s;
     }
-  __syncthreads();
+  }
 }
 
 __device__ __forceinline__ void store_release(unsigned long long* p, unsigned long long v) {
@@ -215,7 +218,32 @@ __global__ void __launch_bounds__(1024) pcg_kernel(PcgArgs a) {
       const bool active = i < n;
       float y0 = 0.f, y1 = 0.f, y2 = 0.f;
       const int kb = active ? rp[i] : 0, ke = active ? rp[i + 1] : 0;
-      for (int k = kb + gl; k < ke; k += LPR) {
+      // The lane's first two blocks: both column gathers are issued before either is used (one L2 round trip).
+      const int k0 = kb + gl, k1 = k0 + LPR;
+      const int c0 = k0 < ke ? (MSMEM ? cols[k0] : __ldg(a.col_idx + kb0 + k0)) : -1;
+      const int c1 = k1 < ke ? (MSMEM ? cols[k1] : __ldg(a.col_idx + kb0 + k1)) : -1;
+      float4 p0c = make_float4(0.f, 0.f, 0.f, 0.f), p1c = p0c, z0c = p0c, z1c = p0c;
+      if (c0 >= 0) p0c = __ldcg(pold + c0);
+      if (c1 >= 0) p1c = __ldcg(pold + c1);
+      if (fused && c0 >= 0) z0c = __ldcg(a.z + c0);
+      if (fused && c1 >= 0) z1c = __ldcg(a.z + c1);
+      if (fused) {
+        p0c = f4(z0c.x + beta * p0c.x, z0c.y + beta * p0c.y, z0c.z + beta * p0c.z);
+        p1c = f4(z1c.x + beta * p1c.x, z1c.y + beta * p1c.y, z1c.z + beta * p1c.z);
+      }
+      if (c0 >= 0) {
+        if (MSMEM)
+          apply(m0s[k0], m1s[k0], m8s[k0], p0c, y0, y1, y2);
+        else
+          apply(__ldg(a.A.a0 + kb0 + k0), __ldg(a.A.a1 + kb0 + k0), __ldg(a.A.a2 + kb0 + k0), p0c, y0, y1, y2);
+      }
+      if (c1 >= 0) {
+        if (MSMEM)
+          apply(m0s[k1], m1s[k1], m8s[k1], p1c, y0, y1, y2);
+        else
+          apply(__ldg(a.A.a0 + kb0 + k1), __ldg(a.A.a1 + kb0 + k1), __ldg(a.A.a2 + kb0 + k1), p1c, y0, y1, y2);
+      }
+      for (int k = k1 + LPR; k < ke; k += LPR) {
         const int c = MSMEM ? cols[k] : __ldg(a.col_idx + kb0 + k);
         float4 pc = __ldcg(pold + c);
         if (fused) {
