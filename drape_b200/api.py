@@ -49,7 +49,8 @@ class RunLog(ctypes.Structure):
         ("final_h", ctypes.c_double), ("gravity_load", ctypes.c_double), ("static_energy", ctypes.c_double),
         ("seconds", ctypes.c_double), ("ms_assembly", ctypes.c_double), ("ms_pcg", ctypes.c_double),
         ("ms_line_search", ctypes.c_double), ("ms_ccd", ctypes.c_double), ("ms_other", ctypes.c_double),
-        ("pcg_launches", ctypes.c_int32), ("pcg_grid", ctypes.c_int32),
+        ("pcg_launches", ctypes.c_int32), ("pcg_grid", ctypes.c_int32), ("device_seconds", ctypes.c_double),
+        ("kernel_launches", ctypes.c_int32), ("pad", ctypes.c_int32),
     ]
 
     def as_dict(self):

@@ -262,7 +262,7 @@ double Context::read_scalar(int slot) {
 }
 
 double Context::reduce_partials(int n, int op, int slot) {
-  check(launch_reduce(partial_.ptr, n, op, scalars_.ptr, slot, stream_), "reduce");
+  kcheck(launch_reduce(partial_.ptr, n, op, scalars_.ptr, slot, stream_), "reduce");
   return read_scalar(slot);
 }
 
@@ -289,7 +289,7 @@ double Context::assemble(const double* x, double inv_h2, double mu, int mode, bo
   a.grad = g_.ptr;
   a.bsr = hessian ? DevBsr{a0_.ptr, a1_.ptr, a2_.ptr} : DevBsr{nullptr, nullptr, nullptr};
   a.partial = partial_.ptr;
-  check(launch_assemble(a, stream_), "assemble");
+  kcheck(launch_assemble(a, stream_), "assemble");
   return std::sqrt(reduce_partials(assemble_grid(host_.R), 0, kNorm));
 }
 
@@ -320,7 +320,7 @@ PcgResult Context::pcg(double rtol, int max_iterations) {
   a.timing = pcg_timing_.ptr;
   check(cudaMemsetAsync(pcg_sync_.ptr, 0, pcg_sync_.n * sizeof(unsigned long long), stream_), "memset");
   check(cudaEventRecord(ev_[0], stream_), "event");
-  check(launch_pcg(a, pcg_cfg_, stream_), "pcg launch");
+  kcheck(launch_pcg(a, pcg_cfg_, stream_), "pcg launch");
   check(cudaEventRecord(ev_[1], stream_), "event");
   check(cudaMemcpyAsync(pinned_state_, pcg_sync_.ptr, sizeof(PcgSyncHeader), cudaMemcpyDeviceToHost, stream_), "read");
   sync();
@@ -338,20 +338,20 @@ PcgResult Context::pcg(double rtol, int max_iterations) {
 }
 
 double Context::max_step(const double* x, const double* d) {
-  check(launch_max_step(dp_, x, d, partial_.ptr, kReduceGrid, stream_), "max_step");
+  kcheck(launch_max_step(dp_, x, d, partial_.ptr, kReduceGrid, stream_), "max_step");
   return reduce_partials(kReduceGrid, 1, kAlpha);
 }
 
 double Context::energy_change(const double* x, const double* d, double alpha, double inv_h2, int mode) {
   EnergyArgs a{dp_, x, xhat_.ptr, d, alpha, inv_h2, mode, partial_.ptr};
-  check(launch_energy_change(a, kReduceGrid, stream_), "energy_change");
+  kcheck(launch_energy_change(a, kReduceGrid, stream_), "energy_change");
   return reduce_partials(kReduceGrid, 0, kDelta);
 }
 
 double Context::static_residual() { return assemble(x_.ptr, 0.0, 0.0, 1, false); }
 
 double Context::static_energy() {
-  check(launch_static_energy(dp_, x_.ptr, partial_.ptr, kReduceGrid, stream_), "static_energy");
+  kcheck(launch_static_energy(dp_, x_.ptr, partial_.ptr, kReduceGrid, stream_), "static_energy");
   return reduce_partials(kReduceGrid, 0, kEnergy);
 }
 
@@ -366,12 +366,12 @@ AttemptResult Context::attempt(double h, double scale) {
     phase_ms_[phase] += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return out;
   };
-  check(launch_predict(dp_, xn_.ptr, h * h, xhat_.ptr, stream_), "predict");
+  kcheck(launch_predict(dp_, xn_.ptr, h * h, xhat_.ptr, stream_), "predict");
   if (opt_.newton_start == 1) {
     // The reference's start: x_n + alpha_max (x_hat - x_n).
-    check(launch_sub(int(nv), xhat_.ptr, xn_.ptr, towards_.ptr, stream_), "towards");
+    kcheck(launch_sub(int(nv), xhat_.ptr, xn_.ptr, towards_.ptr, stream_), "towards");
     double a0 = t_phase(kCcd, [&] { return max_step(xn_.ptr, towards_.ptr); });
-    check(launch_axpy(int(nv), xn_.ptr, a0, towards_.ptr, x_.ptr, stream_), "start");
+    kcheck(launch_axpy(int(nv), xn_.ptr, a0, towards_.ptr, x_.ptr, stream_), "start");
   } else {
     check(cudaMemcpyAsync(x_.ptr, xn_.ptr, nv * sizeof(double), cudaMemcpyDeviceToDevice, stream_), "start");
   }
@@ -396,22 +396,22 @@ AttemptResult Context::attempt(double h, double scale) {
     double slope = 0.0;
     for (;;) {
       res.max_mu = std::max(res.max_mu, mu);
-      check(launch_rhs(host_.R, g_.ptr, b_.ptr, stream_), "rhs");
+      kcheck(launch_rhs(host_.R, g_.ptr, b_.ptr, stream_), "rhs");
       PcgResult pr = pcg(eta, opt_.pcg_max_iterations);
       res.pcg_iterations += pr.iterations;
       check(cudaMemcpyAsync(sol_.ptr, px_.ptr, sizeof(float4) * host_.R, cudaMemcpyDeviceToDevice, stream_), "copy");
       if (opt_.refine && pr.status != kPcgBreakdown) {
-        check(launch_refine_residual(host_.R, row_ptr_.ptr, col_idx_.ptr, DevBsr{a0_.ptr, a1_.ptr, a2_.ptr}, g_.ptr,
+        kcheck(launch_refine_residual(host_.R, row_ptr_.ptr, col_idx_.ptr, DevBsr{a0_.ptr, a1_.ptr, a2_.ptr}, g_.ptr,
                                      sol_.ptr, b_.ptr, partial_.ptr, kReduceGrid, stream_),
               "refine");
         PcgResult pc = pcg(opt_.refine_rtol, opt_.pcg_max_iterations);
         res.pcg_iterations += pc.iterations;
-        if (pc.status != kPcgBreakdown) check(launch_add_rows(host_.R, sol_.ptr, px_.ptr, stream_), "add");
+        if (pc.status != kPcgBreakdown) kcheck(launch_add_rows(host_.R, sol_.ptr, px_.ptr, stream_), "add");
       }
       if (host_.R < host_.V)  // fixed vertices keep a zero direction
         check(cudaMemsetAsync(d_.ptr, 0, nv * sizeof(double), stream_), "memset");
-      check(launch_scatter_direction(dp_, sol_.ptr, d_.ptr, stream_), "scatter");
-      check(launch_slope(dp_, g_.ptr, d_.ptr, partial_.ptr, kReduceGrid, stream_), "slope");
+      kcheck(launch_scatter_direction(dp_, sol_.ptr, d_.ptr, stream_), "scatter");
+      kcheck(launch_slope(dp_, g_.ptr, d_.ptr, partial_.ptr, kReduceGrid, stream_), "slope");
       slope = reduce_partials(kReduceGrid, 0, kSlope);
       bool failed = pr.status == kPcgBreakdown || !(slope < 0.0);
       if (!failed) break;
@@ -442,7 +442,7 @@ AttemptResult Context::attempt(double h, double scale) {
       res.status = 2;
       return res;
     }
-    check(launch_axpy(int(nv), x_.ptr, alpha, d_.ptr, x_.ptr, stream_), "advance");
+    kcheck(launch_axpy(int(nv), x_.ptr, alpha, d_.ptr, x_.ptr, stream_), "advance");
     res.updates++;
     res.halvings += halvings;
     mu = halvings == 0 ? relax_mu(mu) : mu;
@@ -457,7 +457,9 @@ int Context::solve_equilibrium(const double* start, double h0, drape_run_log* lo
   const double h_floor = opt_.h0 * opt_.h_min_factor;
   std::memset(phase_ms_, 0, sizeof phase_ms_);
   pcg_launches_ = 0;
+  kernels_ = 0;
   steps_.clear();
+  check(cudaEventRecord(ev_[4], stream_), "event");
   drape_run_log out{};
   out.gravity_load = L;
   auto t_start = std::chrono::steady_clock::now();
@@ -518,7 +520,7 @@ int Context::solve_equilibrium(const double* start, double h0, drape_run_log* lo
     rec.inner = res.updates;
     rec.rejected = rejected;
     rec.pcg_iterations = res.pcg_iterations;
-    check(launch_min_distance(dp_, x_.ptr, partial_.ptr, kReduceGrid, stream_), "min_distance");
+    kcheck(launch_min_distance(dp_, x_.ptr, partial_.ptr, kReduceGrid, stream_), "min_distance");
     rec.min_distance = reduce_partials(kReduceGrid, 1, kMinDist);
     steps_.push_back(rec);
     out.newton_iterations += res.updates;
@@ -545,6 +547,12 @@ int Context::solve_equilibrium(const double* start, double h0, drape_run_log* lo
   out.ms_other = out.seconds * 1e3 - out.ms_assembly - out.ms_pcg - out.ms_line_search - out.ms_ccd;
   out.pcg_launches = int(pcg_launches_);
   out.pcg_grid = pcg_cfg_.grid;
+  check(cudaEventRecord(ev_[5], stream_), "event");
+  sync();
+  float dev_ms = 0.0f;
+  check(cudaEventElapsedTime(&dev_ms, ev_[4], ev_[5]), "event time");
+  out.device_seconds = dev_ms / 1e3;
+  out.kernel_launches = int(kernels_);
   if (log) *log = out;
   return reason;
 }
@@ -633,17 +641,17 @@ double Context::max_step_host(const double* x, const double* d) {
 
 double Context::static_energy_host(const double* x) {
   xt_.upload(x, 3 * size_t(host_.V), stream_);
-  check(launch_static_energy(dp_, xt_.ptr, partial_.ptr, kReduceGrid, stream_), "static_energy");
+  kcheck(launch_static_energy(dp_, xt_.ptr, partial_.ptr, kReduceGrid, stream_), "static_energy");
   return reduce_partials(kReduceGrid, 0, kEnergy);
 }
 
 float Context::time_spmv(int launches, int lanes_per_row, int threads) {
   DevBsr A{a0_.ptr, a1_.ptr, a2_.ptr};
   for (int i = 0; i < 3; ++i)
-    check(launch_spmv(host_.R, row_ptr_.ptr, col_idx_.ptr, A, pp0_.ptr, pq_.ptr, lanes_per_row, threads, stream_), "spmv");
+    kcheck(launch_spmv(host_.R, row_ptr_.ptr, col_idx_.ptr, A, pp0_.ptr, pq_.ptr, lanes_per_row, threads, stream_), "spmv");
   check(cudaEventRecord(ev_[2], stream_), "event");
   for (int i = 0; i < launches; ++i)
-    check(launch_spmv(host_.R, row_ptr_.ptr, col_idx_.ptr, A, pp0_.ptr, pq_.ptr, lanes_per_row, threads, stream_), "spmv");
+    kcheck(launch_spmv(host_.R, row_ptr_.ptr, col_idx_.ptr, A, pp0_.ptr, pq_.ptr, lanes_per_row, threads, stream_), "spmv");
   check(cudaEventRecord(ev_[3], stream_), "event");
   sync();
   float ms = 0;
@@ -663,9 +671,9 @@ float Context::time_assembly(int launches) {
   a.grad = g_.ptr;
   a.bsr = DevBsr{a0_.ptr, a1_.ptr, a2_.ptr};
   a.partial = partial_.ptr;
-  for (int i = 0; i < 3; ++i) check(launch_assemble(a, stream_), "assemble");
+  for (int i = 0; i < 3; ++i) kcheck(launch_assemble(a, stream_), "assemble");
   check(cudaEventRecord(ev_[2], stream_), "event");
-  for (int i = 0; i < launches; ++i) check(launch_assemble(a, stream_), "assemble");
+  for (int i = 0; i < launches; ++i) kcheck(launch_assemble(a, stream_), "assemble");
   check(cudaEventRecord(ev_[3], stream_), "event");
   sync();
   float ms = 0;

@@ -21,6 +21,8 @@ struct CudaError : std::runtime_error {
       : std::runtime_error(where + ": " + cudaGetErrorString(c)), code(c) {}
 };
 
+void check(cudaError_t e, const char* where);
+
 template <class T> struct DeviceArray {
   T* ptr = nullptr;
   size_t n = 0;
@@ -125,6 +127,12 @@ class Context {
 
  private:
   void configure_pcg();
+  // check() for a kernel launcher, counting the launch.
+  void kcheck(cudaError_t e, const char* where) {
+    check(e, where);
+    ++kernels_;
+  }
+  long long kernels_ = 0;
 
   // static problem arrays
   DeviceArray<double> geom_, hinge_k_, unit_mass_, colliders_;

@@ -91,6 +91,9 @@ typedef struct {
   double ms_assembly, ms_pcg, ms_line_search, ms_ccd, ms_other;
   int32_t pcg_launches; /* persistent PCG kernel launches (one per linear solve) */
   int32_t pcg_grid;     /* CTAs of each PCG launch */
+  double device_seconds; /* CUDA events on the context's stream around the whole solve */
+  int32_t kernel_launches; /* kernels the solve launched (all of this library's own) */
+  int32_t pad;
 } drape_run_log;
 
 /* One accepted PTC step (gpu-ptc.bin columns, run-e7.ts:96). */
