@@ -162,13 +162,12 @@ def run_gpu(args):
     clocks = clock.summary()
     t = sum(secs) / len(secs)
     t_e2e = sum(e2e) / len(e2e)
-    drape = api.Drape.from_arrays(**host, options=opts, device=local)
     if dist:
         v = torch.tensor([t, t_e2e], device=f"cuda:{local}")
         dist.all_reduce(v, op=dist.ReduceOp.MAX)
         t, t_e2e = v.tolist()
     last = logs[-1]
-    R, B = drape.R, drape.B
+    R, B = int(meta["rows"]), int(meta["blocks"])
     bytes_per_iter = 40 * B + 196 * R
     pk = peaks()
     achieved = (bytes_per_iter * last["pcg_iterations"]) / (last["ms_pcg"] / 1e3) / 1e9 if last["ms_pcg"] > 0 else 0.0
