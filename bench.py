@@ -176,7 +176,9 @@ def run_gpu(args):
     if os.path.exists(tpath):
         tr = json.load(open(tpath))
         if tr.get("columns") == args.n:
-            traffic = tr["dram_bytes_per_iteration"] * last["pcg_iterations"] / max(1, last["pcg_launches"])
+            # One launch stages the matrix into shared memory once: its DRAM traffic is per launch, not per
+            # iteration (ncu capture summarised in profiles/pcg_kernel_n129.md).
+            traffic = tr["dram_bytes_per_launch"]
     out = {
         "metric": METRIC, "value": t, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -196,7 +198,9 @@ def run_gpu(args):
         "roofline": {"bound": "hbm", "kernel": "pcg_kernel (persistent block-Jacobi PCG)", "achieved": achieved,
                      "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
                      "traffic": traffic, "peak_source": "fallback" if pk.get("_fallback") else "measured",
-                     "algorithmic_bytes_per_pcg_iteration": bytes_per_iter},
+                     "algorithmic_bytes_per_pcg_iteration": bytes_per_iter,
+                     "algorithmic_bytes_per_launch": bytes_per_iter * last["pcg_iterations"] / max(1, last["pcg_launches"]),
+                     "avg_launch_ms": last["ms_pcg"] / max(1, last["pcg_launches"])},
         "clocks": clocks,
     }
     if rank == 0 and not args.no_cpu_baseline:
