@@ -53,6 +53,10 @@ drape_status create(const drape::HostProblem& p, const drape_options* options, i
 
 }  // namespace
 
+namespace drape {
+void set_global_error(const std::string& message) { g_create_error = message; }
+}  // namespace drape
+
 extern "C" {
 
 const char* drape_version(void) { return "drape_b200 0.1 (sm_100a)"; }

@@ -182,6 +182,25 @@ drape_status drape_time_assembly(drape_ctx* ctx, int32_t launches, float* ms);
  * zeroes the counters. */
 drape_status drape_pcg_profile(drape_ctx* ctx, int64_t* out7, int32_t clear);
 
+/* Block-Jacobi PCG that allocates nothing, for callers that cannot call cudaMalloc: applications whose device
+ * memory all comes from their own pool, or that must not enter the driver's allocator once they are running.
+ * This entry point has no counterpart in the reference; it is the persistent PCG of drape_pcg with its work space
+ * (search directions, diagonal index, grid-reduction words) in one fixed device array of about 3.4 MB that the
+ * library holds on every GPU that loads it, until exit. Limit: 1 to DRAPE_NOALLOC_MAX_ROWS block rows.
+ * All pointers are device memory on the current device, owned by the caller:
+ *   row_ptr [rows+1], col_idx [B]   BSR(3x3) pattern, every row with its diagonal block
+ *   a0, a1 [4B] and a2 [B]          blocks as the assembly writes them: a0 = (m00,m01,m02,m10),
+ *                                   a1 = (m11,m12,m20,m21), a2 = m22 (a0, a1 16-byte aligned)
+ *   rhs, x [4 * rows]               one 16-byte row each (x, y, z, unused); x receives the solution from 0
+ * info = [iterations, status (1 converged, 2 iteration limit, 3 breakdown)], relative = sqrt(rr/rr0) (host).
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress) and should come before
+ * any stream capture. Calls share the one array and run on `stream` (NULL: the default stream) and return after
+ * synchronizing it; calls that overlap on the GPU (other host threads, other streams) race on the array. */
+#define DRAPE_NOALLOC_MAX_ROWS 65536
+drape_status drape_pcg_noalloc(int32_t rows, const int32_t* row_ptr, const int32_t* col_idx, const float* a0,
+                               const float* a1, const float* a2, const float* rhs, float* x, double rtol,
+                               int32_t max_iterations, void* stream, int32_t* info, double* relative);
+
 #ifdef __cplusplus
 }
 #endif
