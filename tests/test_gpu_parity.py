@@ -131,14 +131,16 @@ def _polished_error(oracle, x_g):
 
 @pytest.mark.parametrize("n", [17, 33])
 def test_sheet_solve_reaches_an_f64_equilibrium(n):
-    """Sheet over sphere + plane, PTC from h0 = 1e-3 s to |grad E_s| <= 1e-6 N: the GPU's converged state is
-    within 1e-4 m of the f64 oracle's equilibrium and satisfies the oracle's f64 residual test."""
-    gpu = api.Drape.sheet(n, seed=0, plane=True, options=api.default_options())
+    """Sheet over sphere + plane, PTC from h0 = 1e-3 s: the GPU's converged state is within 1e-4 m of the f64
+    oracle's equilibrium and satisfies the oracle's f64 residual test. The solve stops at |grad E_s| <= 1e-7 N,
+    not the scene's 1e-6 N: the sheet's sliding modes on the frictionless floor are so soft that a 1e-6 N state
+    of the n33 sheet lies ~3e-4 m from the exact equilibrium of its basin, whichever solver produced it."""
+    gpu = api.Drape.sheet(n, seed=0, plane=True, options=api.default_options(equilibrium_absolute=1e-7))
     log = gpu.solve_equilibrium()
-    assert log["reason"] == "tolerance" and log["final_residual"] <= 1e-6, log
+    assert log["reason"] == "tolerance" and log["final_residual"] <= 1e-7, log
     oracle = oracle_py.Scene("sheet", n, seed=0, plane=True)
     err, e_rel, r64 = _polished_error(oracle, gpu.state)
-    assert r64 <= 1.01e-6, r64
+    assert r64 <= 1.01e-7, r64
     assert err <= 1e-4, err
     assert e_rel <= 1e-9, e_rel
 
