@@ -95,6 +95,10 @@ def flush_l2(torch, device):
     del buf
 
 
+PRECOND = {"jacobi": "block-Jacobi PCG", "multilevel": "multilevel V-cycle flexible PCG (omega-Jacobi smoothing)",
+           "learned": "multilevel V-cycle flexible PCG with the network-predicted fine smoother"}
+
+
 def run_gpu(args):
     import numpy as np
     import torch
@@ -112,7 +116,8 @@ def run_gpu(args):
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    opts = api.default_options(pcg_max_iterations=args.pcg_max, max_steps=args.max_steps)
+    precond = {"jacobi": 0, "multilevel": 1, "learned": 2}[args.preconditioner]
+    opts = api.default_options(pcg_max_iterations=args.pcg_max, max_steps=args.max_steps, preconditioner=precond)
     # Host arrays for the end-to-end leg (built outside every timed region).
     pdir = tempfile.mkdtemp(prefix="drape_bench_")
     api.write_sheet_problem(pdir, args.n, seed=args.seed, plane=bool(args.plane))
@@ -183,15 +188,16 @@ def run_gpu(args):
         "metric": METRIC, "value": t, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": f"sheet n{args.n} over sphere r=0.25 + ground plane y=-0.25, block-Jacobi PCG, "
+        "config": {"workload": f"sheet n{args.n} over sphere r=0.25 + ground plane y=-0.25, {PRECOND[args.preconditioner]}, "
                                f"PTC dt0=1e-3 s to |grad E_s|<=1e-6 N", "columns": args.n, "rows": R, "blocks": B,
-                   "seed": args.seed, "preconditioner": "block-jacobi", "parallelism": f"replicas{world}",
+                   "seed": args.seed, "preconditioner": args.preconditioner, "parallelism": f"replicas{world}",
                    "l2": "flushed (512 MiB write) before every timed solve"},
         "solve": {"converged": last["reason"] == "tolerance", "reason": last["reason"],
                   "final_residual_N": last["final_residual"], "ptc_steps": last["ptc_steps"],
                   "newton_iterations": last["newton_iterations"], "pcg_iterations": last["pcg_iterations"],
                   "pcg_per_newton": last["pcg_iterations"] / max(1, last["newton_iterations"]),
                   "rejected_attempts": last["rejected_attempts"], "static_energy_J": last["static_energy"],
+                  "fallbacks_to_jacobi": last["fallbacks"], "mg_levels": last["mg_levels"],
                   "phase_ms": {k: last[k] for k in ("ms_assembly", "ms_pcg", "ms_line_search", "ms_ccd", "ms_other")}},
         "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(sum(l["kernel_launches"] for l in logs)),
@@ -279,6 +285,7 @@ def main():
     ap.add_argument("--max-steps", type=int, default=1000)
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--preconditioner", default="jacobi", choices=["jacobi", "multilevel", "learned"])
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -37,7 +37,7 @@ class Options(ctypes.Structure):
         ("curvature", ctypes.c_int32), ("preconditioner", ctypes.c_int32), ("armijo", ctypes.c_double),
         ("max_halvings", ctypes.c_int32), ("time_budget_s", ctypes.c_double), ("pcg_grid", ctypes.c_int32),
         ("pcg_threads", ctypes.c_int32), ("pcg_lanes", ctypes.c_int32), ("progress", ctypes.c_int32),
-        ("newton_start", ctypes.c_int32), ("tangent", ctypes.c_int32),
+        ("newton_start", ctypes.c_int32), ("tangent", ctypes.c_int32), ("smoother_omega", ctypes.c_double),
     ]
 
 
@@ -50,7 +50,8 @@ class RunLog(ctypes.Structure):
         ("seconds", ctypes.c_double), ("ms_assembly", ctypes.c_double), ("ms_pcg", ctypes.c_double),
         ("ms_line_search", ctypes.c_double), ("ms_ccd", ctypes.c_double), ("ms_other", ctypes.c_double),
         ("pcg_launches", ctypes.c_int32), ("pcg_grid", ctypes.c_int32), ("device_seconds", ctypes.c_double),
-        ("kernel_launches", ctypes.c_int32), ("pad", ctypes.c_int32),
+        ("kernel_launches", ctypes.c_int32), ("fallbacks", ctypes.c_int32), ("mg_levels", ctypes.c_int32),
+        ("pad", ctypes.c_int32),
     ]
 
     def as_dict(self):
@@ -103,6 +104,8 @@ def load():
     lib.drape_step_records.argtypes = [P, P, ctypes.c_int32, P]
     lib.drape_assemble.argtypes = [P, P, P, ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_int32, P, P]
     lib.drape_pcg.argtypes = [P, P, P, ctypes.c_double, ctypes.c_int32, P, P, P]
+    lib.drape_precondition.argtypes = [P, P, P, P]
+    lib.drape_multilevel_view.argtypes = [P, ctypes.c_int32, P, P, P]
     lib.drape_energy_change.argtypes = [P, P, P, ctypes.c_double, P, ctypes.c_double, ctypes.c_int32, P]
     lib.drape_max_step.argtypes = [P, P, P, P]
     lib.drape_static_residual.argtypes = [P, P, P]
@@ -273,6 +276,23 @@ class Drape:
                                        ctypes.byref(rel)))
         return sol, {"iterations": int(info[0]), "status": PCG_STATUS.get(int(info[1]), int(info[1])),
                      "replacements": int(info[2]), "relative": rel.value}
+
+    def precondition(self, r, blocks=None):
+        """One multilevel V-cycle z = M r (the preconditioner of options.preconditioner 1 and 2)."""
+        z = np.zeros(3 * self.R)
+        blk = None if blocks is None else np.ascontiguousarray(blocks, np.float32)
+        self._check(self.lib.drape_precondition(self.h, _ptr(blk), _ptr(_f64(r)), _ptr(z)))
+        return z
+
+    def multilevel_view(self, level, operator=True):
+        """(columns, f64 stencil [225][rows] or None, f32 smoother [9][rows]) of one hierarchy level."""
+        cols = ctypes.c_int32()
+        self._check(self.lib.drape_multilevel_view(self.h, level, ctypes.byref(cols), None, None))
+        n = cols.value
+        op = np.zeros((225, n * n)) if operator and level > 0 else None
+        sm = np.zeros((9, n * n), np.float32)
+        self._check(self.lib.drape_multilevel_view(self.h, level, ctypes.byref(cols), _ptr(op), _ptr(sm)))
+        return n, op, sm
 
     def energy_change(self, x, d, alpha, x_hat=None, h=0.0, mode=0):
         out = ctypes.c_double()

@@ -217,6 +217,9 @@ drape_status drape_sizes(const drape_ctx* ctx, int64_t* out) {
 drape_status drape_set_options(drape_ctx* ctx, const drape_options* options) {
   return guarded(ctx, [&](drape::Context& c) {
     if (!options) return fail(ctx, "options is null", DRAPE_E_ARG);
+    if (options->preconditioner != 0 && c.mg_levels() == 0)
+      return fail(ctx, "the multilevel preconditioner needs every vertex free on an n x n grid with n - 1 even",
+                  DRAPE_E_ARG);
     c.options() = *options;
     return DRAPE_OK;
   });
@@ -279,6 +282,25 @@ drape_status drape_pcg(drape_ctx* ctx, const float* blocks, const double* rhs, d
       info[2] = r.replacements;
     }
     if (relative) *relative = r.relative;
+    return DRAPE_OK;
+  });
+}
+
+drape_status drape_precondition(drape_ctx* ctx, const float* blocks, const double* r, double* z) {
+  return guarded(ctx, [&](drape::Context& c) {
+    if (!r || !z) return fail(ctx, "invalid arguments", DRAPE_E_ARG);
+    if (c.mg_levels() == 0) return fail(ctx, "no multilevel hierarchy for this problem", DRAPE_E_ARG);
+    c.precondition_host(blocks, r, z);
+    return DRAPE_OK;
+  });
+}
+
+drape_status drape_multilevel_view(drape_ctx* ctx, int32_t level, int32_t* columns, double* op, float* smoother) {
+  return guarded(ctx, [&](drape::Context& c) {
+    if (!columns) return fail(ctx, "columns is null", DRAPE_E_ARG);
+    const int n = c.multilevel_view(level, op, smoother);
+    if (n < 0) return fail(ctx, "no such multilevel level", DRAPE_E_ARG);
+    *columns = n;
     return DRAPE_OK;
   });
 }

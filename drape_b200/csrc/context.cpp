@@ -54,15 +54,36 @@ double next_forcing(double previous, double ratio) {
 
 }  // namespace
 
+// Levels of the multilevel hierarchy the problem allows: every vertex a row in vertex order on an n x n grid,
+// couplings within 2 vertices per axis (coarse operators are then 5 x 5 stencils), partial sums within capacity.
+int structured_levels(const HostProblem& p) {
+  const int n = p.columns;
+  // the power method's partial sums cover the row CTAs of every smoothed level (< R / 24 in all)
+  if (n <= 0 || p.R != p.V || n * n != p.V || (p.R + 23) / 24 > kMgPartials) return 0;
+  for (int r = 0; r < p.R; ++r)
+    if (p.row_vertex[r] != r) return 0;
+  for (int r = 0; r < p.R; ++r)
+    for (int k = p.row_ptr[r]; k < p.row_ptr[r + 1]; ++k) {
+      const int c = p.col_idx[k];
+      if (std::abs(c % n - r % n) > 2 || std::abs(c / n - r / n) > 2) return 0;
+    }
+  const int levels = mg_level_count(n);
+  return levels >= 2 ? levels : 0;
+}
+
 Context::Context(const HostProblem& problem, const drape_options& options, int device)
     : host_(problem), opt_(options), device_(device) {
   std::string err = validate(host_);
   if (!err.empty()) throw std::invalid_argument("inconsistent problem: " + err);
+  mg_levels_ = structured_levels(host_);
+  if (opt_.preconditioner != 0 && mg_levels_ == 0)
+    throw std::invalid_argument("the multilevel preconditioner needs every vertex free on an n x n grid with n - 1 even");
   check(cudaSetDevice(device_), "cudaSetDevice");
   check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
   for (auto& e : ev_) check(cudaEventCreate(&e), "cudaEventCreate");
   check(cudaMallocHost(&pinned_, kSlots * sizeof(double)), "cudaMallocHost");
   check(cudaMallocHost(&pinned_state_, sizeof(PcgSyncHeader)), "cudaMallocHost");
+  check(cudaMallocHost(&pinned_mg_, sizeof(MgState) + 16), "cudaMallocHost");
   upload_problem();
 }
 
@@ -72,6 +93,8 @@ Context::~Context() {
     if (e) cudaEventDestroy(e);
   if (pinned_) cudaFreeHost(pinned_);
   if (pinned_state_) cudaFreeHost(pinned_state_);
+  if (pinned_mg_) cudaFreeHost(pinned_mg_);
+  if (mg_graph_) cudaGraphExecDestroy(mg_graph_);
   if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -211,6 +234,7 @@ void Context::upload_problem() {
   gravity_load_ = std::sqrt(s);
 
   configure_pcg();
+  configure_mg();
   sync();
 }
 
@@ -289,6 +313,7 @@ double Context::assemble(const double* x, double inv_h2, double mu, int mode, bo
   a.grad = g_.ptr;
   a.bsr = hessian ? DevBsr{a0_.ptr, a1_.ptr, a2_.ptr} : DevBsr{nullptr, nullptr, nullptr};
   a.partial = partial_.ptr;
+  if (hessian) mg_stale_ = true;
   kcheck(launch_assemble(a, stream_), "assemble");
   return std::sqrt(reduce_partials(assemble_grid(host_.R), 0, kNorm));
 }
@@ -397,14 +422,14 @@ AttemptResult Context::attempt(double h, double scale) {
     for (;;) {
       res.max_mu = std::max(res.max_mu, mu);
       kcheck(launch_rhs(host_.R, g_.ptr, b_.ptr, stream_), "rhs");
-      PcgResult pr = pcg(eta, opt_.pcg_max_iterations);
+      PcgResult pr = direction_solve(eta, opt_.pcg_max_iterations);
       res.pcg_iterations += pr.iterations;
       check(cudaMemcpyAsync(sol_.ptr, px_.ptr, sizeof(float4) * host_.R, cudaMemcpyDeviceToDevice, stream_), "copy");
       if (opt_.refine && pr.status != kPcgBreakdown) {
         kcheck(launch_refine_residual(host_.R, row_ptr_.ptr, col_idx_.ptr, DevBsr{a0_.ptr, a1_.ptr, a2_.ptr}, g_.ptr,
                                      sol_.ptr, b_.ptr, partial_.ptr, kReduceGrid, stream_),
               "refine");
-        PcgResult pc = pcg(opt_.refine_rtol, opt_.pcg_max_iterations);
+        PcgResult pc = direction_solve(opt_.refine_rtol, opt_.pcg_max_iterations);
         res.pcg_iterations += pc.iterations;
         if (pc.status != kPcgBreakdown) kcheck(launch_add_rows(host_.R, sol_.ptr, px_.ptr, stream_), "add");
       }
@@ -458,6 +483,9 @@ int Context::solve_equilibrium(const double* start, double h0, drape_run_log* lo
   std::memset(phase_ms_, 0, sizeof phase_ms_);
   pcg_launches_ = 0;
   kernels_ = 0;
+  fallbacks_ = 0;
+  std::memset(mg_outcome_, 0, sizeof mg_outcome_);
+  mg_iterations_ = 0;
   steps_.clear();
   check(cudaEventRecord(ev_[4], stream_), "event");
   drape_run_log out{};
@@ -553,6 +581,14 @@ int Context::solve_equilibrium(const double* start, double h0, drape_run_log* lo
   check(cudaEventElapsedTime(&dev_ms, ev_[4], ev_[5]), "event time");
   out.device_seconds = dev_ms / 1e3;
   out.kernel_launches = int(kernels_);
+  out.fallbacks = fallbacks_;
+  out.mg_levels = opt_.preconditioner != 0 ? mg_levels_ : 0;
+  if (opt_.progress && out.mg_levels)
+    std::fprintf(stderr,
+                 "multilevel: %lld iterations; solves converged %lld, limit %lld, breakdown %lld, stalled %lld, "
+                 "coarse pivot %lld; block-Jacobi fallback converged %lld, limit %lld, breakdown %lld\n",
+                 mg_iterations_, mg_outcome_[0], mg_outcome_[1], mg_outcome_[2], mg_outcome_[3], mg_outcome_[4],
+                 mg_outcome_[5], mg_outcome_[6], mg_outcome_[7]);
   if (log) *log = out;
   return reason;
 }
@@ -592,26 +628,31 @@ double Context::assemble_host(const double* x, const double* x_hat, double h, do
   return norm;
 }
 
-PcgResult Context::pcg_host(const float* blocks, const double* rhs, double rtol, int max_iterations, double* solution) {
-  const int R = host_.R, B = host_.B;
-  if (blocks) {
-    std::vector<float4> h0(B), h1(B);
-    std::vector<float> h2(B);
-    for (int k = 0; k < B; ++k) {
-      const float* v = blocks + 9 * size_t(k);
-      h0[k] = make_float4(v[0], v[1], v[2], v[3]);
-      h1[k] = make_float4(v[4], v[5], v[6], v[7]);
-      h2[k] = v[8];
-    }
-    a0_.upload(h0.data(), B, stream_);
-    a1_.upload(h1.data(), B, stream_);
-    a2_.upload(h2.data(), B, stream_);
+void Context::upload_blocks(const float* blocks) {
+  const int B = host_.B;
+  std::vector<float4> h0(B), h1(B);
+  std::vector<float> h2(B);
+  for (int k = 0; k < B; ++k) {
+    const float* v = blocks + 9 * size_t(k);
+    h0[k] = make_float4(v[0], v[1], v[2], v[3]);
+    h1[k] = make_float4(v[4], v[5], v[6], v[7]);
+    h2[k] = v[8];
   }
+  a0_.upload(h0.data(), B, stream_);
+  a1_.upload(h1.data(), B, stream_);
+  a2_.upload(h2.data(), B, stream_);
+  mg_stale_ = true;
+  sync();
+}
+
+PcgResult Context::pcg_host(const float* blocks, const double* rhs, double rtol, int max_iterations, double* solution) {
+  const int R = host_.R;
+  if (blocks) upload_blocks(blocks);
   std::vector<float4> b(R);
   for (int r = 0; r < R; ++r)
     b[r] = make_float4(float(rhs[3 * r]), float(rhs[3 * r + 1]), float(rhs[3 * r + 2]), 0.0f);
   b_.upload(b.data(), R, stream_);
-  PcgResult res = pcg(rtol, max_iterations);
+  PcgResult res = direction_solve(rtol, max_iterations);
   std::vector<float4> x(R);
   px_.download(x.data(), R, stream_);
   sync();
@@ -684,6 +725,174 @@ float Context::time_assembly(int launches) {
 }  // namespace drape
 
 namespace drape {
+// ------------------------------------------------------------------------------------ multilevel preconditioner
+
+namespace {
+constexpr int kMgStallWindow = 128; // block Jacobi takes over when |r| fell by < 10% over this many iterations
+}  // namespace
+
+// Hierarchy storage, pointers and the solve graph (the pointers never change).
+void Context::configure_mg() {
+  if (mg_levels_ == 0) return;
+  const int L = mg_levels_, R = host_.R;
+  int n[kMgMaxLevels], rows[kMgMaxLevels];
+  n[0] = host_.columns;
+  rows[0] = R;
+  size_t a_count = 0, s_count = 9 * size_t(R), v_count = 7 * size_t(R);
+  for (int l = 1; l < L; ++l) {
+    n[l] = (n[l - 1] - 1) / 2 + 1;
+    rows[l] = n[l] * n[l];
+    a_count += size_t(kMgStencil) * 9 * rows[l];
+    s_count += 9 * size_t(rows[l]);
+    v_count += 3 * size_t(rows[l]);
+  }
+  mg_a64_.alloc(a_count);
+  mg_a_.alloc(a_count);
+  mg_s_.alloc(s_count);
+  mg_vec_.alloc(v_count);
+  check(cudaMemsetAsync(mg_vec_.ptr, 0, v_count * sizeof(float4), stream_), "memset");
+  check(cudaMemsetAsync(mg_s_.ptr, 0, s_count * sizeof(float), stream_), "memset");
+  const int m = 3 * rows[L - 1];
+  mg_inv_.alloc(size_t(m) * m);
+  mg_partial_.alloc(4 * size_t(kMgPartials));
+  check(cudaMemsetAsync(mg_partial_.ptr, 0, mg_partial_.n * sizeof(float), stream_), "memset");
+  mg_state_.alloc((sizeof(MgState) + sizeof(float) - 1) / sizeof(float));
+  mg_error_.alloc(1);
+
+  MgDevice d{};
+  d.fine = MgFine{R, n[0], row_ptr_.ptr, col_idx_.ptr, diag_pos_.ptr, DevBsr{a0_.ptr, a1_.ptr, a2_.ptr}};
+  d.levels = L;
+  double* a64 = mg_a64_.ptr;
+  float* a32 = mg_a_.ptr;
+  float* sm = mg_s_.ptr;
+  float4* v = mg_vec_.ptr;
+  for (int l = 0; l < L; ++l) {
+    MgLevel& lv = d.lv[l];
+    lv.n = n[l];
+    lv.rows = rows[l];
+    lv.S = sm;
+    sm += 9 * size_t(rows[l]);
+    if (l > 0) {
+      lv.A64 = a64;
+      lv.A = a32;
+      a64 += size_t(kMgStencil) * 9 * rows[l];
+      a32 += size_t(kMgStencil) * 9 * rows[l];
+      lv.r = v;
+      v += rows[l];
+    }
+    lv.z = v;
+    v += rows[l];
+    lv.e = v;
+    v += rows[l];
+  }
+  d.r[0] = v;
+  d.r[1] = v + R;
+  d.p[0] = v + 2 * size_t(R);
+  d.p[1] = v + 3 * size_t(R);
+  d.q = v + 4 * size_t(R);
+  d.b = b_.ptr;
+  d.x = px_.ptr;
+  d.coarse_inv = mg_inv_.ptr;
+  mg_omega_.alloc(kMgMaxLevels);
+  d.omega = mg_omega_.ptr;
+  d.partial = mg_partial_.ptr;
+  d.state = reinterpret_cast<MgState*>(mg_state_.ptr);
+  d.error = mg_error_.ptr;
+  mg_ = d;
+
+  sync();
+  check(mg_build_solve_graph(mg_, stream_, &mg_graph_, &mg_graph_launches_), "multilevel solve graph");
+  mg_stale_ = true;
+}
+
+// Set-up for the matrix now in the BSR planes: smoothers, Galerkin products, coarsest inverse.
+void Context::mg_prepare() {
+  if (!mg_stale_) return;
+  check(cudaMemsetAsync(mg_error_.ptr, 0, sizeof(int), stream_), "memset");
+  const float omega = opt_.smoother_omega > 0 ? float(opt_.smoother_omega) : 0.0f;  // 0: spectral damping
+  kcheck(mg_setup(mg_, omega, true, stream_), "multilevel set-up");
+  // fine smoother, Galerkin products, coarse smoothers, coarsest inverse; the power method and its scaling
+  kernels_ += 2 * (mg_levels_ - 1) + (omega > 0 ? 0 : kMgPowerSteps + mg_levels_ - 1);
+  mg_stale_ = false;
+}
+
+PcgResult Context::mg_pcg(double rtol, int max_iterations, bool* stalled) {
+  *stalled = false;
+  mg_prepare();
+  check(cudaEventRecord(ev_[0], stream_), "event");
+  kcheck(mg_pcg_init(mg_, float(rtol * rtol), max_iterations, kMgStallWindow, stream_), "multilevel init");
+  // The whole loop runs on the device (a conditional WHILE node); one read-back at the end.
+  check(cudaGraphLaunch(mg_graph_, stream_), "graph launch");
+  check(cudaMemcpyAsync(pinned_mg_, mg_.state, sizeof(MgState), cudaMemcpyDeviceToHost, stream_), "read");
+  check(cudaMemcpyAsync(pinned_mg_ + 1, mg_.error, sizeof(int), cudaMemcpyDeviceToHost, stream_), "read");
+  check(cudaEventRecord(ev_[1], stream_), "event");
+  sync();
+  const MgState& st = *pinned_mg_;
+  const bool coarse_error = *reinterpret_cast<const int*>(pinned_mg_ + 1) != 0;
+  *stalled = coarse_error || st.status == 4;
+  // body executions: one per two iterations, plus the one that found the end
+  kernels_ += (long long)(st.iterations / 2 + 1) * mg_graph_launches_;
+  PcgResult r;
+  cudaEventElapsedTime(&r.ms, ev_[0], ev_[1]);
+  phase_ms_[kPcg] += r.ms;
+  pcg_launches_++;
+  r.iterations = st.iterations;
+  // device status 1 converged, 2 iteration limit, 3 breakdown, 4 stalled (reported as the limit)
+  r.status = st.status == 1 ? kPcgConverged : st.status == 3 ? kPcgBreakdown : kPcgIterationLimit;
+  r.relative = st.rr0 > 0 ? std::sqrt(double(st.rr) / double(st.rr0)) : 0.0;
+  return r;
+}
+
+PcgResult Context::direction_solve(double rtol, int max_iterations) {
+  if (opt_.preconditioner == 0 || mg_levels_ == 0) return pcg(rtol, max_iterations);
+  bool stalled = false;
+  PcgResult r = mg_pcg(rtol, max_iterations, &stalled);
+  mg_iterations_ += r.iterations;
+  const bool coarse_failed = stalled && *reinterpret_cast<const int*>(pinned_mg_ + 1);
+  mg_outcome_[coarse_failed ? 4 : stalled ? 3 : r.status == kPcgConverged ? 0 : r.status == kPcgBreakdown ? 2 : 1]++;
+  // A breakdown is the Newton's signal to raise mu (as with block Jacobi); only a stalled residual or a failed
+  // coarse factorisation hands the system to block-Jacobi PCG.
+  if (!stalled) return r;
+  ++fallbacks_;
+  PcgResult j = pcg(rtol, max_iterations);
+  mg_outcome_[j.status == kPcgConverged ? 5 : j.status == kPcgBreakdown ? 7 : 6]++;
+  j.iterations += r.iterations;
+  j.ms += r.ms;
+  return j;
+}
+
+void Context::precondition_host(const float* blocks, const double* rhs, double* z) {
+  if (mg_levels_ == 0) throw std::invalid_argument("no multilevel hierarchy for this problem");
+  const int R = host_.R;
+  if (blocks) upload_blocks(blocks);
+  mg_prepare();
+  std::vector<float4> r(R);
+  for (int i = 0; i < R; ++i) r[i] = make_float4(float(rhs[3 * i]), float(rhs[3 * i + 1]), float(rhs[3 * i + 2]), 0.f);
+  check(cudaMemcpyAsync(mg_.r[0], r.data(), R * sizeof(float4), cudaMemcpyHostToDevice, stream_), "upload");
+  kcheck(mg_apply(mg_, stream_), "V-cycle");
+  check(cudaMemcpyAsync(r.data(), mg_.lv[0].e, R * sizeof(float4), cudaMemcpyDeviceToHost, stream_), "download");
+  sync();
+  for (int i = 0; i < R; ++i) {
+    z[3 * i] = r[i].x;
+    z[3 * i + 1] = r[i].y;
+    z[3 * i + 2] = r[i].z;
+  }
+}
+
+int Context::multilevel_view(int level, double* op, float* smoother) {
+  if (level < 0 || level >= mg_levels_) return -1;
+  mg_prepare();
+  const MgLevel& lv = mg_.lv[level];
+  if (op && level > 0)
+    check(cudaMemcpyAsync(op, lv.A64, size_t(kMgStencil) * 9 * lv.rows * sizeof(double), cudaMemcpyDeviceToHost,
+                          stream_), "download");
+  if (smoother)
+    check(cudaMemcpyAsync(smoother, lv.S, 9 * size_t(lv.rows) * sizeof(float), cudaMemcpyDeviceToHost, stream_),
+          "download");
+  sync();
+  return lv.n;
+}
+
 template struct DeviceArray<double>;
 template struct DeviceArray<int>;
 template struct DeviceArray<float>;

@@ -11,6 +11,7 @@
 
 #include "../../include/drape_b200.h"
 #include "kernels.h"
+#include "mg.h"
 #include "problem.h"
 
 namespace drape {
@@ -88,6 +89,14 @@ class Context {
   // Stand-alone timed assembly at the current state (ms per launch).
   float time_assembly(int launches);
 
+  // ---- multilevel preconditioner
+  // Levels of the hierarchy the grid allows (0: not a structured grid of free vertices; only block Jacobi).
+  int mg_levels() const { return mg_levels_; }
+  // One V-cycle z = M r for the given f32 blocks (9B row-major) and right-hand side (the preconditioner check).
+  void precondition_host(const float* blocks, const double* r, double* z);
+  // Level `level`'s grid columns, f64 Galerkin stencil [225][rows] (level >= 1) and smoother [9][rows].
+  int multilevel_view(int level, double* op, float* smoother);
+
   std::string last_error;
 
  private:
@@ -97,6 +106,12 @@ class Context {
   double assemble(const double* x, double inv_h2, double mu, int mode, bool hessian);
   double reduce_partials(int n, int op, int slot);
   PcgResult pcg(double rtol, int max_iterations);
+  // The Newton direction solve: the configured preconditioner, block-Jacobi PCG as its fallback.
+  PcgResult direction_solve(double rtol, int max_iterations);
+  PcgResult mg_pcg(double rtol, int max_iterations, bool* stalled);
+  void configure_mg();
+  void mg_prepare();
+  void upload_blocks(const float* blocks);
   double direction_slope();
   double max_step(const double* x, const double* d);
   double energy_change(const double* x, const double* d, double alpha, double inv_h2, int mode);
@@ -133,6 +148,23 @@ class Context {
     ++kernels_;
   }
   long long kernels_ = 0;
+
+  // multilevel hierarchy (allocated when the grid allows it)
+  MgDevice mg_{};
+  int mg_levels_ = 0;
+  bool mg_stale_ = true;
+  int fallbacks_ = 0;
+  // multilevel solve outcomes: converged, limit, breakdown, stalled, coarse pivot failure, then the block-Jacobi
+  // fallback's converged, limit, breakdown
+  long long mg_outcome_[8] = {};
+  long long mg_iterations_ = 0;
+  DeviceArray<double> mg_a64_;
+  DeviceArray<float> mg_a_, mg_s_, mg_inv_, mg_partial_, mg_state_, mg_omega_;
+  DeviceArray<float4> mg_vec_;
+  DeviceArray<int> mg_error_;
+  MgState* pinned_mg_ = nullptr;
+  cudaGraphExec_t mg_graph_ = nullptr;
+  int mg_graph_launches_ = 0;
 
   // static problem arrays
   DeviceArray<double> geom_, hinge_k_, unit_mass_, colliders_;

@@ -1,0 +1,970 @@
+// Multilevel V-cycle preconditioner and flexible PCG (see mg.h for the hierarchy, layouts and the cycle).
+//
+// Every PCG iteration is a fixed sequence of small kernels (the kernel boundaries are the grid-wide syncs):
+//   restrict 0->1 (+ convergence test), restrict l->l+1 ..., coarse solve, prolong+post-smooth ... l+1->l,
+//   prolong+post-smooth 1->0 (partials z.r, z.r_prev), direction + SpMV (partial p.q), update (partial r.r, next
+//   pre-smoothing).
+// Dot products are per-CTA partials summed by every CTA of the next kernel in one fixed order, so all CTAs take
+// the same decisions and a solve is bit-for-bit repeatable. After convergence, breakdown or the iteration limit
+// (state->done) every kernel returns at once, so a launch sequence longer than needed costs only launch latency.
+#include <cuda_runtime.h>
+
+#include "mg.h"
+
+namespace drape {
+namespace {
+
+constexpr int kLanes = 8;               // lanes per row in level row kernels
+constexpr int kRowThreads = 256;        // 32 rows per CTA
+constexpr int kRestrictRows = 8;        // coarse rows per restriction CTA (one warp each)
+constexpr int kRestrictThreads = 32 * kRestrictRows;
+constexpr int kUpdateThreads = 256;     // one thread per row
+
+enum { kPartZr = 0, kPartZrPrev = 1, kPartPq = 2, kPartRr = 3 };
+enum { kStatusRunning = 0, kStatusConverged = 1, kStatusLimit = 2, kStatusBreakdown = 3, kStatusStalled = 4 };
+
+__device__ __forceinline__ void load_block(const DevBsr& A, int k, float m[9]) {
+  float4 u = A.a0[k], v = A.a1[k];
+  m[0] = u.x; m[1] = u.y; m[2] = u.z; m[3] = u.w;
+  m[4] = v.x; m[5] = v.y; m[6] = v.z; m[7] = v.w;
+  m[8] = A.a2[k];
+}
+
+__device__ __forceinline__ float3 f3(float4 v) { return make_float3(v.x, v.y, v.z); }
+__device__ __forceinline__ float3 add3(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 sub3(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 scale3(float s, float3 a) { return make_float3(s * a.x, s * a.y, s * a.z); }
+__device__ __forceinline__ float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float4 pack(float3 a) { return make_float4(a.x, a.y, a.z, 0.0f); }
+
+__device__ __forceinline__ float3 mul(const float m[9], float3 v) {
+  return make_float3(m[0] * v.x + m[1] * v.y + m[2] * v.z, m[3] * v.x + m[4] * v.y + m[5] * v.z,
+                     m[6] * v.x + m[7] * v.y + m[8] * v.z);
+}
+// S r with S stored as [9][rows]; transposed: S^T r.
+__device__ __forceinline__ float3 smooth(const float* S, int rows, int i, float3 r, bool transpose) {
+  float m[9];
+#pragma unroll
+  for (int e = 0; e < 9; ++e) m[e] = S[e * rows + i];
+  if (!transpose) return mul(m, r);
+  return make_float3(m[0] * r.x + m[3] * r.y + m[6] * r.z, m[1] * r.x + m[4] * r.y + m[7] * r.z,
+                     m[2] * r.x + m[5] * r.y + m[8] * r.z);
+}
+
+// Coarse stencil row I times the vector v at the offset's neighbour (0 outside the grid).
+__device__ __forceinline__ bool stencil_neighbour(int n, int X, int Y, int o, int* J) {
+  int dx = o % 5 - 2, dy = o / 5 - 2, x = X + dx, y = Y + dy;
+  if (x < 0 || y < 0 || x >= n || y >= n) return false;
+  *J = y * n + x;
+  return true;
+}
+
+__device__ __forceinline__ float3 stencil_apply(const float* A, int rows, int I, int o, float3 v) {
+  float m[9];
+#pragma unroll
+  for (int e = 0; e < 9; ++e) m[e] = A[(o * 9 + e) * rows + I];
+  return mul(m, v);
+}
+
+// 1D bilinear weight of fine index f for coarse index C (fine position 2C).
+__device__ __forceinline__ double w1d(int f, int C) {
+  int d = f - 2 * C;
+  return d == 0 ? 1.0 : (d == 1 || d == -1) ? 0.5 : 0.0;
+}
+
+// (P e)(fine vertex x, y): the bilinear interpolation of the coarse correction.
+__device__ __forceinline__ float3 interpolate(const float4* e, int nc, int x, int y) {
+  int X0 = x >> 1, Y0 = y >> 1;
+  int nx = (x & 1) ? 2 : 1, ny = (y & 1) ? 2 : 1;
+  float wx = (x & 1) ? 0.5f : 1.0f, wy = (y & 1) ? 0.5f : 1.0f;
+  float3 s = make_float3(0.f, 0.f, 0.f);
+  for (int b = 0; b < ny; ++b)
+    for (int a = 0; a < nx; ++a) s = add3(s, scale3(wx * wy, f3(e[(Y0 + b) * nc + X0 + a])));
+  return s;
+}
+
+// Sum of n per-CTA partials, the same value in every thread and every CTA (fixed order).
+__device__ float sum_partials(const float* p, int n) {
+  __shared__ float warp_sums[32];
+  float s = 0.0f;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += p[i];
+#pragma unroll
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) warp_sums[threadIdx.x >> 5] = s;
+  __syncthreads();
+  float t = 0.0f;
+  const int nw = (blockDim.x + 31) >> 5;
+  for (int w = 0; w < nw; ++w) t += warp_sums[w];
+  __syncthreads();
+  return t;
+}
+
+// Per-CTA sum of one value per thread (fixed order); the result is valid in thread 0.
+__device__ float cta_sum(float v) {
+  __shared__ float warp_sums[32];
+#pragma unroll
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) warp_sums[threadIdx.x >> 5] = v;
+  __syncthreads();
+  float t = 0.0f;
+  if (threadIdx.x == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    for (int w = 0; w < nw; ++w) t += warp_sums[w];
+  }
+  __syncthreads();
+  return t;
+}
+
+__device__ __forceinline__ float3 group_sum(float3 v) {
+#pragma unroll
+  for (int o = kLanes / 2; o; o >>= 1) {
+    v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+    v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+    v.z += __shfl_xor_sync(0xffffffffu, v.z, o);
+  }
+  return v;
+}
+
+int row_grid(int rows) { return (rows + kRowThreads / kLanes - 1) / (kRowThreads / kLanes); }
+int update_grid(int rows) { return (rows + kUpdateThreads - 1) / kUpdateThreads; }
+int restrict_grid(int coarse_rows) { return (coarse_rows + kRestrictRows - 1) / kRestrictRows; }
+
+// ---------------------------------------------------------------------------------------------- set-up
+
+// A_{l+1}[I][o] = sum_{i in supp I} sum_{j} w(i, I) A_l(i, j) w(j, J), J = I + offset(o); f64 sums.
+// One warp per coarse row: the warp first stages the nine fine support rows' entries (column, weight, block) in
+// shared memory, then lane o < 25 sums the entries landing on offset o, in entry order (deterministic).
+constexpr int kGalerkinWarps = 2;                 // 2 x 225 x 88 B of staged entries per CTA
+constexpr int kGalerkinEntries = 9 * kMgStencil;  // a row couples within 2 vertices per axis: <= 25 blocks
+
+struct GalerkinEntry {
+  double m[9];
+  double w;
+  int j;
+  int pad;
+};
+
+template <bool kSrcBsr>
+__global__ void __launch_bounds__(32 * kGalerkinWarps) galerkin_kernel(MgFine fine, MgLevel src, MgLevel dst,
+                                                                         int* error) {
+  __shared__ GalerkinEntry list[kGalerkinWarps][kGalerkinEntries];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int I = blockIdx.x * kGalerkinWarps + warp;
+  if (I >= dst.rows) return;  // whole warps leave together
+  const int nc = dst.n, nf = src.n, X = I % nc, Y = I / nc;
+  GalerkinEntry* L = list[warp];
+  // fine support row s = lane (lanes 0..8): its first entry and count
+  int i = -1, first = 0, len = 0;
+  if (lane < 9) {
+    const int fx = 2 * X + lane % 3 - 1, fy = 2 * Y + lane / 3 - 1;
+    if (fx >= 0 && fy >= 0 && fx < nf && fy < nf) {
+      i = fy * nf + fx;
+      if (kSrcBsr) {
+        first = fine.row_ptr[i];
+        len = fine.row_ptr[i + 1] - first;
+      } else {
+        len = kMgStencil;
+      }
+    }
+  }
+  int offset = len;  // exclusive prefix over lanes 0..8
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, offset, o);
+    if (lane >= o) offset += v;
+  }
+  const int total = __shfl_sync(0xffffffffu, offset, 8);
+  offset -= len;
+  if (total > kGalerkinEntries) {  // a pattern wider than the 5 x 5 stencil layout: report, write nothing
+    if (lane == 0) *error = 2;
+    return;
+  }
+  for (int s = 0; s < 9; ++s) {
+    const int si = __shfl_sync(0xffffffffu, i, s), sf = __shfl_sync(0xffffffffu, first, s);
+    const int sl = __shfl_sync(0xffffffffu, len, s), so = __shfl_sync(0xffffffffu, offset, s);
+    if (si < 0) continue;
+    const double wi = (s % 3 != 1 ? 0.5 : 1.0) * (s / 3 != 1 ? 0.5 : 1.0);
+    for (int t = lane; t < sl; t += 32) {
+      GalerkinEntry& E = L[so + t];
+      E.w = wi;
+      if (kSrcBsr) {
+        const int k = sf + t;
+        E.j = fine.col_idx[k];
+        float m[9];
+        load_block(fine.A, k, m);
+#pragma unroll
+        for (int e = 0; e < 9; ++e) E.m[e] = m[e];
+      } else {
+        int j;
+        const bool in = stencil_neighbour(nf, si % nf, si / nf, t, &j);
+        E.j = in ? j : -1;
+#pragma unroll
+        for (int e = 0; e < 9; ++e) E.m[e] = in ? src.A64[(t * 9 + e) * src.rows + si] : 0.0;
+      }
+    }
+  }
+  __syncwarp();
+  if (lane < kMgStencil) {
+    double acc[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) acc[e] = 0.0;
+    int J;
+    if (stencil_neighbour(nc, X, Y, lane, &J)) {
+      const int JX = J % nc, JY = J / nc;
+      for (int t = 0; t < total; ++t) {
+        const GalerkinEntry& E = L[t];
+        if (E.j < 0) continue;
+        const double wj = w1d(E.j % nf, JX) * w1d(E.j / nf, JY);
+        if (wj == 0.0) continue;
+        const double w = E.w * wj;
+#pragma unroll
+        for (int e = 0; e < 9; ++e) acc[e] += w * E.m[e];
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+      dst.A64[(lane * 9 + e) * dst.rows + I] = acc[e];
+      dst.A[(lane * 9 + e) * dst.rows + I] = float(acc[e]);
+    }
+  }
+}
+
+__device__ void inverse3(const double m[9], double omega, float out[9]) {
+  double c[9];
+  c[0] = m[4] * m[8] - m[5] * m[7];
+  c[1] = m[2] * m[7] - m[1] * m[8];
+  c[2] = m[1] * m[5] - m[2] * m[4];
+  c[3] = m[5] * m[6] - m[3] * m[8];
+  c[4] = m[0] * m[8] - m[2] * m[6];
+  c[5] = m[2] * m[3] - m[0] * m[5];
+  c[6] = m[3] * m[7] - m[4] * m[6];
+  c[7] = m[1] * m[6] - m[0] * m[7];
+  c[8] = m[0] * m[4] - m[1] * m[3];
+  const double det = m[0] * c[0] + m[1] * c[3] + m[2] * c[6];
+  const bool ok = det != 0.0 && isfinite(det);
+#pragma unroll
+  for (int e = 0; e < 9; ++e) out[e] = ok ? float(omega * c[e] / det) : 0.0f;
+}
+
+// S = omega D^{-1} per row (D the diagonal block).
+template <bool kBsr>
+__global__ void jacobi_smoother_kernel(MgFine fine, MgLevel lv, double omega) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= lv.rows) return;
+  double m[9];
+  if (kBsr) {
+    float f[9];
+    load_block(fine.A, fine.diag_pos[i], f);
+#pragma unroll
+    for (int e = 0; e < 9; ++e) m[e] = f[e];
+  } else {
+#pragma unroll
+    for (int e = 0; e < 9; ++e) m[e] = lv.A64[(12 * 9 + e) * lv.rows + i];
+  }
+  float s[9];
+  inverse3(m, omega, s);
+#pragma unroll
+  for (int e = 0; e < 9; ++e) lv.S[e * lv.rows + i] = s[e];
+}
+
+// Dense inverse of the coarsest operator by Gauss-Jordan elimination with partial pivoting (implicit row
+// exchanges), f64 in shared memory, one CTA. Step k: warp 0 picks the unused row p with the largest |M[p][k]|;
+// every row i != p subtracts (M[i][k] / M[p][k]) row p; row p is scaled by 1 / M[p][k]. Afterwards column k is
+// the unit vector at row perm[k], so row k of the inverse is row perm[k] of the right half.
+__global__ void __launch_bounds__(1024) coarse_inverse_kernel(MgLevel lv, float* inv, int* error) {
+  extern __shared__ double M[];  // [m][2m]
+  __shared__ double s_fac[3 * kMgCoarsestRowsMax];
+  __shared__ double s_row[6 * kMgCoarsestRowsMax];
+  __shared__ int s_used[3 * kMgCoarsestRowsMax], s_perm[3 * kMgCoarsestRowsMax];
+  __shared__ int s_piv;
+  const int m = 3 * lv.rows, w = 2 * m, n = lv.n;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int t = threadIdx.x; t < m * w; t += blockDim.x) M[t] = 0.0;
+  for (int t = threadIdx.x; t < m; t += blockDim.x) s_used[t] = 0;
+  __syncthreads();
+  for (int t = threadIdx.x; t < lv.rows * kMgStencil; t += blockDim.x) {
+    const int I = t / kMgStencil, o = t % kMgStencil;
+    int J;
+    if (!stencil_neighbour(n, I % n, I / n, o, &J)) continue;
+    for (int e = 0; e < 9; ++e) M[(3 * I + e / 3) * w + 3 * J + e % 3] = lv.A64[(o * 9 + e) * lv.rows + I];
+  }
+  for (int t = threadIdx.x; t < m; t += blockDim.x) M[t * w + m + t] = 1.0;
+  __syncthreads();
+  for (int k = 0; k < m; ++k) {
+    if (warp == 0) {
+      double best = -1.0;
+      int piv = -1;
+      for (int i = lane; i < m; i += 32)
+        if (!s_used[i]) {
+          const double v = fabs(M[i * w + k]);
+          if (v > best) best = v, piv = i;
+        }
+#pragma unroll
+      for (int o = 16; o; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int op = __shfl_xor_sync(0xffffffffu, piv, o);
+        if (ob > best || (ob == best && op >= 0 && (piv < 0 || op < piv))) best = ob, piv = op;
+      }
+      if (lane == 0) {
+        if (piv < 0 || !(best > 0.0) || !isfinite(best)) {
+          *error = 1;
+          piv = piv < 0 ? k : piv;
+        }
+        s_piv = piv;
+        s_used[piv] = 1;
+        s_perm[k] = piv;
+      }
+    }
+    __syncthreads();
+    const int p = s_piv;
+    const double d = M[p * w + k];
+    const double rd = d != 0.0 ? 1.0 / d : 0.0;
+    for (int c = threadIdx.x; c < w; c += blockDim.x) s_row[c] = M[p * w + c] * rd;
+    for (int i = threadIdx.x; i < m; i += blockDim.x) s_fac[i] = i == p ? 0.0 : M[i * w + k];
+    __syncthreads();
+    for (int t = threadIdx.x; t < m * w; t += blockDim.x) {
+      const int i = t / w, c = t % w;
+      M[t] = i == p ? s_row[c] : M[t] - s_fac[i] * s_row[c];
+    }
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < m * m; t += blockDim.x) inv[t] = float(M[s_perm[t / m] * w + m + t % m]);
+}
+
+// ---------------------------------------------------------------------------------------------- the cycle
+
+struct RestrictArgs {
+  MgFine fine;        // level-0 operator (kSrcBsr)
+  MgLevel src, dst;   // src.r / src.z: the level's right-hand side and pre-smoothed correction
+  bool coarsest;      // dst is the coarsest level: no pre-smoothing there
+  // convergence test (level-0 restriction of a PCG iteration)
+  MgState* state;
+  const float* rr_partial;
+  int rr_count;
+};
+
+__device__ __forceinline__ float3 warp_sum3(float3 v) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+    v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+    v.z += __shfl_xor_sync(0xffffffffu, v.z, o);
+  }
+  return v;
+}
+
+// r_{l+1} = P^T (r_l - A_l z_l), z_{l+1} = S_{l+1} r_{l+1}: one warp per coarse row; lanes 3s .. 3s + 2 take
+// the 9 fine support rows s (their blocks or stencil offsets interleaved), lanes 27..31 idle.
+// The level-0 restriction of a flexible PCG iteration first tests convergence, the limit and a stall.
+template <bool kSrcBsr, bool kCheck>
+__global__ void __launch_bounds__(kRestrictThreads) restrict_kernel(RestrictArgs a) {
+  if (kCheck) {
+    MgState* st = a.state;
+    if (st->done) return;
+    const float rr = sum_partials(a.rr_partial, a.rr_count);
+    const int it = st->iterations;
+    const float rr0 = it == 0 ? rr : st->rr0;
+    const bool window_end = it > 0 && st->stall_window > 0 && it % st->stall_window == 0;
+    const int window = st->stall_window > 0 ? it / st->stall_window : 0;
+    int status = kStatusRunning;
+    if (rr <= rr0 * st->tol2) status = kStatusConverged;
+    else if (!isfinite(rr)) status = kStatusBreakdown;
+    else if (it >= st->max_iterations) status = kStatusLimit;
+    else if (window_end && !(rr <= 0.81f * st->stall_rr[(window - 1) & 1])) status = kStatusStalled;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      st->rr = rr;
+      if (it == 0) st->rr0 = rr;
+      if (it == 0 || window_end) st->stall_rr[window & 1] = rr;
+      if (status != kStatusRunning) {
+        st->status = status;
+        st->done = 1;
+      }
+    }
+    if (status != kStatusRunning) return;
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int I = blockIdx.x * kRestrictRows + warp;
+  const int s = lane / 3, k3 = lane % 3;
+  float3 t = make_float3(0.f, 0.f, 0.f);
+  if (I < a.dst.rows && lane < 27) {
+    const int nc = a.dst.n, nf = a.src.n;
+    const int X = I % nc, Y = I / nc, ax = s % 3 - 1, by = s / 3 - 1;
+    const int fx = 2 * X + ax, fy = 2 * Y + by;
+    if (fx >= 0 && fy >= 0 && fx < nf && fy < nf) {
+      const int i = fy * nf + fx;
+      float3 acc = make_float3(0.f, 0.f, 0.f);
+      if (kSrcBsr) {
+        for (int k = a.fine.row_ptr[i] + k3; k < a.fine.row_ptr[i + 1]; k += 3) {
+          float m[9];
+          load_block(a.fine.A, k, m);
+          acc = add3(acc, mul(m, f3(a.src.z[a.fine.col_idx[k]])));
+        }
+      } else {
+        for (int o = k3; o < kMgStencil; o += 3) {
+          int j;
+          if (stencil_neighbour(nf, fx, fy, o, &j)) acc = add3(acc, stencil_apply(a.src.A, a.src.rows, i, o, f3(a.src.z[j])));
+        }
+      }
+      const float w = (ax ? 0.5f : 1.0f) * (by ? 0.5f : 1.0f);
+      t = scale3(w, k3 == 0 ? sub3(f3(a.src.r[i]), acc) : scale3(-1.0f, acc));
+    }
+  }
+  t = warp_sum3(t);
+  if (lane == 0 && I < a.dst.rows) {
+    a.dst.r[I] = pack(t);
+    if (!a.coarsest) a.dst.z[I] = pack(smooth(a.dst.S, a.dst.rows, I, t, false));
+  }
+}
+
+// e_L = A_L^{-1} r_L (dense f32 inverse), one CTA: r staged in shared memory, one warp per output entry.
+__global__ void __launch_bounds__(1024) coarse_solve_kernel(MgLevel lv, const float* inv, const MgState* state) {
+  if (state && state->done) return;
+  __shared__ float rs[3 * kMgCoarsestRowsMax];
+  const int m = 3 * lv.rows;
+  const float* r = reinterpret_cast<const float*>(lv.r);
+  float* e = reinterpret_cast<float*>(lv.e);
+  for (int j = threadIdx.x; j < m; j += blockDim.x) rs[j] = r[4 * (j / 3) + j % 3];
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+  for (int k = warp; k < m; k += warps) {
+    float s = 0.0f;
+    for (int j = lane; j < m; j += 32) s += inv[k * m + j] * rs[j];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) e[4 * (k / 3) + k % 3] = s;
+  }
+  for (int k = threadIdx.x; k < lv.rows; k += blockDim.x) e[4 * k + 3] = 0.0f;
+}
+
+struct ProlongArgs {
+  MgFine fine;       // level-0 operator (kFine)
+  MgLevel lv;        // level l: r, z (pre-smoothed), S, A; writes e
+  MgLevel coarse;    // level l + 1: e
+  const MgState* state;
+  // level 0 only: partial dots of the new z with the current and previous residuals
+  const float4* r_prev;
+  float* zr_partial;
+  float* zrp_partial;
+};
+
+// y = z_l + P e_{l+1};  e_l = y + S^T (r_l - A_l y), y at the neighbours interpolated on the fly.
+template <bool kFine>
+__global__ void __launch_bounds__(kRowThreads) prolong_kernel(ProlongArgs a) {
+  if (a.state && a.state->done) return;
+  const int lane = threadIdx.x % kLanes;
+  const int i = blockIdx.x * (kRowThreads / kLanes) + threadIdx.x / kLanes;
+  const int n = a.lv.n, nc = a.coarse.n;
+  const bool active = i < a.lv.rows;
+  float3 acc = make_float3(0.f, 0.f, 0.f);
+  if (active) {
+    if (kFine) {
+      for (int k = a.fine.row_ptr[i] + lane; k < a.fine.row_ptr[i + 1]; k += kLanes) {
+        const int j = a.fine.col_idx[k];
+        const float3 y = add3(f3(a.lv.z[j]), interpolate(a.coarse.e, nc, j % n, j / n));
+        float m[9];
+        load_block(a.fine.A, k, m);
+        acc = add3(acc, mul(m, y));
+      }
+    } else {
+      const int X = i % n, Y = i / n;
+      for (int o = lane; o < kMgStencil; o += kLanes) {
+        int j;
+        if (!stencil_neighbour(n, X, Y, o, &j)) continue;
+        const float3 y = add3(f3(a.lv.z[j]), interpolate(a.coarse.e, nc, j % n, j / n));
+        acc = add3(acc, stencil_apply(a.lv.A, a.lv.rows, i, o, y));
+      }
+    }
+  }
+  acc = group_sum(acc);
+  float zr = 0.0f, zrp = 0.0f;
+  if (active && lane == 0) {
+    const float3 r = f3(a.lv.r[i]);
+    const float3 y = add3(f3(a.lv.z[i]), interpolate(a.coarse.e, nc, i % n, i / n));
+    const float3 e = add3(y, smooth(a.lv.S, a.lv.rows, i, sub3(r, acc), true));
+    a.lv.e[i] = pack(e);
+    if (kFine && a.zr_partial) {  // inside flexible PCG only (a stand-alone cycle has no r_prev)
+      zr = dot3(e, r);
+      zrp = dot3(e, f3(a.r_prev[i]));
+    }
+  }
+  if (kFine && a.zr_partial) {
+    zr = cta_sum(zr);
+    zrp = cta_sum(zrp);
+    if (threadIdx.x == 0) {
+      a.zr_partial[blockIdx.x] = zr;
+      a.zrp_partial[blockIdx.x] = zrp;
+    }
+  }
+}
+
+struct DirectionArgs {
+  MgFine fine;
+  const float4* z;      // preconditioned residual (level-0 e)
+  const float4* p_old;
+  float4* p_new;
+  float4* q;
+  MgState* state;
+  const float* zr_partial;
+  const float* zrp_partial;
+  int zr_count;
+  float* pq_partial;
+};
+
+// beta (Polak-Ribiere form of flexible CG) = z.(r - r_prev) / rz_old;  p = z + beta p_old;  q = A p.
+__global__ void __launch_bounds__(kRowThreads) direction_kernel(DirectionArgs a) {
+  MgState* st = a.state;
+  if (st->done) return;
+  const float zr = sum_partials(a.zr_partial, a.zr_count);
+  const float zrp = sum_partials(a.zrp_partial, a.zr_count);
+  const bool first = st->iterations == 0;
+  const float beta = first ? 0.0f : (zr - zrp) / st->rz_old;
+  const int lane = threadIdx.x % kLanes;
+  const int i = blockIdx.x * (kRowThreads / kLanes) + threadIdx.x / kLanes;
+  const bool active = i < a.fine.R;
+  float3 acc = make_float3(0.f, 0.f, 0.f);
+  if (active) {
+    for (int k = a.fine.row_ptr[i] + lane; k < a.fine.row_ptr[i + 1]; k += kLanes) {
+      const int j = a.fine.col_idx[k];
+      const float3 p = first ? f3(a.z[j]) : add3(f3(a.z[j]), scale3(beta, f3(a.p_old[j])));
+      float m[9];
+      load_block(a.fine.A, k, m);
+      acc = add3(acc, mul(m, p));
+    }
+  }
+  acc = group_sum(acc);
+  float pq = 0.0f;
+  if (active && lane == 0) {
+    const float3 p = first ? f3(a.z[i]) : add3(f3(a.z[i]), scale3(beta, f3(a.p_old[i])));
+    a.p_new[i] = pack(p);
+    a.q[i] = pack(acc);
+    pq = dot3(p, acc);
+  }
+  pq = cta_sum(pq);
+  if (threadIdx.x == 0) a.pq_partial[blockIdx.x] = pq;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->zr = zr;
+    st->beta = beta;
+  }
+}
+
+struct UpdateArgs {
+  int R;
+  const float4* p;
+  const float4* q;
+  const float4* r_cur;
+  float4* r_next;
+  float4* x;
+  const float* S0;       // level-0 smoother
+  float4* z_pre;         // next pre-smoothing S0 r
+  MgState* state;
+  const float* pq_partial;
+  int pq_count;
+  float* rr_partial;
+  cudaGraphConditionalHandle cond;  // the solve graph's WHILE condition
+  int set_cond;                     // this launch ends the graph body: clear the condition once done
+};
+
+// alpha = z.r / p.q;  x += alpha p;  r_next = r - alpha q;  z_pre = S0 r_next.
+__global__ void __launch_bounds__(kUpdateThreads) update_kernel(UpdateArgs a) {
+  MgState* st = a.state;
+  if (st->done) {
+    if (a.set_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(a.cond, 0);
+    return;
+  }
+  const float pq = sum_partials(a.pq_partial, a.pq_count);
+  const float zr = st->zr;
+  const float alpha = zr / pq;
+  if (!(pq > 0.0f) || !isfinite(alpha)) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      st->pq = pq;
+      st->status = kStatusBreakdown;
+      st->done = 1;
+      if (a.set_cond) cudaGraphSetConditional(a.cond, 0);
+    }
+    return;
+  }
+  const int i = blockIdx.x * kUpdateThreads + threadIdx.x;
+  float rr = 0.0f;
+  if (i < a.R) {
+    const float3 p = f3(a.p[i]);
+    a.x[i] = pack(add3(f3(a.x[i]), scale3(alpha, p)));
+    const float3 r = sub3(f3(a.r_cur[i]), scale3(alpha, f3(a.q[i])));
+    a.r_next[i] = pack(r);
+    a.z_pre[i] = pack(smooth(a.S0, a.R, i, r, false));
+    rr = dot3(r, r);
+  }
+  rr = cta_sum(rr);
+  if (threadIdx.x == 0) a.rr_partial[blockIdx.x] = rr;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->pq = pq;
+    st->alpha = alpha;
+    st->rz_old = zr;
+    st->iterations = st->iterations + 1;
+  }
+}
+
+struct InitArgs {
+  int R;
+  const float4* b;
+  float4* x;
+  float4* r0;
+  float4* r1;
+  float4* p0;
+  float4* p1;
+  const float* S0;
+  float4* z_pre;
+  float* rr_partial;
+  MgState* state;
+  float tol2;
+  int max_iterations;
+  int stall_window;
+};
+
+__global__ void __launch_bounds__(kUpdateThreads) init_kernel(InitArgs a) {
+  const int i = blockIdx.x * kUpdateThreads + threadIdx.x;
+  float rr = 0.0f;
+  const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (i < a.R) {
+    const float3 b = f3(a.b[i]);
+    a.x[i] = zero;
+    a.r0[i] = pack(b);
+    a.r1[i] = zero;
+    a.p0[i] = zero;
+    a.p1[i] = zero;
+    a.z_pre[i] = pack(smooth(a.S0, a.R, i, b, false));
+    rr = dot3(b, b);
+  }
+  rr = cta_sum(rr);
+  if (threadIdx.x == 0) a.rr_partial[blockIdx.x] = rr;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    MgState s{};
+    s.tol2 = a.tol2;
+    s.max_iterations = a.max_iterations;
+    s.stall_window = a.stall_window;
+    *a.state = s;
+  }
+}
+
+// z_pre = S0 r (the pre-smoothing of a stand-alone V-cycle).
+__global__ void presmooth_kernel(int R, const float* S0, const float4* r, float4* z) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < R) z[i] = pack(smooth(S0, R, i, f3(r[i]), false));
+}
+
+MgLevel level0(const MgDevice& d, int parity) {
+  MgLevel l = d.lv[0];
+  l.r = d.r[parity];
+  return l;
+}
+
+// The V-cycle on level-0 right-hand side r[parity] with z_pre already in lv[0].z; result in lv[0].e.
+cudaError_t launch_cycle(const MgDevice& d, int parity, bool in_pcg, cudaStream_t s, int* launches) {
+  const int L = d.levels;
+  MgState* st = in_pcg ? d.state : nullptr;
+  for (int l = 0; l + 1 < L; ++l) {
+    RestrictArgs a{};
+    a.fine = d.fine;
+    a.src = l == 0 ? level0(d, parity) : d.lv[l];
+    a.dst = d.lv[l + 1];
+    a.coarsest = l + 2 == L;
+    a.state = d.state;
+    a.rr_partial = d.partial + kPartRr * kMgPartials;
+    a.rr_count = update_grid(d.fine.R);
+    const int grid = restrict_grid(a.dst.rows);
+    if (l == 0 && in_pcg) restrict_kernel<true, true><<<grid, kRestrictThreads, 0, s>>>(a);
+    else if (l == 0) restrict_kernel<true, false><<<grid, kRestrictThreads, 0, s>>>(a);
+    else if (in_pcg) restrict_kernel<false, false><<<grid, kRestrictThreads, 0, s>>>(a);
+    else restrict_kernel<false, false><<<grid, kRestrictThreads, 0, s>>>(a);
+    ++*launches;
+  }
+  coarse_solve_kernel<<<1, 1024, 0, s>>>(d.lv[L - 1], d.coarse_inv, st);
+  ++*launches;
+  for (int l = L - 2; l >= 0; --l) {
+    ProlongArgs a{};
+    a.fine = d.fine;
+    a.lv = l == 0 ? level0(d, parity) : d.lv[l];
+    a.coarse = d.lv[l + 1];
+    a.state = st;
+    if (l == 0 && in_pcg) {
+      a.r_prev = d.r[1 - parity];
+      a.zr_partial = d.partial + kPartZr * kMgPartials;
+      a.zrp_partial = d.partial + kPartZrPrev * kMgPartials;
+    }
+    const int grid = row_grid(a.lv.rows);
+    if (l == 0) prolong_kernel<true><<<grid, kRowThreads, 0, s>>>(a);
+    else prolong_kernel<false><<<grid, kRowThreads, 0, s>>>(a);
+    ++*launches;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+int mg_level_count(int n) {
+  int levels = 1;
+  while (n > kMgCoarsestMax && (n - 1) % 2 == 0 && levels < kMgMaxLevels) {
+    n = (n - 1) / 2 + 1;
+    ++levels;
+  }
+  return n <= kMgCoarsestMax ? levels : 1;
+}
+
+cudaError_t mg_fine_jacobi_smoother(const MgDevice& d, float omega, cudaStream_t s) {
+  const int R = d.fine.R;
+  jacobi_smoother_kernel<true><<<(R + 255) / 256, 256, 0, s>>>(d.fine, d.lv[0], omega);
+  return cudaGetLastError();
+}
+
+namespace {
+
+// Reproducible start vector of the power method: components uniform in [-1, 1) from a hash of the index.
+__device__ __forceinline__ float hash_unit(unsigned x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return float(x & 0xffffffu) * (2.0f / 16777216.0f) - 1.0f;
+}
+
+struct PowerArgs {
+  MgFine fine;
+  MgLevel lv[kMgMaxLevels];
+  int cta_start[kMgMaxLevels + 1];  // first CTA of each level (indexed from level `first`)
+  int first, end;                   // levels [first, end)
+  int parity;                       // reads z (0) or e (1) of each level, writes the other; partial region
+  int start;                        // first step: the hashed start vector instead of the read buffer
+  float* partial;                   // two regions of kMgPartials per-CTA |w|^2
+};
+
+// One power-method step on every level at once: w = D^{-1} A (v / |v|), |v| from the previous step's partials.
+// S holds D^{-1} during the set-up.
+__global__ void __launch_bounds__(kRowThreads) power_kernel(PowerArgs a) {
+  int l = a.first;
+  while (l + 1 < a.end && int(blockIdx.x) >= a.cta_start[l + 1]) ++l;
+  const MgLevel lv = a.lv[l];
+  const int c0 = a.cta_start[l], c1 = a.cta_start[l + 1];
+  float scale = 1.0f;
+  if (!a.start) {
+    const float ss = sum_partials(a.partial + (1 - a.parity) * kMgPartials + c0, c1 - c0);
+    scale = ss > 0.0f ? rsqrtf(ss) : 0.0f;
+  }
+  const float4* v = a.parity ? lv.e : lv.z;
+  float4* w = a.parity ? lv.z : lv.e;
+  const int lane = threadIdx.x % kLanes;
+  const int i = (blockIdx.x - c0) * (kRowThreads / kLanes) + threadIdx.x / kLanes;
+  const bool active = i < lv.rows;
+  auto value = [&](int j) -> float3 {
+    if (a.start) {
+      const unsigned h = 3u * unsigned(j) + 7919u * unsigned(l);
+      return make_float3(hash_unit(h), hash_unit(h + 1), hash_unit(h + 2));
+    }
+    return scale3(scale, f3(v[j]));
+  };
+  float3 acc = make_float3(0.f, 0.f, 0.f);
+  if (active) {
+    if (l == 0) {
+      for (int k = a.fine.row_ptr[i] + lane; k < a.fine.row_ptr[i + 1]; k += kLanes) {
+        float m[9];
+        load_block(a.fine.A, k, m);
+        acc = add3(acc, mul(m, value(a.fine.col_idx[k])));
+      }
+    } else {
+      const int n = lv.n, X = i % n, Y = i / n;
+      for (int o = lane; o < kMgStencil; o += kLanes) {
+        int j;
+        if (stencil_neighbour(n, X, Y, o, &j)) acc = add3(acc, stencil_apply(lv.A, lv.rows, i, o, value(j)));
+      }
+    }
+  }
+  acc = group_sum(acc);
+  float ww = 0.0f;
+  if (active && lane == 0) {
+    const float3 r = smooth(lv.S, lv.rows, i, acc, false);
+    w[i] = pack(r);
+    ww = dot3(r, r);
+  }
+  ww = cta_sum(ww);
+  if (threadIdx.x == 0) a.partial[a.parity * kMgPartials + blockIdx.x] = ww;
+}
+
+// lambda_l = |D^{-1} A v| for the unit v of the last step; omega_l from it (one warp).
+__global__ void power_finish_kernel(PowerArgs a, float* omega) {
+  const int lane = threadIdx.x;
+  const float* p = a.partial + a.parity * kMgPartials;
+  for (int l = a.first; l < a.end; ++l) {
+    float s = 0.0f;
+    for (int c = a.cta_start[l] + lane; c < a.cta_start[l + 1]; c += 32) s += p[c];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) {
+      const float lambda = sqrtf(s);
+      omega[l] = lambda > 0.0f && isfinite(lambda) ? 2.0f / (1.1f * lambda * (1.0f + 1.0f / 30.0f)) : 0.3f;
+    }
+  }
+}
+
+__global__ void scale_smoother_kernel(float* S, int count, const float* omega) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < count) S[t] *= *omega;
+}
+
+}  // namespace
+
+int mg_power_ctas(const MgDevice& d, int first, int end) {
+  int c = 0;
+  for (int l = first; l < end; ++l) c += row_grid(d.lv[l].rows);
+  return c;
+}
+
+cudaError_t mg_setup(const MgDevice& d, float omega, bool fine_smoother, cudaStream_t s) {
+  if (d.levels < 2) return cudaErrorInvalidValue;
+  cudaError_t e;
+  const int first = fine_smoother ? 0 : 1, end = d.levels - 1;  // smoothed levels
+  const double fixed = omega > 0.0f ? omega : 1.0;              // D^{-1} alone before the power method
+  if (fine_smoother) jacobi_smoother_kernel<true><<<(d.fine.R + 255) / 256, 256, 0, s>>>(d.fine, d.lv[0], fixed);
+  for (int l = 0; l + 1 < d.levels; ++l) {
+    const int grid = (d.lv[l + 1].rows + kGalerkinWarps - 1) / kGalerkinWarps;
+    if (l == 0) galerkin_kernel<true><<<grid, 32 * kGalerkinWarps, 0, s>>>(d.fine, d.lv[0], d.lv[1], d.error);
+    else galerkin_kernel<false><<<grid, 32 * kGalerkinWarps, 0, s>>>(d.fine, d.lv[l], d.lv[l + 1], d.error);
+    if (l + 2 < d.levels) {
+      const MgLevel& c = d.lv[l + 1];
+      jacobi_smoother_kernel<false><<<(c.rows + 255) / 256, 256, 0, s>>>(d.fine, c, fixed);
+    }
+  }
+  if (omega <= 0.0f && first < end) {
+    PowerArgs pa{};
+    pa.fine = d.fine;
+    for (int l = 0; l < d.levels; ++l) pa.lv[l] = d.lv[l];
+    pa.first = first;
+    pa.end = end;
+    pa.cta_start[first] = 0;
+    for (int l = first; l < end; ++l) pa.cta_start[l + 1] = pa.cta_start[l] + row_grid(d.lv[l].rows);
+    pa.partial = d.partial;
+    const int grid = pa.cta_start[end];
+    if (grid > kMgPartials) return cudaErrorInvalidValue;
+    for (int k = 0; k < kMgPowerSteps; ++k) {
+      pa.parity = k & 1;
+      pa.start = k == 0;
+      power_kernel<<<grid, kRowThreads, 0, s>>>(pa);
+    }
+    pa.parity = (kMgPowerSteps - 1) & 1;
+    power_finish_kernel<<<1, 32, 0, s>>>(pa, d.omega);
+    for (int l = first; l < end; ++l) {
+      const int count = 9 * d.lv[l].rows;
+      scale_smoother_kernel<<<(count + 255) / 256, 256, 0, s>>>(d.lv[l].S, count, d.omega + l);
+    }
+  }
+  const MgLevel& top = d.lv[d.levels - 1];
+  const int m = 3 * top.rows;
+  const size_t smem = size_t(m) * 2 * m * sizeof(double);
+  if ((e = cudaFuncSetAttribute(coarse_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))) != cudaSuccess)
+    return e;
+  coarse_inverse_kernel<<<1, 1024, smem, s>>>(top, d.coarse_inv, d.error);
+  return cudaGetLastError();
+}
+
+cudaError_t mg_pcg_init(const MgDevice& d, float tol2, int max_iterations, int stall_window, cudaStream_t s) {
+  InitArgs a{};
+  a.R = d.fine.R;
+  a.b = d.b;
+  a.x = d.x;
+  a.r0 = d.r[0];
+  a.r1 = d.r[1];
+  a.p0 = d.p[0];
+  a.p1 = d.p[1];
+  a.S0 = d.lv[0].S;
+  a.z_pre = d.lv[0].z;
+  a.rr_partial = d.partial + kPartRr * kMgPartials;
+  a.state = d.state;
+  a.tol2 = tol2;
+  a.max_iterations = max_iterations;
+  a.stall_window = stall_window;
+  init_kernel<<<update_grid(a.R), kUpdateThreads, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+namespace {
+
+// Iterations of parity 0 and 1 (one graph body); the second update kernel owns the WHILE condition.
+cudaError_t launch_body(const MgDevice& d, cudaGraphConditionalHandle cond, cudaStream_t s, int* launches) {
+  const int R = d.fine.R;
+  for (int par = 0; par < 2; ++par) {
+    cudaError_t e = launch_cycle(d, par, true, s, launches);
+    if (e != cudaSuccess) return e;
+    DirectionArgs da{};
+    da.fine = d.fine;
+    da.z = d.lv[0].e;
+    da.p_old = d.p[1 - par];
+    da.p_new = d.p[par];
+    da.q = d.q;
+    da.state = d.state;
+    da.zr_partial = d.partial + kPartZr * kMgPartials;
+    da.zrp_partial = d.partial + kPartZrPrev * kMgPartials;
+    da.zr_count = row_grid(R);
+    da.pq_partial = d.partial + kPartPq * kMgPartials;
+    direction_kernel<<<row_grid(R), kRowThreads, 0, s>>>(da);
+    UpdateArgs ua{};
+    ua.R = R;
+    ua.p = d.p[par];
+    ua.q = d.q;
+    ua.r_cur = d.r[par];
+    ua.r_next = d.r[1 - par];
+    ua.x = d.x;
+    ua.S0 = d.lv[0].S;
+    ua.z_pre = d.lv[0].z;
+    ua.state = d.state;
+    ua.pq_partial = d.partial + kPartPq * kMgPartials;
+    ua.pq_count = row_grid(R);
+    ua.rr_partial = d.partial + kPartRr * kMgPartials;
+    ua.cond = cond;
+    ua.set_cond = par == 1;
+    update_kernel<<<update_grid(R), kUpdateThreads, 0, s>>>(ua);
+    *launches += 2;
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+}  // namespace
+
+cudaError_t mg_build_solve_graph(const MgDevice& d, cudaStream_t s, cudaGraphExec_t* exec, int* launches_per_body) {
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaGraphCreate(&graph, 0);
+  if (e != cudaSuccess) return e;
+  cudaGraphConditionalHandle cond;
+  cudaGraphNodeParams p{};
+  cudaGraphNode_t node;
+  if ((e = cudaGraphConditionalHandleCreate(&cond, graph, 1, cudaGraphCondAssignDefault)) != cudaSuccess) goto done;
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = cond;
+  p.conditional.type = cudaGraphCondTypeWhile;
+  p.conditional.size = 1;
+  if ((e = cudaGraphAddNode(&node, graph, nullptr, 0, &p)) != cudaSuccess) goto done;
+  {
+    cudaGraph_t body = p.conditional.phGraph_out[0];
+    if ((e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
+        cudaSuccess)
+      goto done;
+    *launches_per_body = 0;
+    cudaError_t le = launch_body(d, cond, s, launches_per_body);
+    e = cudaStreamEndCapture(s, &body);
+    if (le != cudaSuccess) e = le;
+    if (e != cudaSuccess) goto done;
+  }
+  e = cudaGraphInstantiate(exec, graph, 0);
+done:
+  cudaGraphDestroy(graph);
+  return e;
+}
+
+cudaError_t mg_apply(const MgDevice& d, cudaStream_t s) {
+  const int R = d.fine.R;
+  presmooth_kernel<<<(R + 255) / 256, 256, 0, s>>>(R, d.lv[0].S, d.r[0], d.lv[0].z);
+  int launches = 0;
+  return launch_cycle(d, 0, false, s, &launches);
+}
+
+}  // namespace drape

@@ -1,0 +1,112 @@
+// Multilevel (geometric V-cycle) preconditioner over the sheet's structured grid and the flexible PCG that uses
+// it. This preconditioner has no counterpart in the reference, whose only direction solver is block-Jacobi PCG
+// (engine/oracle/src/pcg.rs:37-281, engine/gpu/src/solver.ts:126-191); block-Jacobi stays the fallback.
+//
+// Hierarchy. The fine level is the drape's BSR(3x3) matrix over an n x n vertex grid (row = vertex, vertex =
+// y * n + x). Level l + 1 has (n_l - 1) / 2 + 1 columns; the prolongation P is bilinear per displacement component
+// (fine vertex 2X + a takes coarse X with weight 1 if a == 0 and X, X + 1 with 1/2 if a == 1), restriction is
+// P^T, and coarse operators are Galerkin products A_{l+1} = P^T A_l P, summed in f64. Every coarse operator is a
+// 5 x 5 stencil of 3x3 blocks (a fine coupling reaches 2 vertices away, a hinge's opposite vertices); the
+// coarsest level (n <= 5) is solved exactly through its dense inverse.
+//
+// Coarse stencil layout (f32 copy used by the iteration, f64 master used by the next Galerkin product):
+//   A[(o * 9 + e) * rows + I]   o = (dy + 2) * 5 + (dx + 2) the offset of column vertex J = I + (dx, dy),
+//                               e = 3 * row + col within the block; entries outside the grid are zero.
+// Smoother blocks (one 3x3 per row, any level): S[e * rows + I].
+//
+// One V-cycle z = M r (pre-smoothing S, post-smoothing S^T, so M is symmetric when S is symmetric or the post
+// step uses the transpose of the pre step):
+//   level l:  z_l = S_l r_l;  r_{l+1} = P^T (r_l - A_l z_l);  ...;  e_L = A_L^{-1} r_L;
+//             y_l = z_l + P e_{l+1};  e_l = y_l + S_l^T (r_l - A_l y_l).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "device_problem.h"
+
+namespace drape {
+
+constexpr int kMgMaxLevels = 10;
+constexpr int kMgStencil = 25;
+constexpr int kMgCoarsestMax = 5;      // coarsen while n > 5 and n - 1 is even
+constexpr int kMgCoarsestRowsMax = 25; // dense coarse inverse of at most 75 x 75 (n <= 5)
+
+struct MgLevel {
+  int n = 0, rows = 0;
+  // coarse levels (l >= 1)
+  double* A64 = nullptr;  // [225][rows]
+  float* A = nullptr;     // [225][rows]
+  // every level
+  float* S = nullptr;     // smoother [9][rows]
+  float4* r = nullptr;    // level right-hand side (level 0: the PCG residual, owned by the solver)
+  float4* z = nullptr;    // pre-smoothed correction
+  float4* e = nullptr;    // correction after post-smoothing (level 0: the preconditioned residual)
+};
+
+// Flexible PCG state (device). Written by CTA 0 of the kernels; every CTA computes the same sums.
+// status: 1 converged, 2 iteration limit, 3 breakdown (p.q <= 0: the matrix or the preconditioner is not positive
+// definite), 4 stalled (|r| fell by less than 10% over stall_window iterations).
+// stall_rr[w & 1] holds rr at the end of stall window w: the test at the end of window w reads slot (w - 1) & 1
+// while CTA 0 writes slot w & 1, so no CTA reads a word another CTA of the same kernel writes.
+struct MgState {
+  float rr0, rr, zr, pq, alpha, beta, rz_old, tol2;
+  int iterations, status, done, max_iterations, stall_window, pad;
+  float stall_rr[2];
+};
+
+struct MgFine {
+  int R, n;
+  const int* row_ptr;
+  const int* col_idx;
+  const int* diag_pos;
+  DevBsr A;
+};
+
+// The device side of one hierarchy; every pointer is owned by the context.
+struct MgDevice {
+  MgFine fine;
+  int levels = 0;
+  MgLevel lv[kMgMaxLevels];
+  float* coarse_inv = nullptr;   // dense f32 inverse of the coarsest operator, [m][m], m = 3 rows
+  float* omega = nullptr;        // [kMgMaxLevels] damping of each level's Jacobi smoother (set-up output)
+  double* coarse_work = nullptr; // f64 [m][2m] Gauss-Jordan work space
+  // flexible PCG vectors (level 0, float4 rows)
+  const float4* b = nullptr;
+  float4* x = nullptr;
+  float4* r[2] = {};   // residual, double-buffered (current, previous)
+  float4* p[2] = {};   // search direction, double-buffered
+  float4* q = nullptr;
+  float* partial = nullptr;  // [4][kMgPartials]: zr, z.r_prev, pq, rr per CTA
+  MgState* state = nullptr;
+  int* error = nullptr;      // coarse factorisation found a zero pivot
+};
+
+constexpr int kMgRowsPerCta = 32;  // level-0 row kernels: 8 lanes per row, 256 threads
+constexpr int kMgPartials = 4096;  // capacity of each partial array (R <= 131072 rows)
+
+// Number of levels for an n x n grid (1 if it cannot be coarsened).
+int mg_level_count(int n);
+
+// Set-up after every assembly: Galerkin products down the hierarchy, smoothers omega_l D_l^{-1} (from level 1 when
+// `fine_smoother` is false: a network supplies level 0), the coarsest dense inverse. omega > 0 fixes every
+// level's damping; omega == 0 takes omega_l = 2 / (1.1 lambda_l (1 + 1/30)), the degree-1 Chebyshev smoother on
+// [lambda_l / 30, 1.1 lambda_l], with lambda_l = max eigenvalue of D_l^{-1} A_l from kMgPowerSteps steps of the
+// power method (all levels in one launch per step). A damping above 2 / lambda_l makes the smoother diverge on
+// the highest modes; the sheet drape's fine level has lambda ~ 3.4, so a fixed 0.6 is already unstable there.
+constexpr int kMgPowerSteps = 10;
+cudaError_t mg_setup(const MgDevice& d, float omega, bool fine_smoother, cudaStream_t s);
+// CTAs of the level row kernels summed over levels [first, end) (the power method's partial sums).
+int mg_power_ctas(const MgDevice& d, int first, int end);
+// Smoothers omega * D^{-1} at level 0 only.
+cudaError_t mg_fine_jacobi_smoother(const MgDevice& d, float omega, cudaStream_t s);
+
+// Flexible PCG: clear the state and start from x = 0, r = b.
+cudaError_t mg_pcg_init(const MgDevice& d, float tol2, int max_iterations, int stall_window, cudaStream_t s);
+// The whole flexible PCG loop as one executable graph: a conditional WHILE node whose body is two iterations
+// (the double buffers return to parity 0); the body's last kernel clears the condition once state->done is set
+// (convergence, iteration limit, breakdown or stall), so one graph launch runs the solve to its end on the device.
+// `launches_per_body` receives the kernels of one body execution.
+cudaError_t mg_build_solve_graph(const MgDevice& d, cudaStream_t s, cudaGraphExec_t* exec, int* launches_per_body);
+// One V-cycle z = M r on level 0 alone (r in d.r[0], z in d.lv[0].e): the preconditioner check.
+cudaError_t mg_apply(const MgDevice& d, cudaStream_t s);
+
+}  // namespace drape

@@ -30,13 +30,6 @@ __device__ __forceinline__ float dot3(float4 a, float4 b) { return a.x * b.x + a
 __device__ __forceinline__ unsigned long long pack(unsigned gen, float v) {
   return (static_cast<unsigned long long>(gen) << 32) | __float_as_uint(v);
 }
-__device__ __forceinline__ unsigned long long load_volatile(const unsigned long long* p) {
-  return *reinterpret_cast<const volatile unsigned long long*>(p);
-}
-__device__ __forceinline__ void store_volatile(unsigned long long* p, unsigned long long v) {
-  *reinterpret_cast<volatile unsigned long long*>(p) = v;
-}
-
 // CTA sum of NV per-thread floats into out[] (valid in thread 0 after the call).
 template <int NV> __device__ __forceinline__ void cta_sum(float (&v)[NV], float* out) {
   __shared__ float red[NV][32];

@@ -70,7 +70,11 @@ typedef struct {
   int32_t refine;              /* 1: one f64 residual refinement of every Newton direction */
   double refine_rtol;          /* relative tolerance of the refinement solve */
   int32_t curvature;           /* 1: keep the barrier's b'(I - nn^T)/|x - c| Hessian term (not SPD) */
-  int32_t preconditioner;      /* 0: block Jacobi */
+  int32_t preconditioner;      /* 0: block Jacobi (the reference's); 1: multilevel V-cycle over the structured grid with
+                                  omega-Jacobi smoothing, in flexible PCG; 2: the same V-cycle with the fine-level
+                                  smoother predicted by the preconditioner network (drape_load_network). 1 and 2 need
+                                  every vertex free (rows = vertices) on an n x n grid with n - 1 even; block-Jacobi
+                                  PCG takes over whenever their residual stops falling (drape_run_log.fallbacks) */
   double armijo;
   int32_t max_halvings;
   double time_budget_s;        /* 0: none */
@@ -81,6 +85,8 @@ typedef struct {
                                   (drape-e4.ts:55-62, e7_ptc.rs:129-133) */
   int32_t tangent;             /* 0: exact tangent (drape.rs:15-21 TangentKind::Exact) with Levenberg-Marquardt mu;
                                   1: projected (clamped membrane stress, Gauss-Newton hinge): SPD up to the barrier */
+  double smoother_omega;       /* multilevel: damping of the Jacobi smoothers; 0 (default): per level
+                                  2 / (1.1 lambda (1 + 1/30)) from the power method on D^{-1} A (stable) */
 } drape_options;
 
 /* Outcome of drape_solve_equilibrium (gpu-result.json fields, run-e7.ts:100-106). */
@@ -93,6 +99,8 @@ typedef struct {
   int32_t pcg_grid;     /* CTAs of each PCG launch */
   double device_seconds; /* CUDA events on the context's stream around the whole solve */
   int32_t kernel_launches; /* kernels the solve launched (all of this library's own) */
+  int32_t fallbacks;       /* multilevel solves handed to block-Jacobi PCG (breakdown or stalled residual) */
+  int32_t mg_levels;       /* levels of the multilevel hierarchy (0: block Jacobi) */
   int32_t pad;
 } drape_run_log;
 
@@ -156,8 +164,8 @@ drape_status drape_step_records(const drape_ctx* ctx, drape_step_record* out, in
  * (replaces evaluateKernelsWithInertia, drape-e4.ts; oracle DrapeStep::residual/tangent, drape.rs:304-322). */
 drape_status drape_assemble(drape_ctx* ctx, const double* x, const double* x_hat, double h, double mu, int32_t mode,
                             int32_t curvature, double* grad, float* blocks);
-/* Block-Jacobi PCG from 0 on the given f32 blocks (NULL: the last assembled matrix) and f64 rhs (3R, rounded to
- * f32); info = [iterations, status (1 converged, 2 iteration limit, 3 breakdown, 4 timeout), replacements],
+/* PCG from 0 on the given f32 blocks (NULL: the last assembled matrix) and f64 rhs (3R, rounded to f32), with
+ * the configured preconditioner (block Jacobi unless options.preconditioner selects the multilevel one); info = [iterations, status (1 converged, 2 iteration limit, 3 breakdown, 4 timeout), replacements],
  * relative = recursive sqrt(rr/rr0) (replaces solveOnce, solver.ts:179-191; oracle pcg::solve, pcg.rs:271-291). */
 drape_status drape_pcg(drape_ctx* ctx, const float* blocks, const double* rhs, double rtol, int32_t max_iterations,
                        double* solution, int32_t* info, double* relative);
@@ -172,6 +180,14 @@ drape_status drape_max_step(drape_ctx* ctx, const double* x, const double* d, do
  * e7_ptc.rs:43-51). */
 drape_status drape_static_residual(drape_ctx* ctx, const double* x, double* out);
 drape_status drape_static_energy(drape_ctx* ctx, const double* x, double* out);
+
+/* The multilevel preconditioner (no counterpart in the reference): z = M r, one V-cycle for the given f32 blocks
+ * (NULL: the last assembled matrix) and rhs r (3R f64, rounded to f32); z is 3R f64. */
+drape_status drape_precondition(drape_ctx* ctx, const float* blocks, const double* r, double* z);
+/* Level `level` of the hierarchy for the current matrix: *columns = its grid columns, op (level >= 1, may be NULL)
+ * the f64 Galerkin stencil [225][rows] (offset o = (dy + 2) * 5 + dx + 2, entry e = 3 * row + col), smoother
+ * (may be NULL) the f32 blocks [9][rows]. DRAPE_E_ARG when the problem has no hierarchy or level is out of range. */
+drape_status drape_multilevel_view(drape_ctx* ctx, int32_t level, int32_t* columns, double* op, float* smoother);
 
 /* Timed stand-alone launches for the roofline: average device ms per launch of the BSR SpMV on the last
  * assembled matrix (lanes per row 4/8/16/32) and of the row assembly at the current state. */
