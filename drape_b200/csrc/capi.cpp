@@ -355,6 +355,15 @@ drape_status drape_time_assembly(drape_ctx* ctx, int32_t launches, float* ms) {
   });
 }
 
+drape_status drape_time_multilevel(drape_ctx* ctx, int32_t iterations, float* out3) {
+  return guarded(ctx, [&](drape::Context& c) {
+    if (iterations < 2 || !out3) return fail(ctx, "invalid arguments", DRAPE_E_ARG);
+    if (c.mg_levels() == 0) return fail(ctx, "no multilevel hierarchy for this problem", DRAPE_E_ARG);
+    c.time_multilevel(iterations, out3);
+    return DRAPE_OK;
+  });
+}
+
 drape_status drape_pcg_profile(drape_ctx* ctx, int64_t* out, int32_t clear) {
   return guarded(ctx, [&](drape::Context& c) {
     if (!out) return fail(ctx, "out is null", DRAPE_E_ARG);

@@ -392,6 +392,7 @@ AttemptResult Context::attempt(double h, double scale) {
     return out;
   };
   kcheck(launch_predict(dp_, xn_.ptr, h * h, xhat_.ptr, stream_), "predict");
+  mg_setups_since_power_ = 1 << 20;  // a new step size: fresh spectral estimates at the first set-up
   if (opt_.newton_start == 1) {
     // The reference's start: x_n + alpha_max (x_hat - x_n).
     kcheck(launch_sub(int(nv), xhat_.ptr, xn_.ptr, towards_.ptr, stream_), "towards");
@@ -747,7 +748,7 @@ void Context::configure_mg() {
     v_count += 3 * size_t(rows[l]);
   }
   mg_a64_.alloc(a_count);
-  mg_a_.alloc(a_count);
+  mg_a_.alloc(a_count / 9 * 3);  // one 48-byte block (3 float4) per (row, offset)
   mg_s_.alloc(s_count);
   mg_vec_.alloc(v_count);
   check(cudaMemsetAsync(mg_vec_.ptr, 0, v_count * sizeof(float4), stream_), "memset");
@@ -763,7 +764,7 @@ void Context::configure_mg() {
   d.fine = MgFine{R, n[0], row_ptr_.ptr, col_idx_.ptr, diag_pos_.ptr, DevBsr{a0_.ptr, a1_.ptr, a2_.ptr}};
   d.levels = L;
   double* a64 = mg_a64_.ptr;
-  float* a32 = mg_a_.ptr;
+  float4* a32 = mg_a_.ptr;
   float* sm = mg_s_.ptr;
   float4* v = mg_vec_.ptr;
   for (int l = 0; l < L; ++l) {
@@ -776,7 +777,7 @@ void Context::configure_mg() {
       lv.A64 = a64;
       lv.A = a32;
       a64 += size_t(kMgStencil) * 9 * rows[l];
-      a32 += size_t(kMgStencil) * 9 * rows[l];
+      a32 += size_t(kMgStencil) * 3 * rows[l];
       lv.r = v;
       v += rows[l];
     }
@@ -801,7 +802,13 @@ void Context::configure_mg() {
   mg_ = d;
 
   sync();
-  check(mg_build_solve_graph(mg_, stream_, &mg_graph_, &mg_graph_launches_), "multilevel solve graph");
+  // Programmatic dependent launch inside the loop body where the driver accepts it, plain edges otherwise.
+  mg_graph_pdl_ = mg_build_solve_graph(mg_, stream_, &mg_graph_, &mg_graph_launches_, true) == cudaSuccess;
+  if (!mg_graph_pdl_) {
+    cudaGetLastError();
+    mg_graph_ = nullptr;
+    check(mg_build_solve_graph(mg_, stream_, &mg_graph_, &mg_graph_launches_, false), "multilevel solve graph");
+  }
   mg_stale_ = true;
 }
 
@@ -810,9 +817,11 @@ void Context::mg_prepare() {
   if (!mg_stale_) return;
   check(cudaMemsetAsync(mg_error_.ptr, 0, sizeof(int), stream_), "memset");
   const float omega = opt_.smoother_omega > 0 ? float(opt_.smoother_omega) : 0.0f;  // 0: spectral damping
-  kcheck(mg_setup(mg_, omega, true, stream_), "multilevel set-up");
+  const bool reuse = omega == 0.0f && mg_setups_since_power_ < 4;
+  mg_setups_since_power_ = reuse ? mg_setups_since_power_ + 1 : 1;
+  kcheck(mg_setup(mg_, omega, true, reuse, stream_), "multilevel set-up");
   // fine smoother, Galerkin products, coarse smoothers, coarsest inverse; the power method and its scaling
-  kernels_ += 2 * (mg_levels_ - 1) + (omega > 0 ? 0 : kMgPowerSteps + mg_levels_ - 1);
+  kernels_ += 2 * (mg_levels_ - 1) + (omega > 0 ? 0 : (reuse ? 0 : kMgPowerSteps + 1) + mg_levels_ - 2);
   mg_stale_ = false;
 }
 
@@ -877,6 +886,31 @@ void Context::precondition_host(const float* blocks, const double* rhs, double* 
     z[3 * i + 1] = r[i].y;
     z[3 * i + 2] = r[i].z;
   }
+}
+
+void Context::time_multilevel(int iterations, float* out3) {
+  if (mg_levels_ == 0) throw std::invalid_argument("no multilevel hierarchy for this problem");
+  mg_prepare();
+  check(cudaMemcpyAsync(mg_.r[0], b_.ptr, host_.R * sizeof(float4), cudaMemcpyDeviceToDevice, stream_), "copy");
+  for (int k = 0; k < 3; ++k) kcheck(mg_apply(mg_, stream_), "V-cycle");
+  check(cudaEventRecord(ev_[2], stream_), "event");
+  for (int k = 0; k < iterations; ++k) kcheck(mg_apply(mg_, stream_), "V-cycle");
+  check(cudaEventRecord(ev_[3], stream_), "event");
+  sync();
+  cudaEventElapsedTime(&out3[0], ev_[2], ev_[3]);
+  out3[0] /= iterations;
+  // exactly `iterations` iterations: tolerance 0, no stall test
+  kcheck(mg_pcg_init(mg_, 0.0f, 2, 0, stream_), "multilevel init");
+  check(cudaGraphLaunch(mg_graph_, stream_), "graph launch");
+  kcheck(mg_pcg_init(mg_, 0.0f, iterations, 0, stream_), "multilevel init");
+  check(cudaEventRecord(ev_[2], stream_), "event");
+  check(cudaGraphLaunch(mg_graph_, stream_), "graph launch");
+  check(cudaEventRecord(ev_[3], stream_), "event");
+  check(cudaMemcpyAsync(pinned_mg_, mg_.state, sizeof(MgState), cudaMemcpyDeviceToHost, stream_), "read");
+  sync();
+  cudaEventElapsedTime(&out3[1], ev_[2], ev_[3]);
+  out3[1] /= std::max(1, pinned_mg_->iterations);
+  out3[2] = mg_graph_pdl_ ? 1.0f : 0.0f;
 }
 
 int Context::multilevel_view(int level, double* op, float* smoother) {

@@ -88,6 +88,10 @@ class Context {
   float time_spmv(int launches, int lanes_per_row, int threads);
   // Stand-alone timed assembly at the current state (ms per launch).
   float time_assembly(int launches);
+  // Multilevel timings on the last assembled matrix: [ms per stand-alone V-cycle (plain launches), ms per flexible
+  // PCG iteration inside the solve graph (a fixed number of iterations), 1 if the graph links its kernels by
+  // programmatic dependent launch].
+  void time_multilevel(int iterations, float* out3);
 
   // ---- multilevel preconditioner
   // Levels of the hierarchy the grid allows (0: not a structured grid of free vertices; only block Jacobi).
@@ -153,18 +157,21 @@ class Context {
   MgDevice mg_{};
   int mg_levels_ = 0;
   bool mg_stale_ = true;
+  int mg_setups_since_power_ = 1 << 20;  // the power method reruns at a new attempt and every 4th set-up
   int fallbacks_ = 0;
   // multilevel solve outcomes: converged, limit, breakdown, stalled, coarse pivot failure, then the block-Jacobi
   // fallback's converged, limit, breakdown
   long long mg_outcome_[8] = {};
   long long mg_iterations_ = 0;
   DeviceArray<double> mg_a64_;
-  DeviceArray<float> mg_a_, mg_s_, mg_inv_, mg_partial_, mg_state_, mg_omega_;
+  DeviceArray<float> mg_s_, mg_inv_, mg_partial_, mg_state_, mg_omega_;
+  DeviceArray<float4> mg_a_;
   DeviceArray<float4> mg_vec_;
   DeviceArray<int> mg_error_;
   MgState* pinned_mg_ = nullptr;
   cudaGraphExec_t mg_graph_ = nullptr;
   int mg_graph_launches_ = 0;
+  bool mg_graph_pdl_ = false;
 
   // static problem arrays
   DeviceArray<double> geom_, hinge_k_, unit_mass_, colliders_;

@@ -21,6 +21,28 @@ constexpr int kRestrictThreads = 32 * kRestrictRows;
 constexpr int kUpdateThreads = 256;     // one thread per row
 
 enum { kPartZr = 0, kPartZrPrev = 1, kPartPq = 2, kPartRr = 3 };
+
+// Programmatic dependent launch: a kernel of the cycle lets the next one launch at once (its CTAs then wait in
+// griddepcontrol.wait until this grid has completed and its writes are visible). Both are no-ops for a kernel
+// launched without the attribute.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+template <typename... Params, typename... Args>
+cudaError_t launch(void (*kernel)(Params...), int grid, int block, cudaStream_t s, bool pdl, Args... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
 enum { kStatusRunning = 0, kStatusConverged = 1, kStatusLimit = 2, kStatusBreakdown = 3, kStatusStalled = 4 };
 
 __device__ __forceinline__ void load_block(const DevBsr& A, int k, float m[9]) {
@@ -59,10 +81,10 @@ __device__ __forceinline__ bool stencil_neighbour(int n, int X, int Y, int o, in
   return true;
 }
 
-__device__ __forceinline__ float3 stencil_apply(const float* A, int rows, int I, int o, float3 v) {
-  float m[9];
-#pragma unroll
-  for (int e = 0; e < 9; ++e) m[e] = A[(o * 9 + e) * rows + I];
+__device__ __forceinline__ float3 stencil_apply(const float4* A, int I, int o, float3 v) {
+  const float4* b = A + (size_t(I) * kMgStencil + o) * 3;
+  const float4 u = b[0], w = b[1], t = b[2];
+  const float m[9] = {u.x, u.y, u.z, u.w, w.x, w.y, w.z, w.w, t.x};
   return mul(m, v);
 }
 
@@ -224,10 +246,11 @@ __global__ void __launch_bounds__(32 * kGalerkinWarps) galerkin_kernel(MgFine fi
       }
     }
 #pragma unroll
-    for (int e = 0; e < 9; ++e) {
-      dst.A64[(lane * 9 + e) * dst.rows + I] = acc[e];
-      dst.A[(lane * 9 + e) * dst.rows + I] = float(acc[e]);
-    }
+    for (int e = 0; e < 9; ++e) dst.A64[(lane * 9 + e) * dst.rows + I] = acc[e];
+    float4* b = dst.A + (size_t(I) * kMgStencil + lane) * 3;
+    b[0] = make_float4(float(acc[0]), float(acc[1]), float(acc[2]), float(acc[3]));
+    b[1] = make_float4(float(acc[4]), float(acc[5]), float(acc[6]), float(acc[7]));
+    b[2] = make_float4(float(acc[8]), 0.0f, 0.0f, 0.0f);
   }
 }
 
@@ -360,6 +383,7 @@ __device__ __forceinline__ float3 warp_sum3(float3 v) {
 // The level-0 restriction of a flexible PCG iteration first tests convergence, the limit and a stall.
 template <bool kSrcBsr, bool kCheck>
 __global__ void __launch_bounds__(kRestrictThreads) restrict_kernel(RestrictArgs a) {
+  pdl_enter();
   if (kCheck) {
     MgState* st = a.state;
     if (st->done) return;
@@ -395,16 +419,25 @@ __global__ void __launch_bounds__(kRestrictThreads) restrict_kernel(RestrictArgs
     if (fx >= 0 && fy >= 0 && fx < nf && fy < nf) {
       const int i = fy * nf + fx;
       float3 acc = make_float3(0.f, 0.f, 0.f);
-      if (kSrcBsr) {
-        for (int k = a.fine.row_ptr[i] + k3; k < a.fine.row_ptr[i + 1]; k += 3) {
+      if (kSrcBsr) {  // <= 25 blocks per row: <= 9 per lane, column indices fetched first
+        const int k0 = a.fine.row_ptr[i] + k3, k1 = a.fine.row_ptr[i + 1];
+        int jj[9];
+#pragma unroll
+        for (int t = 0; t < 9; ++t) jj[t] = k0 + 3 * t < k1 ? a.fine.col_idx[k0 + 3 * t] : -1;
+#pragma unroll
+        for (int t = 0; t < 9; ++t) {
+          if (jj[t] < 0) continue;
           float m[9];
-          load_block(a.fine.A, k, m);
-          acc = add3(acc, mul(m, f3(a.src.z[a.fine.col_idx[k]])));
+          load_block(a.fine.A, k0 + 3 * t, m);
+          acc = add3(acc, mul(m, f3(a.src.z[jj[t]])));
         }
       } else {
-        for (int o = k3; o < kMgStencil; o += 3) {
+#pragma unroll
+        for (int t = 0; t < 9; ++t) {
+          const int o = k3 + 3 * t;
           int j;
-          if (stencil_neighbour(nf, fx, fy, o, &j)) acc = add3(acc, stencil_apply(a.src.A, a.src.rows, i, o, f3(a.src.z[j])));
+          if (o < kMgStencil && stencil_neighbour(nf, fx, fy, o, &j))
+            acc = add3(acc, stencil_apply(a.src.A, i, o, f3(a.src.z[j])));
         }
       }
       const float w = (ax ? 0.5f : 1.0f) * (by ? 0.5f : 1.0f);
@@ -420,6 +453,7 @@ __global__ void __launch_bounds__(kRestrictThreads) restrict_kernel(RestrictArgs
 
 // e_L = A_L^{-1} r_L (dense f32 inverse), one CTA: r staged in shared memory, one warp per output entry.
 __global__ void __launch_bounds__(1024) coarse_solve_kernel(MgLevel lv, const float* inv, const MgState* state) {
+  pdl_enter();
   if (state && state->done) return;
   __shared__ float rs[3 * kMgCoarsestRowsMax];
   const int m = 3 * lv.rows;
@@ -438,6 +472,68 @@ __global__ void __launch_bounds__(1024) coarse_solve_kernel(MgLevel lv, const fl
   for (int k = threadIdx.x; k < lv.rows; k += blockDim.x) e[4 * k + 3] = 0.0f;
 }
 
+// The last two levels in one CTA (T = L - 2, n_T <= 9, and the coarsest C): t = r_T - A_T z_T; r_C = P^T t;
+// e_C = A_C^{-1} r_C; y = z_T + P e_C; e_T = y + S_T^T (r_T - A_T y). Replaces a restriction, the coarse solve
+// and a prolongation (three launches) with one; the vectors stay in shared memory, one warp per row product.
+constexpr int kTailRows = 81;  // n_T <= 9
+__global__ void __launch_bounds__(1024) tail_kernel(MgLevel T, MgLevel C, const float* inv, const MgState* state) {
+  pdl_enter();
+  if (state && state->done) return;
+  __shared__ float3 t_s[kTailRows], y_s[kTailRows];
+  __shared__ float rc_s[3 * kMgCoarsestRowsMax], ec_s[3 * kMgCoarsestRowsMax];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+  const int n = T.n, nc = C.n, m = 3 * C.rows;
+  for (int i = warp; i < T.rows; i += warps) {
+    float3 acc = make_float3(0.f, 0.f, 0.f);
+    int j;
+    if (lane < kMgStencil && stencil_neighbour(n, i % n, i / n, lane, &j)) acc = stencil_apply(T.A, i, lane, f3(T.z[j]));
+    acc = warp_sum3(acc);
+    if (lane == 0) t_s[i] = sub3(f3(T.r[i]), acc);
+  }
+  __syncthreads();
+  for (int I = threadIdx.x; I < C.rows; I += blockDim.x) {
+    const int X = I % nc, Y = I / nc;
+    float3 r = make_float3(0.f, 0.f, 0.f);
+    for (int s = 0; s < 9; ++s) {
+      const int ax = s % 3 - 1, by = s / 3 - 1, fx = 2 * X + ax, fy = 2 * Y + by;
+      if (fx < 0 || fy < 0 || fx >= n || fy >= n) continue;
+      r = add3(r, scale3((ax ? 0.5f : 1.0f) * (by ? 0.5f : 1.0f), t_s[fy * n + fx]));
+    }
+    rc_s[3 * I] = r.x;
+    rc_s[3 * I + 1] = r.y;
+    rc_s[3 * I + 2] = r.z;
+  }
+  __syncthreads();
+  for (int k = warp; k < m; k += warps) {
+    float s = 0.0f;
+    for (int j = lane; j < m; j += 32) s += inv[k * m + j] * rc_s[j];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) ec_s[k] = s;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < T.rows; i += blockDim.x) {
+    const int x = i % n, y = i / n, X0 = x >> 1, Y0 = y >> 1;
+    const int nx = (x & 1) ? 2 : 1, ny = (y & 1) ? 2 : 1;
+    const float w = ((x & 1) ? 0.5f : 1.0f) * ((y & 1) ? 0.5f : 1.0f);
+    float3 v = f3(T.z[i]);
+    for (int b = 0; b < ny; ++b)
+      for (int a = 0; a < nx; ++a) {
+        const int J = (Y0 + b) * nc + X0 + a;
+        v = add3(v, scale3(w, make_float3(ec_s[3 * J], ec_s[3 * J + 1], ec_s[3 * J + 2])));
+      }
+    y_s[i] = v;
+  }
+  __syncthreads();
+  for (int i = warp; i < T.rows; i += warps) {
+    float3 acc = make_float3(0.f, 0.f, 0.f);
+    int j;
+    if (lane < kMgStencil && stencil_neighbour(n, i % n, i / n, lane, &j)) acc = stencil_apply(T.A, i, lane, y_s[j]);
+    acc = warp_sum3(acc);
+    if (lane == 0) T.e[i] = pack(add3(y_s[i], smooth(T.S, T.rows, i, sub3(f3(T.r[i]), acc), true)));
+  }
+}
+
 struct ProlongArgs {
   MgFine fine;       // level-0 operator (kFine)
   MgLevel lv;        // level l: r, z (pre-smoothed), S, A; writes e
@@ -452,6 +548,7 @@ struct ProlongArgs {
 // y = z_l + P e_{l+1};  e_l = y + S^T (r_l - A_l y), y at the neighbours interpolated on the fly.
 template <bool kFine>
 __global__ void __launch_bounds__(kRowThreads) prolong_kernel(ProlongArgs a) {
+  pdl_enter();
   if (a.state && a.state->done) return;
   const int lane = threadIdx.x % kLanes;
   const int i = blockIdx.x * (kRowThreads / kLanes) + threadIdx.x / kLanes;
@@ -459,21 +556,29 @@ __global__ void __launch_bounds__(kRowThreads) prolong_kernel(ProlongArgs a) {
   const bool active = i < a.lv.rows;
   float3 acc = make_float3(0.f, 0.f, 0.f);
   if (active) {
-    if (kFine) {
-      for (int k = a.fine.row_ptr[i] + lane; k < a.fine.row_ptr[i + 1]; k += kLanes) {
-        const int j = a.fine.col_idx[k];
+    if (kFine) {  // <= 25 blocks per row: <= 4 per lane, column indices fetched first
+      const int k0 = a.fine.row_ptr[i] + lane, k1 = a.fine.row_ptr[i + 1];
+      int jj[4];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) jj[t] = k0 + kLanes * t < k1 ? a.fine.col_idx[k0 + kLanes * t] : -1;
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        if (jj[t] < 0) continue;
+        const int j = jj[t];
         const float3 y = add3(f3(a.lv.z[j]), interpolate(a.coarse.e, nc, j % n, j / n));
         float m[9];
-        load_block(a.fine.A, k, m);
+        load_block(a.fine.A, k0 + kLanes * t, m);
         acc = add3(acc, mul(m, y));
       }
     } else {
       const int X = i % n, Y = i / n;
-      for (int o = lane; o < kMgStencil; o += kLanes) {
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int o = lane + kLanes * t;
         int j;
-        if (!stencil_neighbour(n, X, Y, o, &j)) continue;
+        if (o >= kMgStencil || !stencil_neighbour(n, X, Y, o, &j)) continue;
         const float3 y = add3(f3(a.lv.z[j]), interpolate(a.coarse.e, nc, j % n, j / n));
-        acc = add3(acc, stencil_apply(a.lv.A, a.lv.rows, i, o, y));
+        acc = add3(acc, stencil_apply(a.lv.A, i, o, y));
       }
     }
   }
@@ -514,6 +619,7 @@ struct DirectionArgs {
 
 // beta (Polak-Ribiere form of flexible CG) = z.(r - r_prev) / rz_old;  p = z + beta p_old;  q = A p.
 __global__ void __launch_bounds__(kRowThreads) direction_kernel(DirectionArgs a) {
+  pdl_enter();
   MgState* st = a.state;
   if (st->done) return;
   const float zr = sum_partials(a.zr_partial, a.zr_count);
@@ -524,12 +630,18 @@ __global__ void __launch_bounds__(kRowThreads) direction_kernel(DirectionArgs a)
   const int i = blockIdx.x * (kRowThreads / kLanes) + threadIdx.x / kLanes;
   const bool active = i < a.fine.R;
   float3 acc = make_float3(0.f, 0.f, 0.f);
-  if (active) {
-    for (int k = a.fine.row_ptr[i] + lane; k < a.fine.row_ptr[i + 1]; k += kLanes) {
-      const int j = a.fine.col_idx[k];
+  if (active) {  // <= 25 blocks per row: <= 4 per lane, column indices fetched first
+    const int k0 = a.fine.row_ptr[i] + lane, k1 = a.fine.row_ptr[i + 1];
+    int jj[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) jj[t] = k0 + kLanes * t < k1 ? a.fine.col_idx[k0 + kLanes * t] : -1;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      if (jj[t] < 0) continue;
+      const int j = jj[t];
       const float3 p = first ? f3(a.z[j]) : add3(f3(a.z[j]), scale3(beta, f3(a.p_old[j])));
       float m[9];
-      load_block(a.fine.A, k, m);
+      load_block(a.fine.A, k0 + kLanes * t, m);
       acc = add3(acc, mul(m, p));
     }
   }
@@ -568,6 +680,7 @@ struct UpdateArgs {
 
 // alpha = z.r / p.q;  x += alpha p;  r_next = r - alpha q;  z_pre = S0 r_next.
 __global__ void __launch_bounds__(kUpdateThreads) update_kernel(UpdateArgs a) {
+  pdl_enter();
   MgState* st = a.state;
   if (st->done) {
     if (a.set_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(a.cond, 0);
@@ -660,10 +773,13 @@ MgLevel level0(const MgDevice& d, int parity) {
 }
 
 // The V-cycle on level-0 right-hand side r[parity] with z_pre already in lv[0].z; result in lv[0].e.
-cudaError_t launch_cycle(const MgDevice& d, int parity, bool in_pcg, cudaStream_t s, int* launches) {
+cudaError_t launch_cycle(const MgDevice& d, int parity, bool in_pcg, bool pdl, cudaStream_t s, int* launches) {
   const int L = d.levels;
   MgState* st = in_pcg ? d.state : nullptr;
-  for (int l = 0; l + 1 < L; ++l) {
+  // with three or more levels, the last two run in one CTA (tail_kernel: level L - 2 is a stencil level, n <= 9)
+  const bool tail = L >= 3;
+  const int last_restricted = tail ? L - 2 : L - 1;
+  for (int l = 0; l < last_restricted; ++l) {
     RestrictArgs a{};
     a.fine = d.fine;
     a.src = l == 0 ? level0(d, parity) : d.lv[l];
@@ -673,15 +789,20 @@ cudaError_t launch_cycle(const MgDevice& d, int parity, bool in_pcg, cudaStream_
     a.rr_partial = d.partial + kPartRr * kMgPartials;
     a.rr_count = update_grid(d.fine.R);
     const int grid = restrict_grid(a.dst.rows);
-    if (l == 0 && in_pcg) restrict_kernel<true, true><<<grid, kRestrictThreads, 0, s>>>(a);
-    else if (l == 0) restrict_kernel<true, false><<<grid, kRestrictThreads, 0, s>>>(a);
-    else if (in_pcg) restrict_kernel<false, false><<<grid, kRestrictThreads, 0, s>>>(a);
-    else restrict_kernel<false, false><<<grid, kRestrictThreads, 0, s>>>(a);
+    cudaError_t e;
+    if (l == 0 && in_pcg) e = launch(restrict_kernel<true, true>, grid, kRestrictThreads, s, pdl, a);
+    else if (l == 0) e = launch(restrict_kernel<true, false>, grid, kRestrictThreads, s, pdl, a);
+    else e = launch(restrict_kernel<false, false>, grid, kRestrictThreads, s, pdl, a);
+    if (e != cudaSuccess) return e;
     ++*launches;
   }
-  coarse_solve_kernel<<<1, 1024, 0, s>>>(d.lv[L - 1], d.coarse_inv, st);
+  cudaError_t e = tail ? launch(tail_kernel, 1, 1024, s, pdl, d.lv[L - 2], d.lv[L - 1], (const float*)d.coarse_inv,
+                                (const MgState*)st)
+                       : launch(coarse_solve_kernel, 1, 1024, s, pdl, d.lv[L - 1], (const float*)d.coarse_inv,
+                                (const MgState*)st);
+  if (e != cudaSuccess) return e;
   ++*launches;
-  for (int l = L - 2; l >= 0; --l) {
+  for (int l = last_restricted - 1; l >= 0; --l) {
     ProlongArgs a{};
     a.fine = d.fine;
     a.lv = l == 0 ? level0(d, parity) : d.lv[l];
@@ -693,8 +814,9 @@ cudaError_t launch_cycle(const MgDevice& d, int parity, bool in_pcg, cudaStream_
       a.zrp_partial = d.partial + kPartZrPrev * kMgPartials;
     }
     const int grid = row_grid(a.lv.rows);
-    if (l == 0) prolong_kernel<true><<<grid, kRowThreads, 0, s>>>(a);
-    else prolong_kernel<false><<<grid, kRowThreads, 0, s>>>(a);
+    e = l == 0 ? launch(prolong_kernel<true>, grid, kRowThreads, s, pdl, a)
+               : launch(prolong_kernel<false>, grid, kRowThreads, s, pdl, a);
+    if (e != cudaSuccess) return e;
     ++*launches;
   }
   return cudaGetLastError();
@@ -775,7 +897,7 @@ __global__ void __launch_bounds__(kRowThreads) power_kernel(PowerArgs a) {
       const int n = lv.n, X = i % n, Y = i / n;
       for (int o = lane; o < kMgStencil; o += kLanes) {
         int j;
-        if (stencil_neighbour(n, X, Y, o, &j)) acc = add3(acc, stencil_apply(lv.A, lv.rows, i, o, value(j)));
+        if (stencil_neighbour(n, X, Y, o, &j)) acc = add3(acc, stencil_apply(lv.A, i, o, value(j)));
       }
     }
   }
@@ -819,7 +941,7 @@ int mg_power_ctas(const MgDevice& d, int first, int end) {
   return c;
 }
 
-cudaError_t mg_setup(const MgDevice& d, float omega, bool fine_smoother, cudaStream_t s) {
+cudaError_t mg_setup(const MgDevice& d, float omega, bool fine_smoother, bool reuse_omega, cudaStream_t s) {
   if (d.levels < 2) return cudaErrorInvalidValue;
   cudaError_t e;
   const int first = fine_smoother ? 0 : 1, end = d.levels - 1;  // smoothed levels
@@ -845,13 +967,15 @@ cudaError_t mg_setup(const MgDevice& d, float omega, bool fine_smoother, cudaStr
     pa.partial = d.partial;
     const int grid = pa.cta_start[end];
     if (grid > kMgPartials) return cudaErrorInvalidValue;
-    for (int k = 0; k < kMgPowerSteps; ++k) {
-      pa.parity = k & 1;
-      pa.start = k == 0;
-      power_kernel<<<grid, kRowThreads, 0, s>>>(pa);
+    if (!reuse_omega) {
+      for (int k = 0; k < kMgPowerSteps; ++k) {
+        pa.parity = k & 1;
+        pa.start = k == 0;
+        power_kernel<<<grid, kRowThreads, 0, s>>>(pa);
+      }
+      pa.parity = (kMgPowerSteps - 1) & 1;
+      power_finish_kernel<<<1, 32, 0, s>>>(pa, d.omega);
     }
-    pa.parity = (kMgPowerSteps - 1) & 1;
-    power_finish_kernel<<<1, 32, 0, s>>>(pa, d.omega);
     for (int l = first; l < end; ++l) {
       const int count = 9 * d.lv[l].rows;
       scale_smoother_kernel<<<(count + 255) / 256, 256, 0, s>>>(d.lv[l].S, count, d.omega + l);
@@ -889,10 +1013,10 @@ cudaError_t mg_pcg_init(const MgDevice& d, float tol2, int max_iterations, int s
 namespace {
 
 // Iterations of parity 0 and 1 (one graph body); the second update kernel owns the WHILE condition.
-cudaError_t launch_body(const MgDevice& d, cudaGraphConditionalHandle cond, cudaStream_t s, int* launches) {
+cudaError_t launch_body(const MgDevice& d, cudaGraphConditionalHandle cond, bool pdl, cudaStream_t s, int* launches) {
   const int R = d.fine.R;
   for (int par = 0; par < 2; ++par) {
-    cudaError_t e = launch_cycle(d, par, true, s, launches);
+    cudaError_t e = launch_cycle(d, par, true, pdl, s, launches);
     if (e != cudaSuccess) return e;
     DirectionArgs da{};
     da.fine = d.fine;
@@ -905,7 +1029,7 @@ cudaError_t launch_body(const MgDevice& d, cudaGraphConditionalHandle cond, cuda
     da.zrp_partial = d.partial + kPartZrPrev * kMgPartials;
     da.zr_count = row_grid(R);
     da.pq_partial = d.partial + kPartPq * kMgPartials;
-    direction_kernel<<<row_grid(R), kRowThreads, 0, s>>>(da);
+    if ((e = launch(direction_kernel, row_grid(R), kRowThreads, s, pdl, da)) != cudaSuccess) return e;
     UpdateArgs ua{};
     ua.R = R;
     ua.p = d.p[par];
@@ -921,7 +1045,7 @@ cudaError_t launch_body(const MgDevice& d, cudaGraphConditionalHandle cond, cuda
     ua.rr_partial = d.partial + kPartRr * kMgPartials;
     ua.cond = cond;
     ua.set_cond = par == 1;
-    update_kernel<<<update_grid(R), kUpdateThreads, 0, s>>>(ua);
+    if ((e = launch(update_kernel, update_grid(R), kUpdateThreads, s, pdl, ua)) != cudaSuccess) return e;
     *launches += 2;
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
@@ -930,7 +1054,8 @@ cudaError_t launch_body(const MgDevice& d, cudaGraphConditionalHandle cond, cuda
 
 }  // namespace
 
-cudaError_t mg_build_solve_graph(const MgDevice& d, cudaStream_t s, cudaGraphExec_t* exec, int* launches_per_body) {
+cudaError_t mg_build_solve_graph(const MgDevice& d, cudaStream_t s, cudaGraphExec_t* exec, int* launches_per_body,
+                                 bool pdl) {
   cudaGraph_t graph = nullptr;
   cudaError_t e = cudaGraphCreate(&graph, 0);
   if (e != cudaSuccess) return e;
@@ -949,7 +1074,7 @@ cudaError_t mg_build_solve_graph(const MgDevice& d, cudaStream_t s, cudaGraphExe
         cudaSuccess)
       goto done;
     *launches_per_body = 0;
-    cudaError_t le = launch_body(d, cond, s, launches_per_body);
+    cudaError_t le = launch_body(d, cond, pdl, s, launches_per_body);
     e = cudaStreamEndCapture(s, &body);
     if (le != cudaSuccess) e = le;
     if (e != cudaSuccess) goto done;
@@ -964,7 +1089,7 @@ cudaError_t mg_apply(const MgDevice& d, cudaStream_t s) {
   const int R = d.fine.R;
   presmooth_kernel<<<(R + 255) / 256, 256, 0, s>>>(R, d.lv[0].S, d.r[0], d.lv[0].z);
   int launches = 0;
-  return launch_cycle(d, 0, false, s, &launches);
+  return launch_cycle(d, 0, false, false, s, &launches);
 }
 
 }  // namespace drape

@@ -9,9 +9,11 @@
 // 5 x 5 stencil of 3x3 blocks (a fine coupling reaches 2 vertices away, a hinge's opposite vertices); the
 // coarsest level (n <= 5) is solved exactly through its dense inverse.
 //
-// Coarse stencil layout (f32 copy used by the iteration, f64 master used by the next Galerkin product):
-//   A[(o * 9 + e) * rows + I]   o = (dy + 2) * 5 + (dx + 2) the offset of column vertex J = I + (dx, dy),
-//                               e = 3 * row + col within the block; entries outside the grid are zero.
+// Coarse stencil layouts, o = (dy + 2) * 5 + (dx + 2) the offset of column vertex J = I + (dx, dy), e = 3 * row +
+// col within the block, entries outside the grid zero:
+//   A64[(o * 9 + e) * rows + I]        f64 master (the next Galerkin product, the coarsest inverse)
+//   A[(I * 25 + o) * 3 + q], q < 3     f32 copy read by the cycle: one 48-byte block per (row, offset) as three
+//                                      float4 (m00 m01 m02 m10 | m11 m12 m20 m21 | m22 0 0 0)
 // Smoother blocks (one 3x3 per row, any level): S[e * rows + I].
 //
 // One V-cycle z = M r (pre-smoothing S, post-smoothing S^T, so M is symmetric when S is symmetric or the post
@@ -34,7 +36,7 @@ struct MgLevel {
   int n = 0, rows = 0;
   // coarse levels (l >= 1)
   double* A64 = nullptr;  // [225][rows]
-  float* A = nullptr;     // [225][rows]
+  float4* A = nullptr;    // [rows][25][3] f32 blocks, 48 B each (see the layout above)
   // every level
   float* S = nullptr;     // smoother [9][rows]
   float4* r = nullptr;    // level right-hand side (level 0: the PCG residual, owned by the solver)
@@ -92,8 +94,10 @@ int mg_level_count(int n);
 // [lambda_l / 30, 1.1 lambda_l], with lambda_l = max eigenvalue of D_l^{-1} A_l from kMgPowerSteps steps of the
 // power method (all levels in one launch per step). A damping above 2 / lambda_l makes the smoother diverge on
 // the highest modes; the sheet drape's fine level has lambda ~ 3.4, so a fixed 0.6 is already unstable there.
+// `reuse_omega` skips the power method and scales by the omega_l of the last one (systems of one PTC attempt
+// change little from one Newton update to the next).
 constexpr int kMgPowerSteps = 10;
-cudaError_t mg_setup(const MgDevice& d, float omega, bool fine_smoother, cudaStream_t s);
+cudaError_t mg_setup(const MgDevice& d, float omega, bool fine_smoother, bool reuse_omega, cudaStream_t s);
 // CTAs of the level row kernels summed over levels [first, end) (the power method's partial sums).
 int mg_power_ctas(const MgDevice& d, int first, int end);
 // Smoothers omega * D^{-1} at level 0 only.
@@ -104,8 +108,10 @@ cudaError_t mg_pcg_init(const MgDevice& d, float tol2, int max_iterations, int s
 // The whole flexible PCG loop as one executable graph: a conditional WHILE node whose body is two iterations
 // (the double buffers return to parity 0); the body's last kernel clears the condition once state->done is set
 // (convergence, iteration limit, breakdown or stall), so one graph launch runs the solve to its end on the device.
-// `launches_per_body` receives the kernels of one body execution.
-cudaError_t mg_build_solve_graph(const MgDevice& d, cudaStream_t s, cudaGraphExec_t* exec, int* launches_per_body);
+// `launches_per_body` receives the kernels of one body execution. With `pdl` the body's kernels are linked by
+// programmatic dependencies (each launches while its predecessor finishes).
+cudaError_t mg_build_solve_graph(const MgDevice& d, cudaStream_t s, cudaGraphExec_t* exec, int* launches_per_body,
+                                 bool pdl);
 // One V-cycle z = M r on level 0 alone (r in d.r[0], z in d.lv[0].e): the preconditioner check.
 cudaError_t mg_apply(const MgDevice& d, cudaStream_t s);
 

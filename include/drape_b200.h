@@ -193,6 +193,10 @@ drape_status drape_multilevel_view(drape_ctx* ctx, int32_t level, int32_t* colum
  * assembled matrix (lanes per row 4/8/16/32) and of the row assembly at the current state. */
 drape_status drape_time_spmv(drape_ctx* ctx, int32_t launches, int32_t lanes_per_row, int32_t threads, float* ms);
 drape_status drape_time_assembly(drape_ctx* ctx, int32_t launches, float* ms);
+/* Multilevel timings on the last assembled matrix and right-hand side: out3 = [ms per stand-alone V-cycle,
+ * ms per flexible PCG iteration inside the solve graph (exactly `iterations` iterations), 1 if the graph's kernels
+ * are linked by programmatic dependent launch]. */
+drape_status drape_time_multilevel(drape_ctx* ctx, int32_t iterations, float* out3);
 /* SM-clock cycles CTA 0 of the PCG kernel spent per phase since the last clear: [phase A (p, q = A p),
  * its CTA sum, its grid reduction, phase B (x, r, z), its CTA sum, its grid reduction, iterations]; clear != 0
  * zeroes the counters. */
