@@ -105,6 +105,14 @@ def load():
     lib.drape_assemble.argtypes = [P, P, P, ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_int32, P, P]
     lib.drape_pcg.argtypes = [P, P, P, ctypes.c_double, ctypes.c_int32, P, P, P]
     lib.drape_precondition.argtypes = [P, P, P, P]
+    lib.drape_network_create.argtypes = [ctypes.c_int32, ctypes.c_uint64, ctypes.POINTER(P)]
+    lib.drape_network_destroy.argtypes = [P]
+    lib.drape_network_load.argtypes = [P, ctypes.c_char_p]
+    lib.drape_network_save.argtypes = [P, ctypes.c_char_p]
+    lib.drape_network_parameters.argtypes = [P, P, P]
+    lib.drape_set_network.argtypes = [P, P]
+    lib.drape_network_gradient.argtypes = [P, P, P, P, P, P, P, P]
+    lib.drape_network_train.argtypes = [P, P, ctypes.c_int32, P, P, P, ctypes.c_int32, ctypes.c_double, P]
     lib.drape_multilevel_view.argtypes = [P, ctypes.c_int32, P, P, P]
     lib.drape_energy_change.argtypes = [P, P, P, ctypes.c_double, P, ctypes.c_double, ctypes.c_int32, P]
     lib.drape_max_step.argtypes = [P, P, P, P]
@@ -277,6 +285,11 @@ class Drape:
         return sol, {"iterations": int(info[0]), "status": PCG_STATUS.get(int(info[1]), int(info[1])),
                      "replacements": int(info[2]), "relative": rel.value}
 
+    def set_network(self, network):
+        """Attach the network preconditioner 2 uses (kept alive by this object)."""
+        self._network = network
+        self._check(self.lib.drape_set_network(self.h, network.h if network is not None else None))
+
     def precondition(self, r, blocks=None):
         """One multilevel V-cycle z = M r (the preconditioner of options.preconditioner 1 and 2)."""
         z = np.zeros(3 * self.R)
@@ -340,6 +353,78 @@ def version():
 def _host_call(st):
     if st != 0:
         raise DrapeError(st, load().drape_last_error(None).decode())
+
+
+NETWORK_PARAMETERS = 34177
+NETWORK_FILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "preconditioner_network.bin")
+
+
+class Network:
+    """The preconditioner network (options.preconditioner = 2): a 4-layer mesh message-passing network that scales
+    the multilevel preconditioner's fine Jacobi smoother per row. `Network.trained()` loads the shipped weights."""
+
+    def __init__(self, seed=0, device=0, path=None):
+        self.lib = load()
+        h = P()
+        if self.lib.drape_network_create(device, seed, ctypes.byref(h)) != 0:
+            raise DrapeError(2, self.lib.drape_last_error(None).decode())
+        self.h = h
+        if path:
+            self.load(path)
+
+    @classmethod
+    def trained(cls, device=0):
+        return cls(device=device, path=NETWORK_FILE)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.drape_network_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def _check(self, st, ctx=None):
+        if st != 0:
+            raise DrapeError(st, self.lib.drape_last_error(ctx).decode())
+
+    def load(self, path):
+        self._check(self.lib.drape_network_load(self.h, os.fsencode(path)))
+
+    def save(self, path):
+        self._check(self.lib.drape_network_save(self.h, os.fsencode(path)))
+
+    @property
+    def parameters(self):
+        p = np.zeros(NETWORK_PARAMETERS, np.float32)
+        self._check(self.lib.drape_network_parameters(self.h, _ptr(p), None))
+        return p
+
+    @parameters.setter
+    def parameters(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == NETWORK_PARAMETERS
+        self._check(self.lib.drape_network_parameters(self.h, None, _ptr(p)))
+
+    def gradient(self, drape, blocks, rhs, solution):
+        """(loss, gradient, factors) of one (blocks, rhs, solution) tuple on the drape's pattern."""
+        grad = np.zeros(NETWORK_PARAMETERS, np.float32)
+        fac = np.zeros(drape.R, np.float32)
+        loss = ctypes.c_double()
+        blk = np.ascontiguousarray(blocks, np.float32)
+        self._check(self.lib.drape_network_gradient(drape.h, self.h, _ptr(blk), _ptr(_f64(rhs)), _ptr(_f64(solution)),
+                                                    ctypes.byref(loss), _ptr(grad), _ptr(fac)), drape.h)
+        return loss.value, grad, fac
+
+    def train(self, drape, tuples, steps, lr=1e-3):
+        """Adam over [(blocks, rhs, solution), ...] of the drape's pattern; returns the per-step losses."""
+        keep = [(np.ascontiguousarray(b, np.float32), _f64(r), _f64(x)) for b, r, x in tuples]
+        n = len(keep)
+        B = (P * n)(*[_ptr(k[0]) for k in keep])
+        Rr = (P * n)(*[_ptr(k[1]) for k in keep])
+        X = (P * n)(*[_ptr(k[2]) for k in keep])
+        losses = np.zeros(steps)
+        self._check(self.lib.drape_network_train(drape.h, self.h, n, B, Rr, X, steps, lr, _ptr(losses)), drape.h)
+        return losses
 
 
 def write_sheet_problem(directory, columns, seed=0, radius=0.25, young=5e5, plane=False):

@@ -1,5 +1,7 @@
 // extern "C" boundary of libdrape_b200.so (declarations and reference citations: include/drape_b200.h).
+#include <cstdio>
 #include <cstring>
+#include <vector>
 #include <memory>
 #include <string>
 
@@ -8,6 +10,10 @@
 
 struct drape_ctx {
   std::unique_ptr<drape::Context> impl;
+};
+
+struct drape_network {
+  std::unique_ptr<drape::Network> impl;
 };
 
 namespace {
@@ -221,6 +227,7 @@ drape_status drape_set_options(drape_ctx* ctx, const drape_options* options) {
       return fail(ctx, "the multilevel preconditioner needs every vertex free on an n x n grid with n - 1 even",
                   DRAPE_E_ARG);
     c.options() = *options;
+    c.options_changed();
     return DRAPE_OK;
   });
 }
@@ -282,6 +289,90 @@ drape_status drape_pcg(drape_ctx* ctx, const float* blocks, const double* rhs, d
       info[2] = r.replacements;
     }
     if (relative) *relative = r.relative;
+    return DRAPE_OK;
+  });
+}
+
+drape_status drape_network_create(int32_t device, uint64_t seed, drape_network** out) {
+  if (!out) return fail(nullptr, "out is null", DRAPE_E_ARG);
+  *out = nullptr;
+  try {
+    auto n = std::make_unique<drape_network>();
+    n->impl = std::make_unique<drape::Network>(device, seed);
+    *out = n.release();
+    return DRAPE_OK;
+  } catch (const drape::CudaError& e) {
+    return fail(nullptr, e.what(), DRAPE_E_CUDA);
+  } catch (const std::exception& e) {
+    return fail(nullptr, e.what(), DRAPE_E_ARG);
+  }
+}
+
+void drape_network_destroy(drape_network* net) { delete net; }
+
+drape_status drape_network_parameters(drape_network* net, float* get, const float* set) {
+  if (!net || !net->impl) return fail(nullptr, "null network", DRAPE_E_STATE);
+  try {
+    if (get) net->impl->get(get);
+    if (set) net->impl->set(set);
+    return DRAPE_OK;
+  } catch (const std::exception& e) {
+    return fail(nullptr, e.what(), DRAPE_E_CUDA);
+  }
+}
+
+drape_status drape_network_save(drape_network* net, const char* path) {
+  if (!net || !net->impl || !path) return fail(nullptr, "null network or path", DRAPE_E_ARG);
+  std::vector<float> p(drape::kNnParams);
+  if (drape_status st = drape_network_parameters(net, p.data(), nullptr)) return st;
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return fail(nullptr, std::string("cannot write ") + path, DRAPE_E_IO);
+  const int32_t count = drape::kNnParams;
+  bool ok = std::fwrite("DRAPENN1", 1, 8, f) == 8 && std::fwrite(&count, 4, 1, f) == 1 &&
+            std::fwrite(p.data(), 4, p.size(), f) == p.size();
+  ok = std::fclose(f) == 0 && ok;
+  return ok ? DRAPE_OK : fail(nullptr, std::string("short write to ") + path, DRAPE_E_IO);
+}
+
+drape_status drape_network_load(drape_network* net, const char* path) {
+  if (!net || !net->impl || !path) return fail(nullptr, "null network or path", DRAPE_E_ARG);
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return fail(nullptr, std::string("cannot read ") + path, DRAPE_E_IO);
+  char magic[8];
+  int32_t count = 0;
+  std::vector<float> p(drape::kNnParams);
+  bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "DRAPENN1", 8) == 0 &&
+            std::fread(&count, 4, 1, f) == 1 && count == drape::kNnParams &&
+            std::fread(p.data(), 4, p.size(), f) == p.size();
+  std::fclose(f);
+  if (!ok) return fail(nullptr, std::string("not a drape network file of this layout: ") + path, DRAPE_E_IO);
+  return drape_network_parameters(net, nullptr, p.data());
+}
+
+drape_status drape_set_network(drape_ctx* ctx, drape_network* net) {
+  return guarded(ctx, [&](drape::Context& c) {
+    c.attach_network(net ? net->impl.get() : nullptr);
+    return DRAPE_OK;
+  });
+}
+
+drape_status drape_network_gradient(drape_ctx* ctx, drape_network* net, const float* blocks, const double* rhs,
+                                    const double* solution, double* loss, float* grad, float* factors) {
+  return guarded(ctx, [&](drape::Context& c) {
+    if (!net || !net->impl || !blocks || !rhs || !solution) return fail(ctx, "invalid arguments", DRAPE_E_ARG);
+    const double l = c.network_gradient_host(*net->impl, blocks, rhs, solution, grad, factors);
+    if (loss) *loss = l;
+    return DRAPE_OK;
+  });
+}
+
+drape_status drape_network_train(drape_ctx* ctx, drape_network* net, int32_t tuples, const float* const* blocks,
+                                 const double* const* rhs, const double* const* solutions, int32_t steps, double lr,
+                                 double* losses) {
+  return guarded(ctx, [&](drape::Context& c) {
+    if (!net || !net->impl || tuples < 1 || steps < 0 || !blocks || !rhs || !solutions || !(lr > 0))
+      return fail(ctx, "invalid arguments", DRAPE_E_ARG);
+    c.network_train_host(*net->impl, tuples, blocks, rhs, solutions, steps, lr, losses);
     return DRAPE_OK;
   });
 }

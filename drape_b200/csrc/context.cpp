@@ -643,6 +643,7 @@ void Context::upload_blocks(const float* blocks) {
   a1_.upload(h1.data(), B, stream_);
   a2_.upload(h2.data(), B, stream_);
   mg_stale_ = true;
+  mg_setups_since_power_ = 1 << 20;  // an unrelated matrix: fresh spectral estimates
   sync();
 }
 
@@ -822,6 +823,12 @@ void Context::mg_prepare() {
   kcheck(mg_setup(mg_, omega, true, reuse, stream_), "multilevel set-up");
   // fine smoother, Galerkin products, coarse smoothers, coarsest inverse; the power method and its scaling
   kernels_ += 2 * (mg_levels_ - 1) + (omega > 0 ? 0 : (reuse ? 0 : kMgPowerSteps + 1) + mg_levels_ - 2);
+  if (opt_.preconditioner == 2) {
+    if (!net_) throw std::invalid_argument("preconditioner 2 needs a preconditioner network (drape_set_network)");
+    ensure_nn_buffers();
+    kcheck(nn_forward(nnb_, net_->view(), mg_.omega, mg_.lv[0].S, stream_), "preconditioner network");
+    kernels_ += 2 + kNnLayers;  // features, input layer, message-passing layers, head
+  }
   mg_stale_ = false;
 }
 
@@ -927,8 +934,216 @@ int Context::multilevel_view(int level, double* op, float* smoother) {
   return lv.n;
 }
 
+// ------------------------------------------------------------------------------------ preconditioner network
+
+Network::Network(int dev, uint64_t seed) : device(dev) {
+  check(cudaSetDevice(device), "cudaSetDevice");
+  master.alloc(kNnParams);
+  adam_m.alloc(kNnParams);
+  adam_v.alloc(kNnParams);
+  bf16.alloc(kNnBf16);
+  // Glorot-uniform weights from a 64-bit LCG, zero biases, a zero output layer (f = 1: the untrained network is
+  // the multilevel preconditioner's spectral smoother).
+  std::vector<float> p(kNnParams, 0.0f);
+  uint64_t state = seed * 6364136223846793005ULL + 1442695040888963407ULL;
+  auto uniform = [&]() {
+    state = state * 6364136223846793005ULL + 1442695040888963407ULL;
+    return double(state >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
+  };
+  auto fill = [&](int off, int fan_in, int fan_out) {
+    const double a = std::sqrt(6.0 / (fan_in + fan_out));
+    for (int t = 0; t < fan_in * fan_out; ++t) p[off + t] = float(a * uniform());
+  };
+  fill(kNnOffWin, kNnIn, kNnHidden);
+  for (int l = 0; l < kNnLayers; ++l) fill(kNnOffLayer0 + l * kNnLayerSize, 2 * kNnHidden, kNnHidden);
+  set(p.data());
+}
+
+NnWeights Network::view() {
+  return NnWeights{master.ptr, reinterpret_cast<__nv_bfloat16*>(bf16.ptr), adam_m.ptr, adam_v.ptr};
+}
+
+void Network::set(const float* params) {
+  check(cudaSetDevice(device), "cudaSetDevice");
+  check(cudaMemcpy(master.ptr, params, kNnParams * sizeof(float), cudaMemcpyHostToDevice), "upload");
+  check(cudaMemset(adam_m.ptr, 0, kNnParams * sizeof(float)), "memset");
+  check(cudaMemset(adam_v.ptr, 0, kNnParams * sizeof(float)), "memset");
+  adam_t = 0;
+  check(nn_refresh_bf16(view(), nullptr), "bf16 weights");
+  check(cudaDeviceSynchronize(), "synchronize");
+}
+
+void Network::get(float* params) {
+  check(cudaSetDevice(device), "cudaSetDevice");
+  check(cudaMemcpy(params, master.ptr, kNnParams * sizeof(float), cudaMemcpyDeviceToHost), "download");
+}
+
+namespace {
+enum NnVec { kNb = 0, kNx, kZ1, kT, kC, kY, kU, kZ, kE, kAe, kAx, kGz, kSg, kGy, kGz1, kNnVecs };
+}  // namespace
+
+void Context::ensure_nn_buffers() {
+  if (nnb_.R) return;
+  if (mg_levels_ == 0) throw std::invalid_argument("the preconditioner network needs the multilevel hierarchy");
+  const int R = host_.R, B = host_.B;
+  nn_feat_.alloc(size_t(R) * kNnIn);
+  nn_w_.alloc(B);
+  nn_h_.alloc(size_t(kNnLayers + 1) * R * kNnHidden);
+  nn_o_.alloc(R);
+  nn_dh_.alloc(2 * size_t(R) * kNnHidden);
+  nn_dx_.alloc(2 * size_t(R) * kNnHidden);
+  nn_partial_.alloc(size_t(nn_back_ctas(R)) * kNnParams);
+  nn_grad_.alloc(kNnParams);
+  nn_dfac_.alloc(R);
+  nn_s0_.alloc(9 * size_t(R));
+  nn_zero_.alloc(9 * size_t(R));
+  check(cudaMemsetAsync(nn_zero_.ptr, 0, 9 * size_t(R) * sizeof(float), stream_), "memset");
+  nn_fscale_.alloc(4);
+  nn_vec_.alloc(kNnVecs * size_t(R));
+  check(cudaMemsetAsync(nn_vec_.ptr, 0, nn_vec_.n * sizeof(float4), stream_), "memset");
+  nn_dot_partial_.alloc(256);
+  nn_scalars_.alloc(8);
+  // transpose map of the (symmetric) BSR pattern: entry of (j, i) for every entry (i, j)
+  std::vector<int> tmap(B);
+  for (int i = 0; i < R; ++i)
+    for (int k = host_.row_ptr[i]; k < host_.row_ptr[i + 1]; ++k) {
+      const int j = host_.col_idx[k];
+      auto b0 = host_.col_idx.begin() + host_.row_ptr[j], b1 = host_.col_idx.begin() + host_.row_ptr[j + 1];
+      auto it = std::lower_bound(b0, b1, i);
+      if (it == b1 || *it != i) throw std::invalid_argument("the preconditioner network needs a symmetric pattern");
+      tmap[k] = int(it - host_.col_idx.begin());
+    }
+  nn_transpose_.alloc(B);
+  nn_transpose_.upload(tmap.data(), B, stream_);
+  NnBuffers b{};
+  b.R = R;
+  b.B = B;
+  b.row_ptr = row_ptr_.ptr;
+  b.col_idx = col_idx_.ptr;
+  b.diag_pos = diag_pos_.ptr;
+  b.transpose = nn_transpose_.ptr;
+  b.A = DevBsr{a0_.ptr, a1_.ptr, a2_.ptr};
+  b.feat = nn_feat_.ptr;
+  b.w = nn_w_.ptr;
+  b.h = nn_h_.ptr;
+  b.o = nn_o_.ptr;
+  b.dh = nn_dh_.ptr;
+  b.dx = nn_dx_.ptr;
+  b.partial = nn_partial_.ptr;
+  b.grad = nn_grad_.ptr;
+  sync();
+  nnb_ = b;
+}
+
+void Context::upload_tuple(const float* blocks, const double* rhs, const double* solution) {
+  const int R = host_.R;
+  upload_blocks(blocks);
+  std::vector<float4> v(R);
+  for (int pass = 0; pass < 2; ++pass) {
+    const double* src = pass ? solution : rhs;
+    for (int i = 0; i < R; ++i) v[i] = make_float4(float(src[3 * i]), float(src[3 * i + 1]), float(src[3 * i + 2]), 0.f);
+    check(cudaMemcpyAsync(nn_vec_.ptr + size_t(pass ? kNx : kNb) * R, v.data(), R * sizeof(float4),
+                          cudaMemcpyHostToDevice, stream_), "upload");
+  }
+  sync();
+}
+
+// One V-cycle with the network's smoother S = f S0 on (A, b, x) as separate steps (the cycle kernels with a zero
+// fine smoother give the coarse correction C = P V_1 P^T), the loss ||x - z||_A^2 / ||x||_A^2 and, with
+// `backward`, dL/df through the cycle (g_z = -2 A (x - z) / N; g_y = g_z - A S g_z; g_z1 = g_y - A C g_y) and
+// the network's parameter gradient in nnb_.grad.
+double Context::network_pass(Network& net, bool backward) {
+  const int R = host_.R;
+  auto V = [&](int k) { return nn_vec_.ptr + size_t(k) * R; };
+  const DevBsr A{a0_.ptr, a1_.ptr, a2_.ptr};
+  auto spmv = [&](const float4* x, float4* y) {
+    kcheck(launch_spmv(R, row_ptr_.ptr, col_idx_.ptr, A, x, y, 8, 256, stream_), "spmv");
+  };
+  MgDevice coarse = mg_;
+  coarse.lv[0].S = nn_zero_.ptr;
+  auto C = [&](const float4* v, float4* out) {
+    check(cudaMemcpyAsync(mg_.r[0], v, R * sizeof(float4), cudaMemcpyDeviceToDevice, stream_), "copy");
+    kcheck(mg_apply(coarse, stream_), "coarse correction");
+    check(cudaMemcpyAsync(out, mg_.lv[0].e, R * sizeof(float4), cudaMemcpyDeviceToDevice, stream_), "copy");
+  };
+  // hierarchy with the spectral smoother S0, then S = f S0 from the network
+  mg_setups_since_power_ = 1 << 20;
+  mg_stale_ = true;
+  Network* keep = net_;
+  net_ = nullptr;
+  mg_prepare();
+  net_ = keep;
+  check(cudaMemcpyAsync(nn_s0_.ptr, mg_.lv[0].S, 9 * size_t(R) * sizeof(float), cudaMemcpyDeviceToDevice, stream_),
+        "copy");
+  kcheck(nn_forward(nnb_, net.view(), mg_.omega, mg_.lv[0].S, stream_), "network");
+  const float* S = mg_.lv[0].S;
+  float* fs = nn_fscale_.ptr;
+  check(nn_block_apply(R, S, V(kNb), V(kZ1), stream_), "z1");        // z1 = S b
+  spmv(V(kZ1), V(kT));
+  check(nn_vec(R, V(kNb), V(kT), V(kT), 1.f, -1.f, nullptr, stream_), "t");  // t = b - A z1
+  C(V(kT), V(kC));
+  check(nn_vec(R, V(kZ1), V(kC), V(kY), 1.f, 1.f, nullptr, stream_), "y");    // y = z1 + C t
+  spmv(V(kY), V(kU));
+  check(nn_vec(R, V(kNb), V(kU), V(kU), 1.f, -1.f, nullptr, stream_), "u");   // u = b - A y
+  check(nn_block_apply(R, S, V(kU), V(kZ), stream_), "Su");
+  check(nn_vec(R, V(kY), V(kZ), V(kZ), 1.f, 1.f, nullptr, stream_), "z");     // z = y + S u
+  check(nn_vec(R, V(kNx), V(kZ), V(kE), 1.f, -1.f, nullptr, stream_), "e");   // e = x - z
+  spmv(V(kE), V(kAe));
+  spmv(V(kNx), V(kAx));
+  check(nn_dot(R, V(kNx), V(kAx), nn_dot_partial_.ptr, nn_scalars_.ptr, 0, fs, stream_), "x.Ax");  // fs = -2/N
+  check(nn_dot(R, V(kE), V(kAe), nn_dot_partial_.ptr, nn_scalars_.ptr, 1, nullptr, stream_), "e.Ae");
+  if (backward) {
+    check(nn_vec(R, V(kAe), nullptr, V(kGz), 1.f, 0.f, fs, stream_), "g_z");    // g_z = -2 A e / N
+    check(nn_block_apply(R, S, V(kGz), V(kSg), stream_), "S g_z");
+    spmv(V(kSg), V(kT));
+    check(nn_vec(R, V(kGz), V(kT), V(kGy), 1.f, -1.f, nullptr, stream_), "g_y");  // g_y = g_z - A S g_z
+    C(V(kGy), V(kC));
+    spmv(V(kC), V(kT));
+    check(nn_vec(R, V(kGy), V(kT), V(kGz1), 1.f, -1.f, nullptr, stream_), "g_z1");  // g_z1 = g_y - A C g_y
+    check(nn_dfactor(R, nn_s0_.ptr, V(kGz), V(kU), V(kGz1), V(kNb), nn_dfac_.ptr, stream_), "dL/df");
+    kcheck(nn_backward(nnb_, net.view(), nn_dfac_.ptr, stream_), "network backward");
+  }
+  double sc[2];
+  check(cudaMemcpyAsync(sc, nn_scalars_.ptr, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream_), "read");
+  sync();
+  mg_stale_ = true;  // the hierarchy's fine smoother now holds this tuple's S
+  return sc[0] != 0.0 ? sc[1] / sc[0] : 0.0;
+}
+
+double Context::network_gradient_host(Network& net, const float* blocks, const double* rhs, const double* solution,
+                                      float* grad, float* factors) {
+  ensure_nn_buffers();
+  upload_tuple(blocks, rhs, solution);
+  const double loss = network_pass(net, grad != nullptr);
+  if (grad) check(cudaMemcpyAsync(grad, nn_grad_.ptr, kNnParams * sizeof(float), cudaMemcpyDeviceToHost, stream_),
+                  "download");
+  if (factors) {
+    std::vector<float> o(host_.R);
+    check(cudaMemcpyAsync(o.data(), nn_o_.ptr, host_.R * sizeof(float), cudaMemcpyDeviceToHost, stream_), "download");
+    sync();
+    for (int i = 0; i < host_.R; ++i)
+      factors[i] = 0.5f + kNnFactorSpan / (1.0f + std::exp(-(o[i] + kNnFactorShift)));
+  }
+  sync();
+  return loss;
+}
+
+void Context::network_train_host(Network& net, int tuples, const float* const* blocks, const double* const* rhs,
+                                 const double* const* solutions, int steps, double lr, double* losses) {
+  ensure_nn_buffers();
+  for (int k = 0; k < steps; ++k) {
+    const int t = k % tuples;
+    upload_tuple(blocks[t], rhs[t], solutions[t]);
+    const double loss = network_pass(net, true);
+    if (losses) losses[k] = loss;
+    check(nn_adam(net.view(), nn_grad_.ptr, float(lr), ++net.adam_t, stream_), "adam");
+    sync();
+  }
+}
+
 template struct DeviceArray<double>;
 template struct DeviceArray<int>;
+template struct DeviceArray<unsigned short>;
 template struct DeviceArray<float>;
 template struct DeviceArray<float4>;
 template struct DeviceArray<long long>;

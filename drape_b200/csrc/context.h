@@ -12,6 +12,7 @@
 #include "../../include/drape_b200.h"
 #include "kernels.h"
 #include "mg.h"
+#include "nn.h"
 #include "problem.h"
 
 namespace drape {
@@ -52,6 +53,19 @@ struct AttemptResult {
   int status = 0;  // 0 converged, 1 iteration limit, 2 line search failed, 3 regularisation cap
   bool non_finite = false;
   double max_mu = 0.0;
+};
+
+// The preconditioner network's parameters on one device: f32 master weights, their transposed bf16 copies (the
+// tensor-core operands) and Adam moments. Contexts on that device use it for preconditioner 2 and train it.
+struct Network {
+  int device = 0;
+  DeviceArray<float> master, adam_m, adam_v;
+  DeviceArray<unsigned short> bf16;
+  int adam_t = 0;
+  Network(int device, uint64_t seed);
+  NnWeights view();
+  void set(const float* params);
+  void get(float* params);
 };
 
 class Context {
@@ -100,6 +114,21 @@ class Context {
   void precondition_host(const float* blocks, const double* r, double* z);
   // Level `level`'s grid columns, f64 Galerkin stencil [225][rows] (level >= 1) and smoother [9][rows].
   int multilevel_view(int level, double* op, float* smoother);
+
+  // ---- preconditioner network
+  void attach_network(Network* net) { net_ = net; mg_stale_ = true; }
+  // The preconditioner or its damping may have changed: rebuild the hierarchy's smoothers before the next use.
+  void options_changed() {
+    mg_stale_ = true;
+    mg_setups_since_power_ = 1 << 20;
+  }
+  // Loss ||x - M b||_A^2 / ||x||_A^2 of one V-cycle with the network's smoother on one (blocks, b, x) tuple, its
+  // parameter gradient (kNnParams, may be null) and the smoother factors f (R, may be null).
+  double network_gradient_host(Network& net, const float* blocks, const double* rhs, const double* solution,
+                               float* grad, float* factors);
+  // Adam on the tuples: `steps` steps, each over one tuple in turn; losses[k] of step k (before its update).
+  void network_train_host(Network& net, int tuples, const float* const* blocks, const double* const* rhs,
+                          const double* const* solutions, int steps, double lr, double* losses);
 
   std::string last_error;
 
@@ -172,6 +201,18 @@ class Context {
   cudaGraphExec_t mg_graph_ = nullptr;
   int mg_graph_launches_ = 0;
   bool mg_graph_pdl_ = false;
+
+  // preconditioner network (attached, not owned) and its per-row buffers
+  Network* net_ = nullptr;
+  NnBuffers nnb_{};
+  DeviceArray<float> nn_feat_, nn_w_, nn_h_, nn_o_, nn_dh_, nn_dx_, nn_partial_, nn_grad_, nn_dfac_, nn_s0_, nn_zero_,
+      nn_fscale_;
+  DeviceArray<int> nn_transpose_;
+  DeviceArray<float4> nn_vec_;
+  DeviceArray<double> nn_dot_partial_, nn_scalars_;
+  void ensure_nn_buffers();
+  double network_pass(Network& net, bool backward);
+  void upload_tuple(const float* blocks, const double* rhs, const double* solution);
 
   // static problem arrays
   DeviceArray<double> geom_, hinge_k_, unit_mass_, colliders_;

@@ -1,0 +1,86 @@
+// The preconditioner network: a mesh message-passing network that predicts, per fine-level row, a factor on the
+// multilevel preconditioner's Jacobi smoother (S_i = f_i omega D_i^{-1}, f_i in (0.5, 1.135)). It has no
+// counterpart in the reference. Trained on (matrix, right-hand side, PCG solution) tuples of drape solves to
+// minimise the A-norm error of one V-cycle; the flexible PCG around it (block Jacobi as fallback) decides
+// convergence on its own residual, so the converged state never depends on the network.
+//
+// Architecture (hidden width 64, BF16 weights, FP32 accumulation):
+//   h0 = relu(W_in^T x + b_in)                       x: 16 features per row (nn_features_kernel)
+//   h_l = relu(W_l^T [h_{l-1}, m_{l-1}] + b_l)      m_i = sum_{j != i} w_ij h_j, w_ij = |A_ij|_F / sum_k |A_ik|_F
+//   o = w_o . h_4 + b_o,  f = 0.5 + 0.635 sigmoid(o + 1.3093)   l = 1..4
+// Dense layers run as mma.sync m16n8k16 bf16 tiles with f32 accumulators (inputs and weights rounded to bf16);
+// the training backward pass runs in f32 on CUDA cores.
+//
+// Parameter layout (one f32 array, row k = input, column n = output unit):
+//   W_in [16][64] | b_in [64] | 4 x (W_l [128][64] | b_l [64]) | w_o [64] | b_o [1]
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "device_problem.h"
+
+namespace drape {
+
+constexpr int kNnIn = 16, kNnHidden = 64, kNnLayers = 4;
+constexpr int kNnOffWin = 0, kNnOffBin = kNnIn * kNnHidden;
+constexpr int kNnLayerSize = 2 * kNnHidden * kNnHidden + kNnHidden;
+constexpr int kNnOffLayer0 = kNnOffBin + kNnHidden;
+constexpr int kNnOffWo = kNnOffLayer0 + kNnLayers * kNnLayerSize;
+constexpr int kNnOffBo = kNnOffWo + kNnHidden;
+constexpr int kNnParams = kNnOffBo + 1;  // 34,177
+constexpr int kNnBf16 = kNnIn * kNnHidden + kNnLayers * 2 * kNnHidden * kNnHidden;  // transposed bf16 weights
+constexpr int kNnRowsPerCta = 64;       // forward layer tile (4 warps x 16 rows)
+constexpr int kNnBackRows = 32;         // backward tile
+// Smoother factor f = 0.5 + kNnFactorSpan sigmoid(o + kNnFactorShift): f(0) = 1 and f < 1.135, so f omega_0 stays
+// below 2 / lambda_0 (omega_0 = 2 / (1.1 lambda_0 (1 + 1/30))): the learned smoother cannot turn unstable.
+constexpr float kNnFactorSpan = 0.635f;
+constexpr float kNnFactorShift = 1.3093333f;  // ln(0.5 / (kNnFactorSpan - 0.5))
+
+// Device buffers of one network evaluation / training pass over R rows and B blocks (owned by the caller).
+struct NnBuffers {
+  int R, B;
+  const int* row_ptr;
+  const int* col_idx;
+  const int* diag_pos;
+  const int* transpose;  // [B] index of block (j, i) for block (i, j)
+  DevBsr A;
+  float* feat;    // [R][16]
+  float* w;       // [B] aggregation weights (0 on the diagonal)
+  float* h;       // [5][R][64] activations h0..h4
+  float* o;       // [R] output before the sigmoid
+  float* dh;      // [2][R][64] backward ping-pong
+  float* dx;      // [R][128]
+  float* partial; // [ctas][kNnParams] per-CTA gradient partials (backward)
+  float* grad;    // [kNnParams]
+};
+
+struct NnWeights {
+  float* master;              // [kNnParams] f32
+  __nv_bfloat16* bf16;        // [kNnBf16] transposed: Wt_in [64][16] | Wt_l [64][128] per layer
+  float* adam_m;
+  float* adam_v;
+};
+
+int nn_back_ctas(int R);
+// Features, aggregation weights and the forward pass; f_i (0.5 + sigmoid) scales level-0 smoother rows S [9][R].
+cudaError_t nn_forward(const NnBuffers& b, const NnWeights& w, const float* omega0, float* S, cudaStream_t s);
+// Backward from dL/df_i (dfactor [R]) into b.grad (overwritten).
+cudaError_t nn_backward(const NnBuffers& b, const NnWeights& w, const float* dfactor, cudaStream_t s);
+// One Adam step (lr, beta1 0.9, beta2 0.999, eps 1e-8, step t >= 1), then the bf16 copies.
+cudaError_t nn_adam(const NnWeights& w, const float* grad, float lr, int t, cudaStream_t s);
+cudaError_t nn_refresh_bf16(const NnWeights& w, cudaStream_t s);
+
+// Training vector operations on float4 rows.
+// out = scale (a x + b y)  (y may be null; scale a device f32, null for 1)
+cudaError_t nn_vec(int R, const float4* x, const float4* y, float4* out, float a, float b, const float* scale,
+                   cudaStream_t s);
+// out_i = S_i v_i, S [9][R]
+cudaError_t nn_block_apply(int R, const float* S, const float4* v, float4* out, cudaStream_t s);
+// scalars[slot] = x . y (f64, fixed-order reduction over 148 CTA partials); fscale (if given) = -2 / (x . y)
+cudaError_t nn_dot(int R, const float4* x, const float4* y, double* partial, double* scalars, int slot, float* fscale,
+                   cudaStream_t s);
+// dL/df_i from the gradients at the post- and pre-smoothing outputs
+cudaError_t nn_dfactor(int R, const float* S0, const float4* g_post, const float4* u, const float4* g_pre,
+                       const float4* b, float* dfac, cudaStream_t s);
+
+}  // namespace drape

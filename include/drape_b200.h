@@ -202,6 +202,34 @@ drape_status drape_time_multilevel(drape_ctx* ctx, int32_t iterations, float* ou
  * zeroes the counters. */
 drape_status drape_pcg_profile(drape_ctx* ctx, int64_t* out7, int32_t clear);
 
+/* The preconditioner network (no counterpart in the reference): a 4-layer mesh message-passing network (hidden
+ * width 64, BF16 weights, FP32 accumulation) that predicts, per fine-level row, a factor f in (0.5, 1.135) on the
+ * multilevel preconditioner's Jacobi smoother; options.preconditioner = 2 uses the network attached to the
+ * context. Parameters: DRAPE_NETWORK_PARAMETERS f32 values, layout W_in[16][64] b_in[64], 4 x (W[128][64] b[64]),
+ * w_out[64] b_out. The file format is "DRAPENN1", an int32 count, then the f32 values (little-endian). */
+#define DRAPE_NETWORK_PARAMETERS 34177
+typedef struct drape_network drape_network;
+/* Glorot-uniform weights from `seed`, zero biases and a zero output layer (f = 1: the untrained network gives
+ * the multilevel preconditioner's spectral smoother). */
+drape_status drape_network_create(int32_t device, uint64_t seed, drape_network** out);
+void drape_network_destroy(drape_network* net);
+drape_status drape_network_load(drape_network* net, const char* path);
+drape_status drape_network_save(drape_network* net, const char* path);
+/* get (may be NULL) receives the parameters; set (may be NULL) replaces them (and clears the Adam moments). */
+drape_status drape_network_parameters(drape_network* net, float* get, const float* set);
+/* Attach (NULL: detach) the network the context's preconditioner 2 uses; the context does not own it. */
+drape_status drape_set_network(drape_ctx* ctx, drape_network* net);
+/* Loss ||x - M b||_A^2 / ||x||_A^2 of one V-cycle M with the network's smoother on one tuple (blocks 9B f32,
+ * rhs b and solution x 3R f64, A x = b), the gradient of the loss (DRAPE_NETWORK_PARAMETERS, may be NULL) and the
+ * factors f (R, may be NULL). */
+drape_status drape_network_gradient(drape_ctx* ctx, drape_network* net, const float* blocks, const double* rhs,
+                                    const double* solution, double* loss, float* grad, float* factors);
+/* Trains on `tuples` tuples of this context's pattern: `steps` Adam steps (learning rate lr), step k on tuple
+ * k % tuples; losses[k] (may be NULL) is step k's loss before its update. */
+drape_status drape_network_train(drape_ctx* ctx, drape_network* net, int32_t tuples, const float* const* blocks,
+                                 const double* const* rhs, const double* const* solutions, int32_t steps, double lr,
+                                 double* losses);
+
 /* Block-Jacobi PCG that allocates nothing, for callers that cannot call cudaMalloc: applications whose device
  * memory all comes from their own pool, or that must not enter the driver's allocator once they are running.
  * This entry point has no counterpart in the reference; it is the persistent PCG of drape_pcg with its work space

@@ -1,0 +1,111 @@
+"""The preconditioner network on the GPU against its numpy oracle (tests/network_ref.py), its training, and full
+solves with the learned preconditioner (needs a B200).
+
+Tolerances: both sides round the dense layers' operands to bf16; the device accumulates in f32 and runs the
+V-cycle in f32, the oracle in f64: factors within 2e-3, the loss within 2e-3 relative, the parameter gradient
+within 2e-2 relative L2.
+"""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+import scipy.sparse.linalg as spla
+
+from drape_b200 import api
+from tests import multilevel_ref as ml
+from tests import network_ref as nr
+from tests import oracle_py
+
+pytestmark = pytest.mark.gpu
+
+
+def _tuple(d, n, seed):
+    """(blocks, b, x) of the projected (SPD) PTC system at the drape's current state; x solved in f64."""
+    log_h = d.final_h()
+    x = d.state
+    x_hat = x + log_h * log_h * np.tile([0.0, -9.81, 0.0], d.V)
+    d.set_options(api.default_options(tangent=1))
+    g, blocks = d.assemble(x, x_hat=x_hat, h=log_h, mode=0, curvature=False)
+    d.set_options(api.default_options())
+    rp, ci = oracle_py.Scene("sheet", n, seed=seed, plane=True).pattern()
+    A = ml.bsr_matrix(rp, ci, blocks)
+    b = -g
+    return blocks, b, spla.spsolve(A.tocsc(), b), rp, ci
+
+
+def _drape_at(n, steps, seed=0):
+    d = api.Drape.sheet(n, seed=seed, plane=True, options=api.default_options(max_steps=steps))
+    d.solve_equilibrium(check=False)
+    return d
+
+
+def test_network_gradient_matches_the_oracle():
+    d = _drape_at(17, 10)
+    blocks, b, x, rp, ci = _tuple(d, 17, 0)
+    net = api.Network(seed=1)
+    p = nr.init_params(7, scale_out=0.5)
+    net.parameters = p
+    loss, grad, fac = net.gradient(d, blocks, b, x)
+    L, g, f = nr.network_loss(p.astype(np.float64), rp, ci, blocks, 17, b, x, bf=True)
+    assert np.ptp(f) > 1e-2
+    assert np.abs(fac - f).max() <= 2e-3, np.abs(fac - f).max()
+    assert abs(loss - L) <= 2e-3 * L, (loss, L)
+    assert np.linalg.norm(grad - g) <= 2e-2 * np.linalg.norm(g), np.linalg.norm(grad - g) / np.linalg.norm(g)
+
+
+def test_untrained_network_leaves_the_spectral_smoother():
+    d = _drape_at(17, 10)
+    blocks, b, x, _, _ = _tuple(d, 17, 0)
+    net = api.Network(seed=5)
+    _, _, fac = net.gradient(d, blocks, b, x)
+    assert np.abs(fac - 1.0).max() <= 1e-6
+
+
+def test_training_lowers_the_vcycle_error():
+    """Adam on the GPU lowers the one-cycle A-norm error on random error probes e (b = A e) of three PTC systems
+    (the probes carry the high-frequency error the fine smoother acts on)."""
+    d = _drape_at(17, 5)
+    rng = np.random.default_rng(4)
+    tuples = []
+    for extra in (0, 10, 25):
+        if extra:
+            d.set_options(api.default_options(max_steps=extra))
+            d.solve_equilibrium(start=d.state, h0=d.final_h(), check=False)
+        blocks, _, _, rp, ci = _tuple(d, 17, 0)
+        A = ml.bsr_matrix(rp, ci, blocks)
+        for _ in range(2):
+            e = rng.standard_normal(A.shape[0])
+            tuples.append((blocks, A @ e, e))
+    net = api.Network(seed=2)
+    before = [net.gradient(d, *t)[0] for t in tuples]
+    net.train(d, tuples, steps=120, lr=3e-3)
+    after = [net.gradient(d, *t)[0] for t in tuples]
+    assert np.mean(after) < 0.95 * np.mean(before), (before, after)
+
+
+def test_network_file_round_trip():
+    net = api.Network(seed=3)
+    p = nr.init_params(11, scale_out=0.3)
+    net.parameters = p
+    with tempfile.TemporaryDirectory() as t:
+        path = os.path.join(t, "net.bin")
+        net.save(path)
+        other = api.Network(seed=4, path=path)
+        assert np.array_equal(other.parameters, p)
+
+
+@pytest.mark.parametrize("n", [17, 33])
+def test_learned_preconditioner_solve_reaches_an_f64_equilibrium(n):
+    """With the learned smoother (the shipped weights when present) the drape lands on an f64 equilibrium within
+    1e-4 m, as with block Jacobi: the converged state does not depend on the network."""
+    from tests.test_gpu_parity import _polished_error
+    net = api.Network.trained() if os.path.exists(api.NETWORK_FILE) else api.Network(seed=0)
+    gpu = api.Drape.sheet(n, seed=0, plane=True,
+                          options=api.default_options(equilibrium_absolute=1e-7, preconditioner=2))
+    gpu.set_network(net)
+    log = gpu.solve_equilibrium()
+    assert log["reason"] == "tolerance" and log["final_residual"] <= 1e-7, log
+    oracle = oracle_py.Scene("sheet", n, seed=0, plane=True)
+    err, e_rel, r64 = _polished_error(oracle, gpu.state)
+    assert r64 <= 1.01e-7 and err <= 1e-4 and e_rel <= 1e-9, (r64, err, e_rel)
