@@ -3,8 +3,11 @@
 Workload: the 1.0 m sheet of n x n vertices (default n = 129: 16641 vertices, 32768 triangles, 48896 hinges,
 180993 BSR blocks) over a sphere of radius 0.25 m and a ground plane at y = -0.25 m, isotropic StVK E = 5e5 Pa,
 nu = 0.3, t = 5e-4 m, k_b = 1e-5 N m, IPC d_hat = 2e-3 m, kappa = 1e3; PTC from dt0 = 1e-3 s to
-|grad E_s| <= 1e-6 N with block-Jacobi PCG (rtol 1e-6, <= 2000 iterations). One step = one full cold solve to
-the converged state. Synthetic scene (the reference ships no dataset; seeded jitter, seed 0).
+|grad E_s| <= 1e-6 N, PCG rtol 1e-6, <= 2000 iterations. One step = one full cold solve to the converged state.
+Direction solver (--preconditioner): learned (default: the multilevel V-cycle flexible PCG with the shipped
+network's fine smoother), multilevel (spectral Jacobi smoothing), jacobi (the reference's block-Jacobi PCG).
+--compare adds one device-timed solve with each of the other two on the same workload (the learned-vs-Jacobi
+comparison of the metric). Synthetic scene (the reference ships no dataset; seeded jitter, seed 0).
 
 value: seconds per converged solve with the problem resident in HBM (CUDA-event-timed solve, max over ranks).
 e2e:   the same through the C ABI from host arrays: drape_create (host->device copies) + solve + drape_get_state
@@ -95,6 +98,18 @@ def flush_l2(torch, device):
     del buf
 
 
+def multilevel_bytes_per_iteration(n, R, B):
+    """Algorithmic bytes of one multilevel flexible PCG iteration: the fine matrix read three times (pre-smoothing
+    residual in the restriction, post-smoothing residual, the direction SpMV: 40 B per block + 28 B per row each),
+    each coarse level's 5 x 5 stencil of 48-byte blocks read twice (restriction, prolongation), and the level-0
+    vectors of the direction and update steps (x, r, p, q, z: 100 B per row)."""
+    total = 3 * (40 * B + 28 * R) + 100 * R
+    while n > 5 and (n - 1) % 2 == 0:
+        n = (n - 1) // 2 + 1
+        total += 2 * (25 * 48 + 48) * n * n
+    return total
+
+
 PRECOND = {"jacobi": "block-Jacobi PCG", "multilevel": "multilevel V-cycle flexible PCG (omega-Jacobi smoothing)",
            "learned": "multilevel V-cycle flexible PCG with the network-predicted fine smoother"}
 
@@ -116,8 +131,11 @@ def run_gpu(args):
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    precond = {"jacobi": 0, "multilevel": 1, "learned": 2}[args.preconditioner]
-    opts = api.default_options(pcg_max_iterations=args.pcg_max, max_steps=args.max_steps, preconditioner=precond)
+    def options_for(name):
+        return api.default_options(pcg_max_iterations=args.pcg_max, max_steps=args.max_steps,
+                                   preconditioner={"jacobi": 0, "multilevel": 1, "learned": 2}[name])
+
+    net = api.Network.trained(device=local) if args.preconditioner == "learned" or args.compare else None
     # Host arrays for the end-to-end leg (built outside every timed region).
     pdir = tempfile.mkdtemp(prefix="drape_bench_")
     api.write_sheet_problem(pdir, args.n, seed=args.seed, plane=bool(args.plane))
@@ -137,14 +155,16 @@ def run_gpu(args):
         if dist:
             dist.barrier()
 
-    def one_step():
+    def one_step(name=args.preconditioner):
         """One step through the public C ABI from host buffers: drape_create (host->device copies of the problem),
         the solve (timed on the device with CUDA events on the library's stream, bracketed by a synchronize), and
         drape_get_state (device->host copy of the converged positions)."""
         flush_l2(torch, local)
         barrier()
         t0 = time.perf_counter()
-        drape = api.Drape.from_arrays(**host, options=opts, device=local)
+        drape = api.Drape.from_arrays(**host, options=options_for(name), device=local)
+        if name == "learned":
+            drape.set_network(net)
         torch.cuda.synchronize()
         log = drape.solve_equilibrium(check=False)
         state = drape.state
@@ -173,17 +193,34 @@ def run_gpu(args):
         t, t_e2e = v.tolist()
     last = logs[-1]
     R, B = int(meta["rows"]), int(meta["blocks"])
-    bytes_per_iter = 40 * B + 196 * R
     pk = peaks()
-    achieved = (bytes_per_iter * last["pcg_iterations"]) / (last["ms_pcg"] / 1e3) / 1e9 if last["ms_pcg"] > 0 else 0.0
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "pcg_traffic.json")
-    if os.path.exists(tpath):
-        tr = json.load(open(tpath))
-        if tr.get("columns") == args.n:
-            # One launch stages the matrix into shared memory once: its DRAM traffic is per launch, not per
-            # iteration (ncu capture summarised in profiles/pcg_kernel_n129.md).
-            traffic = tr["dram_bytes_per_launch"]
+    if args.preconditioner == "jacobi":
+        kernel = "pcg_kernel (persistent block-Jacobi PCG)"
+        bytes_per_iter = 40 * B + 196 * R
+        tpath = os.path.join(ROOT, "profiles", "pcg_traffic.json")
+        if os.path.exists(tpath):
+            tr = json.load(open(tpath))
+            if tr.get("columns") == args.n:
+                # One launch stages the matrix into shared memory once: its DRAM traffic is per launch, not per
+                # iteration (ncu capture summarised in profiles/pcg_kernel_n129.md).
+                traffic = tr["dram_bytes_per_launch"]
+    else:
+        kernel = "multilevel flexible PCG iteration (restrict/tail/prolong/direction/update kernels, one graph)"
+        bytes_per_iter = multilevel_bytes_per_iteration(args.n, R, B)
+    achieved = (bytes_per_iter * last["pcg_iterations"]) / (last["ms_pcg"] / 1e3) / 1e9 if last["ms_pcg"] > 0 else 0.0
+    comparison = {}
+    if args.compare:
+        for other in ("jacobi", "multilevel", "learned"):
+            if other == args.preconditioner:
+                continue
+            log_o, s_o, _, _ = one_step(other)
+            comparison[other] = {"seconds": s_o, "ptc_steps": log_o["ptc_steps"],
+                                 "newton_iterations": log_o["newton_iterations"],
+                                 "pcg_iterations": log_o["pcg_iterations"],
+                                 "pcg_per_newton": log_o["pcg_iterations"] / max(1, log_o["newton_iterations"]),
+                                 "fallbacks_to_jacobi": log_o["fallbacks"], "converged": log_o["reason"] == "tolerance",
+                                 "final_residual_N": log_o["final_residual"]}
     out = {
         "metric": METRIC, "value": t, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -201,7 +238,7 @@ def run_gpu(args):
                   "phase_ms": {k: last[k] for k in ("ms_assembly", "ms_pcg", "ms_line_search", "ms_ccd", "ms_other")}},
         "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(sum(l["kernel_launches"] for l in logs)),
-        "roofline": {"bound": "hbm", "kernel": "pcg_kernel (persistent block-Jacobi PCG)", "achieved": achieved,
+        "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved,
                      "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
                      "traffic": traffic, "peak_source": "fallback" if pk.get("_fallback") else "measured",
                      "algorithmic_bytes_per_pcg_iteration": bytes_per_iter,
@@ -209,6 +246,9 @@ def run_gpu(args):
                      "avg_launch_ms": last["ms_pcg"] / max(1, last["pcg_launches"])},
         "clocks": clocks,
     }
+    if comparison:
+        comparison["this_run"] = args.preconditioner
+        out["comparison"] = comparison
     if rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args, last)
     if dist:
@@ -285,7 +325,8 @@ def main():
     ap.add_argument("--max-steps", type=int, default=1000)
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--preconditioner", default="jacobi", choices=["jacobi", "multilevel", "learned"])
+    ap.add_argument("--preconditioner", default="learned", choices=["jacobi", "multilevel", "learned"])
+    ap.add_argument("--compare", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
