@@ -355,6 +355,24 @@ def _host_call(st):
         raise DrapeError(st, load().drape_last_error(None).decode())
 
 
+def spmv_benchmark(row_ptr, col_idx, values, x, launches=20, lanes_per_row=8, threads=256, device=0, result=False):
+    """Device ms per launch of the BSR(3x3) SpMV on the given matrix (and y = A x if `result`)."""
+    lib = load()
+    lib.drape_spmv_benchmark.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int64, P, P, P, P, ctypes.c_int32,
+                                         ctypes.c_int32, ctypes.c_int32, P, P]
+    rp = np.ascontiguousarray(row_ptr, np.int32)
+    ci = np.ascontiguousarray(col_idx, np.int32)
+    vals = np.ascontiguousarray(values, np.float32)
+    xx = np.ascontiguousarray(x, np.float32)
+    y = np.zeros(3 * (len(rp) - 1), np.float32) if result else None
+    ms = ctypes.c_float()
+    st = lib.drape_spmv_benchmark(device, len(rp) - 1, len(ci), _ptr(rp), _ptr(ci), _ptr(vals), _ptr(xx), launches,
+                                  lanes_per_row, threads, _ptr(y), ctypes.byref(ms))
+    if st != 0:
+        raise DrapeError(st, lib.drape_last_error(None).decode())
+    return (ms.value, y) if result else ms.value
+
+
 NETWORK_PARAMETERS = 34177
 NETWORK_FILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "preconditioner_network.bin")
 

@@ -377,6 +377,78 @@ drape_status drape_network_train(drape_ctx* ctx, drape_network* net, int32_t tup
   });
 }
 
+drape_status drape_spmv_benchmark(int32_t device, int32_t rows, int64_t blocks, const int32_t* row_ptr,
+                                  const int32_t* col_idx, const float* values, const float* x, int32_t launches,
+                                  int32_t lanes_per_row, int32_t threads, float* y, float* ms) {
+  if (rows < 1 || blocks < 1 || !row_ptr || !col_idx || !values || !x || !ms || launches < 1 ||
+      (lanes_per_row != 4 && lanes_per_row != 8 && lanes_per_row != 16 && lanes_per_row != 32) ||
+      threads < lanes_per_row || threads > 256 || threads % 32)
+    return fail(nullptr, "invalid SpMV benchmark arguments", DRAPE_E_ARG);
+  if (row_ptr[0] != 0 || row_ptr[rows] != blocks) return fail(nullptr, "row_ptr does not span the blocks", DRAPE_E_ARG);
+  for (int64_t k = 0; k < blocks; ++k)
+    if (col_idx[k] < 0 || col_idx[k] >= rows) return fail(nullptr, "column index out of range", DRAPE_E_ARG);
+  try {
+    drape::check(cudaSetDevice(device), "cudaSetDevice");
+    std::vector<float4> h0(blocks), h1(blocks), hx(rows);
+    std::vector<float> h2(blocks);
+    for (int64_t k = 0; k < blocks; ++k) {
+      const float* v = values + 9 * k;
+      h0[k] = make_float4(v[0], v[1], v[2], v[3]);
+      h1[k] = make_float4(v[4], v[5], v[6], v[7]);
+      h2[k] = v[8];
+    }
+    for (int r = 0; r < rows; ++r) hx[r] = make_float4(x[3 * r], x[3 * r + 1], x[3 * r + 2], 0.0f);
+    drape::DeviceArray<int> d_rp, d_ci;
+    drape::DeviceArray<float4> d_a0, d_a1, d_x, d_y;
+    drape::DeviceArray<float> d_a2;
+    d_rp.alloc(rows + 1);
+    d_ci.alloc(blocks);
+    d_a0.alloc(blocks);
+    d_a1.alloc(blocks);
+    d_a2.alloc(blocks);
+    d_x.alloc(rows);
+    d_y.alloc(rows);
+    d_rp.upload(row_ptr, rows + 1, nullptr);
+    d_ci.upload(col_idx, blocks, nullptr);
+    d_a0.upload(h0.data(), blocks, nullptr);
+    d_a1.upload(h1.data(), blocks, nullptr);
+    d_a2.upload(h2.data(), blocks, nullptr);
+    d_x.upload(hx.data(), rows, nullptr);
+    const drape::DevBsr A{d_a0.ptr, d_a1.ptr, d_a2.ptr};
+    cudaEvent_t e0, e1;
+    drape::check(cudaEventCreate(&e0), "event");
+    drape::check(cudaEventCreate(&e1), "event");
+    for (int k = 0; k < 3; ++k)
+      drape::check(drape::launch_spmv(rows, d_rp.ptr, d_ci.ptr, A, d_x.ptr, d_y.ptr, lanes_per_row, threads, nullptr),
+                   "spmv");
+    drape::check(cudaEventRecord(e0), "event");
+    for (int k = 0; k < launches; ++k)
+      drape::check(drape::launch_spmv(rows, d_rp.ptr, d_ci.ptr, A, d_x.ptr, d_y.ptr, lanes_per_row, threads, nullptr),
+                   "spmv");
+    drape::check(cudaEventRecord(e1), "event");
+    drape::check(cudaEventSynchronize(e1), "synchronize");
+    float t = 0.0f;
+    cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = t / launches;
+    if (y) {
+      d_y.download(hx.data(), rows, nullptr);
+      drape::check(cudaDeviceSynchronize(), "synchronize");
+      for (int r = 0; r < rows; ++r) {
+        y[3 * r] = hx[r].x;
+        y[3 * r + 1] = hx[r].y;
+        y[3 * r + 2] = hx[r].z;
+      }
+    }
+    return DRAPE_OK;
+  } catch (const drape::CudaError& e) {
+    return fail(nullptr, e.what(), DRAPE_E_CUDA);
+  } catch (const std::exception& e) {
+    return fail(nullptr, e.what(), DRAPE_E_ARG);
+  }
+}
+
 drape_status drape_precondition(drape_ctx* ctx, const float* blocks, const double* r, double* z) {
   return guarded(ctx, [&](drape::Context& c) {
     if (!r || !z) return fail(ctx, "invalid arguments", DRAPE_E_ARG);

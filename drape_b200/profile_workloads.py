@@ -2,6 +2,13 @@
 
     python -m drape_b200.profile_workloads cycle   [--n 129] [--steps 20]   # multilevel V-cycle and PCG iteration
     python -m drape_b200.profile_workloads network [--n 129] [--steps 20]   # preconditioner network forward
+    python -m drape_b200.profile_workloads spmv    [--drapes 128]          # batched and n257 BSR SpMV, autotuned
+
+spmv builds the batched configuration: `drapes` sheets with n drawn from {33, 49, 65, 97, 129}, sphere radius
+U(0.15, 0.35) m, E log-uniform in [1e5, 2e6] Pa (master seed 7), each assembled on the GPU at its start state
+(h = 1e-2 s), concatenated block-diagonally; and the single n257 sheet's matrix. For each it times every
+lanes-per-row x threads shape of the SpMV kernel, keeps the fastest, checks its y against numpy (f64 of the same
+f32 blocks) and reports algorithmic GB/s (40 B per block + 28 B per row) against the measured HBM peak.
 
 Both drive `steps` PTC steps of the n x n sheet drape (sphere + ground plane) with the multilevel preconditioner,
 assemble the projected (SPD) PTC system at that state, and then:
@@ -30,12 +37,80 @@ def system(n, steps):
     return d, blocks, -g
 
 
+def sheet_matrix(n, seed, radius, young):
+    """(row_ptr, col_idx, 9B f32 blocks) of the sheet drape's PTC system at its start state (h = 1e-2 s)."""
+    import tempfile
+    d = api.Drape.sheet(n, seed=seed, radius=radius, young=young, plane=True)
+    x = d.state
+    h = 1e-2
+    _, blocks = d.assemble(x, x_hat=x + h * h * np.tile(GRAVITY, d.V), h=h, mode=0)
+    with tempfile.TemporaryDirectory() as t:
+        api.write_sheet_problem(t, n, seed=seed, radius=radius, young=young, plane=True)
+        _, arr = api.read_problem_arrays(t)
+    d.close()
+    return arr["row_ptr"].astype(np.int64), arr["col_idx"].astype(np.int64), blocks
+
+
+def spmv_workload(drapes):
+    import json as _json
+    import os
+    rng = np.random.default_rng(7)
+    parts, offset = [], 0
+    sizes = []
+    for _ in range(drapes):
+        n = int(rng.choice([33, 49, 65, 97, 129]))
+        rp, ci, blk = sheet_matrix(n, int(rng.integers(1, 1 << 30)), float(rng.uniform(0.15, 0.35)),
+                                   float(np.exp(rng.uniform(np.log(1e5), np.log(2e6)))))
+        parts.append((rp, ci + offset, blk))
+        offset += len(rp) - 1
+        sizes.append(n)
+    rp_all = [np.zeros(1, np.int64)]
+    base = 0
+    for rp, _, _ in parts:
+        rp_all.append(rp[1:] + base)
+        base += rp[-1]
+    batch = (np.concatenate(rp_all), np.concatenate([p[1] for p in parts]), np.concatenate([p[2] for p in parts]))
+    single = sheet_matrix(257, 0, 0.25, 5e5)
+    try:
+        peak = _json.load(open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                                            "MEASURED_PEAKS.json")))["hbm_gbs"]
+    except Exception:
+        peak = 6650.0
+    out = {}
+    for name, (rp, ci, blk) in (("batched", batch), ("n257", single)):
+        R, B = len(rp) - 1, len(ci)
+        x = np.random.default_rng(1).standard_normal(3 * R).astype(np.float32)
+        shapes = {}
+        for lanes in (4, 8, 16, 32):
+            for threads in (128, 256):
+                shapes[f"{lanes}x{threads}"] = api.spmv_benchmark(rp, ci, blk, x, 20, lanes, threads)
+        best = min(shapes, key=shapes.get)
+        lanes, threads = (int(v) for v in best.split("x"))
+        ms, y = api.spmv_benchmark(rp, ci, blk, x, 20, lanes, threads, result=True)
+        Bm = blk.reshape(-1, 3, 3).astype(np.float64)
+        rows = np.repeat(np.arange(R), np.diff(rp))
+        ref = np.zeros((R, 3))
+        np.add.at(ref, rows, np.einsum("kab,kb->ka", Bm, x.reshape(-1, 3).astype(np.float64)[ci]))
+        err = float(np.linalg.norm(y - ref.reshape(-1)) / np.linalg.norm(ref))
+        bytes_ = 40 * B + 28 * R
+        out[name] = {"rows": R, "blocks": B, "algorithmic_MB": bytes_ / 1e6, "best_shape": best, "ms": ms,
+                     "GB_per_s": bytes_ / (ms * 1e-3) / 1e9, "fraction_of_peak": bytes_ / (ms * 1e-3) / 1e9 / peak,
+                     "peak_GB_per_s": peak, "relative_error_vs_numpy": err, "all_shapes_ms": shapes}
+    out["batched"]["drapes"] = drapes
+    out["batched"]["columns_histogram"] = {str(n): sizes.count(n) for n in sorted(set(sizes))}
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("workload", choices=["cycle", "network"])
+    ap.add_argument("workload", choices=["cycle", "network", "spmv"])
     ap.add_argument("--n", type=int, default=129)
     ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--drapes", type=int, default=128)
     args = ap.parse_args(argv)
+    if args.workload == "spmv":
+        print(json.dumps(spmv_workload(args.drapes)), flush=True)
+        return 0
     d, blocks, b = system(args.n, args.steps)
     lib = api.load()
     out = {"workload": args.workload, "columns": args.n, "ptc_steps": args.steps}

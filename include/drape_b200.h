@@ -193,6 +193,14 @@ drape_status drape_multilevel_view(drape_ctx* ctx, int32_t level, int32_t* colum
  * assembled matrix (lanes per row 4/8/16/32) and of the row assembly at the current state. */
 drape_status drape_time_spmv(drape_ctx* ctx, int32_t launches, int32_t lanes_per_row, int32_t threads, float* ms);
 drape_status drape_time_assembly(drape_ctx* ctx, int32_t launches, float* ms);
+/* Stand-alone BSR(3x3) SpMV y = A x on any matrix given by host arrays (row_ptr [rows+1], col_idx [blocks],
+ * values [9 blocks] f32 row-major, x [3 rows]), e.g. the block-diagonal concatenation of many drapes (the batched
+ * configuration, per-instance row offsets folded into col_idx): uploads, runs 3 warm-up and `launches` timed
+ * launches of the lanes_per_row (4/8/16/32) x threads (<= 256) kernel shape, *ms = device ms per launch, y
+ * (3 rows, may be NULL) = the result. No counterpart in the reference (its SpMV is spmv_dot.wgsl). */
+drape_status drape_spmv_benchmark(int32_t device, int32_t rows, int64_t blocks, const int32_t* row_ptr,
+                                  const int32_t* col_idx, const float* values, const float* x, int32_t launches,
+                                  int32_t lanes_per_row, int32_t threads, float* y, float* ms);
 /* Multilevel timings on the last assembled matrix and right-hand side: out3 = [ms per stand-alone V-cycle,
  * ms per flexible PCG iteration inside the solve graph (exactly `iterations` iterations), 1 if the graph's kernels
  * are linked by programmatic dependent launch]. */
