@@ -1,0 +1,273 @@
+// `drape`: the GPU stage of the run-e*.sh pipeline as one command, in place of `node src/node/run-e7.ts` (its
+// flags: engine/gpu/src/node/run-e7.ts:37-43; its outputs: run-e7.ts:93-107, state-files.ts).
+//
+//   drape --case <dir> [--mode cold|warm|prolong] [--start <state prefix>]
+//         [--preconditioner jacobi|multilevel|learned] [--network <weights file>] [--device <n>]
+//   environment: E7_BUDGET_S (time budget of the solve, s), E7_PROGRESS (one stderr line per accepted step)
+//
+// Reads <dir>/problem.json + problem.bin (`oracle e7-generate`), solves to equilibrium with the rules of the
+// problem's "ptc", "newton", "pcg" and "robust" blocks (the reference's start x_k + alpha (x_hat - x_k), its
+// inner-count controller, Eisenstat-Walker forcing), and writes <dir>/gpu-<mode>/:
+//   gpu-result.json               schema e7-gpu/1: the run-e7.ts fields this solver records
+//   gpu-ptc.bin                   f64 [accepted steps][7]: step, h, residual, inner, rejected, pcgIterations, minDistance
+//   gpu-equilibrium.{json,bin}    the equilibrium as an f32 state file with its final_h
+//   gpu-states.bin                f32: the start state, then the equilibrium
+//   gpu-iterations.bin, gpu-robust.bin, gpu-attempts.bin: empty (per-Newton and per-attempt records are not kept)
+// Exit status: 0 when the solve ran to a stop rule, 1 on an error, 2 on a usage error.
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/drape_b200.h"
+#include "problem.h"
+
+namespace {
+
+const char* kUsage =
+    "usage: drape --case <case dir> [--mode cold|warm|prolong] [--start <state prefix>]\n"
+    "             [--preconditioner jacobi|multilevel|learned] [--network <weights>] [--device <n>]\n";
+
+struct Args {
+  std::string dir, mode = "cold", start, preconditioner = "jacobi", network;
+  int device = 0;
+};
+
+bool parse(int argc, char** argv, Args* a, std::string* err) {
+  for (int i = 1; i < argc; ++i) {
+    const std::string k = argv[i];
+    auto value = [&](std::string* out) {
+      if (i + 1 >= argc) return false;
+      *out = argv[++i];
+      return true;
+    };
+    std::string dev;
+    bool ok = k == "--case" ? value(&a->dir)
+              : k == "--mode" ? value(&a->mode)
+              : k == "--start" ? value(&a->start)
+              : k == "--preconditioner" ? value(&a->preconditioner)
+              : k == "--network" ? value(&a->network)
+              : k == "--device" ? (value(&dev) && (a->device = std::atoi(dev.c_str()), true))
+                                : false;
+    if (!ok) {
+      *err = "unknown or incomplete option " + k;
+      return false;
+    }
+  }
+  if (a->dir.empty()) *err = "--case is required";
+  else if (a->mode != "cold" && a->mode != "warm" && a->mode != "prolong") *err = "unknown mode " + a->mode;
+  else if (a->mode != "cold" && a->start.empty()) *err = "mode " + a->mode + " needs --start <state prefix>";
+  else if (a->preconditioner != "jacobi" && a->preconditioner != "multilevel" && a->preconditioner != "learned")
+    *err = "unknown preconditioner " + a->preconditioner;
+  return err->empty();
+}
+
+// An f32 or f64 state file pair (e7_state.rs:9-40): positions and final_h.
+bool read_state(const std::string& prefix, std::vector<double>* xyz, double* final_h, std::string* err) {
+  std::string text;
+  try {
+    text = drape::read_text_file(prefix + ".json");
+  } catch (const std::exception& e) {
+    *err = e.what();
+    return false;
+  }
+  const bool single = text.find("\"f32\"") != std::string::npos;
+  *final_h = drape::json_number(text, "", "final_h");
+  std::ifstream f(prefix + ".bin", std::ios::binary);
+  std::vector<char> bytes((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+  const size_t width = single ? 4 : 8;
+  if (!f.good() && !f.eof()) {
+    *err = prefix + ".bin: cannot read";
+    return false;
+  }
+  xyz->resize(bytes.size() / width);
+  for (size_t i = 0; i < xyz->size(); ++i) {
+    if (single) {
+      float v;
+      std::memcpy(&v, bytes.data() + 4 * i, 4);
+      (*xyz)[i] = v;
+    } else {
+      std::memcpy(&(*xyz)[i], bytes.data() + 8 * i, 8);
+    }
+  }
+  return true;
+}
+
+bool write_bytes(const std::string& path, const void* data, size_t n) {
+  std::ofstream f(path, std::ios::binary);
+  f.write(static_cast<const char*>(data), std::streamsize(n));
+  return bool(f);
+}
+
+double rule(const std::string& text, const char* block, const char* key, double fallback) {
+  const double v = drape::json_number(text, block, key);
+  return std::isfinite(v) ? v : fallback;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  Args a;
+  std::string err;
+  if (!parse(argc, argv, &a, &err)) {
+    std::fprintf(stderr, "drape: %s\n%s", err.c_str(), kUsage);
+    return 2;
+  }
+  std::string text;
+  try {
+    text = drape::read_text_file(a.dir + "/problem.json");
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "drape: %s\n", e.what());
+    return 1;
+  }
+  drape_options o;
+  drape_default_options(&o);
+  o.h0 = rule(text, "ptc", "h0", o.h0);
+  o.h_max = rule(text, "ptc", "h_max", o.h_max);
+  o.h_min_factor = rule(text, "ptc", "h_min_factor", o.h_min_factor);
+  o.growth = rule(text, "ptc", "growth", o.growth);
+  o.shrink = rule(text, "ptc", "shrink", o.shrink);
+  o.max_rejections = int(rule(text, "ptc", "max_rejections", o.max_rejections));
+  o.inner_tolerance = rule(text, "ptc", "inner_tolerance", o.inner_tolerance);
+  o.inner_max = int(rule(text, "ptc", "inner_max_iterations", o.inner_max));
+  o.max_steps = int(rule(text, "ptc", "max_steps", o.max_steps));
+  o.equilibrium_relative = rule(text, "ptc", "equilibrium_f64", 1e-8);
+  o.equilibrium_absolute = 0.0;
+  o.armijo = rule(text, "newton", "armijo", o.armijo);
+  o.max_halvings = int(rule(text, "newton", "max_halvings", o.max_halvings));
+  o.pcg_max_iterations = int(rule(text, "pcg", "max_iterations", o.pcg_max_iterations));
+  o.replace_every = int(rule(text, "pcg", "replace_every", 0));
+  o.replace_above = rule(text, "pcg", "replace_above", o.replace_above);
+  o.forcing = 1;
+  o.newton_start = 1;
+  o.controller = 0;
+  o.preconditioner = a.preconditioner == "jacobi" ? 0 : a.preconditioner == "multilevel" ? 1 : 2;
+  if (const char* b = std::getenv("E7_BUDGET_S")) o.time_budget_s = std::atof(b);
+  o.progress = std::getenv("E7_PROGRESS") != nullptr;
+
+  std::vector<double> start;
+  double h0 = o.h0;
+  if (!a.start.empty()) {
+    if (!read_state(a.start, &start, &h0, &err)) {
+      std::fprintf(stderr, "drape: %s\n", err.c_str());
+      return 1;
+    }
+  }
+  drape_ctx* ctx = nullptr;
+  if (drape_create_from_files(a.dir.c_str(), &o, a.device, &ctx) != DRAPE_OK) {
+    std::fprintf(stderr, "drape: %s\n", drape_last_error(nullptr));
+    return 1;
+  }
+  int64_t sizes[6];
+  drape_sizes(ctx, sizes);
+  const size_t V = size_t(sizes[0]);
+  if (!start.empty() && start.size() != 3 * V) {
+    std::fprintf(stderr, "drape: %s has %zu values, the problem %zu vertices\n", a.start.c_str(), start.size(), V);
+    drape_destroy(ctx);
+    return 1;
+  }
+  drape_network* net = nullptr;
+  if (o.preconditioner == 2) {
+    std::string path = a.network;
+    if (path.empty()) {  // the shipped weights beside the executable
+      char self[4096];
+      const ssize_t n = readlink("/proc/self/exe", self, sizeof self - 1);
+      path = n > 0 ? std::string(self, size_t(n)) : std::string(argv[0]);
+      path = path.substr(0, path.rfind('/') + 1) + "preconditioner_network.bin";
+    }
+    if (drape_network_create(a.device, 0, &net) != DRAPE_OK || drape_network_load(net, path.c_str()) != DRAPE_OK ||
+        drape_set_network(ctx, net) != DRAPE_OK) {
+      std::fprintf(stderr, "drape: preconditioner network %s: %s\n", path.c_str(), drape_last_error(nullptr));
+      drape_destroy(ctx);
+      drape_network_destroy(net);
+      return 1;
+    }
+  }
+  std::vector<double> x0(3 * V);
+  drape_get_state(ctx, x0.data(), nullptr);
+  if (!start.empty()) x0 = start;
+  drape_run_log log{};
+  const drape_status st = drape_solve_equilibrium(ctx, start.empty() ? nullptr : start.data(), h0, &log);
+  if (st != DRAPE_OK && st != DRAPE_E_DIVERGED && st != DRAPE_E_TIMEOUT) {
+    std::fprintf(stderr, "drape: %s\n", drape_last_error(ctx));
+    drape_destroy(ctx);
+    drape_network_destroy(net);
+    return 1;
+  }
+  std::vector<double> x(3 * V);
+  double final_h = 0.0;
+  drape_get_state(ctx, x.data(), &final_h);
+  int32_t count = 0;
+  drape_step_records(ctx, nullptr, 0, &count);
+  std::vector<drape_step_record> recs(size_t(count > 0 ? count : 1));
+  drape_step_records(ctx, recs.data(), count, &count);
+
+  const std::string out = a.dir + "/gpu-" + a.mode;
+  ::mkdir(out.c_str(), 0755);
+  std::vector<double> ptc;
+  for (int i = 0; i < count; ++i) {
+    const drape_step_record& r = recs[size_t(i)];
+    const double row[7] = {double(r.step), r.h, r.residual, double(r.inner), double(r.rejected),
+                           double(r.pcg_iterations), r.min_distance};
+    ptc.insert(ptc.end(), row, row + 7);
+  }
+  std::vector<float> eq(x.begin(), x.end()), states(x0.begin(), x0.end());
+  states.insert(states.end(), eq.begin(), eq.end());
+  bool ok = write_bytes(out + "/gpu-ptc.bin", ptc.data(), ptc.size() * sizeof(double)) &&
+            write_bytes(out + "/gpu-equilibrium.bin", eq.data(), eq.size() * sizeof(float)) &&
+            write_bytes(out + "/gpu-states.bin", states.data(), states.size() * sizeof(float)) &&
+            write_bytes(out + "/gpu-iterations.bin", nullptr, 0) && write_bytes(out + "/gpu-robust.bin", nullptr, 0) &&
+            write_bytes(out + "/gpu-attempts.bin", nullptr, 0);
+  {
+    std::ofstream f(out + "/gpu-equilibrium.json");
+    char buf[256];
+    std::snprintf(buf, sizeof buf, "{\"vertices\":%zu,\"final_h\":%.17g,\"dtype\":\"f32\"}\n", V, final_h);
+    f << buf;
+    ok = ok && bool(f);
+  }
+  cudaDeviceProp prop{};
+  cudaGetDeviceProperties(&prop, a.device);
+  static const char* kStop[] = {"tolerance", "cap", "stalled", "time_budget"};
+  const char* stop = log.reason >= 0 && log.reason < 4 ? kStop[log.reason] : "error";
+  const int steps = log.ptc_steps > 0 ? log.ptc_steps : 1;
+  {
+    std::ofstream f(out + "/gpu-result.json");
+    char buf[4096];
+    std::snprintf(
+        buf, sizeof buf,
+        "{\n  \"schema\": \"e7-gpu/1\",\n  \"backend\": \"drape_b200-cuda\",\n  \"adapter\": \"%s\",\n  \"mode\": \"%s\",\n"
+        "  \"preconditioner\": \"%s\",\n  \"grid_columns\": %d,\n  \"stop\": \"%s\",\n  \"cap\": %d,\n"
+        "  \"accepted_steps\": %d,\n  \"rejected_attempts\": %d,\n  \"newton_iterations_total\": %d,\n"
+        "  \"pcg_iterations_total\": %d,\n  \"final_h\": %.17g,\n  \"final_residual\": %.17g,\n"
+        "  \"final_relative_residual\": %.17g,\n  \"trajectory_ms\": %.6f,\n  \"ms_per_step\": %.6f,\n"
+        "  \"device_ms\": %.6f,\n  \"phase_ms_per_step\": {\"assembly\": %.6f, \"pcg\": %.6f, \"line_search\": %.6f, "
+        "\"ccd\": %.6f, \"other\": %.6f},\n  \"kernel_launches\": %d,\n  \"fallbacks_to_jacobi\": %d,\n"
+        "  \"record_tables\": \"gpu-iterations.bin, gpu-robust.bin and gpu-attempts.bin are empty: per-Newton and "
+        "per-attempt records are not kept\"\n}\n",
+        prop.name, a.mode.c_str(), a.preconditioner.c_str(), int(drape::json_number(text, "", "grid_columns")), stop,
+        o.max_steps, log.ptc_steps, log.rejected_attempts, log.newton_iterations, log.pcg_iterations, log.final_h,
+        log.final_residual, log.final_relative_residual, 1e3 * log.seconds, 1e3 * log.seconds / steps,
+        1e3 * log.device_seconds, log.ms_assembly / steps, log.ms_pcg / steps, log.ms_line_search / steps,
+        log.ms_ccd / steps, log.ms_other / steps, log.kernel_launches, log.fallbacks);
+    f << buf;
+    ok = ok && bool(f);
+  }
+  std::printf("%s %s: %d steps (+%d rejected), stop %s, r/L %.2e, %.2f s, h next %.2e\n",
+              a.dir.substr(a.dir.rfind('/') + 1).c_str(), a.mode.c_str(), log.ptc_steps, log.rejected_attempts, stop,
+              log.final_relative_residual, log.seconds, final_h);
+  drape_destroy(ctx);
+  drape_network_destroy(net);
+  if (!ok) {
+    std::fprintf(stderr, "drape: cannot write the outputs in %s\n", out.c_str());
+    return 1;
+  }
+  return 0;
+}

@@ -424,4 +424,10 @@ void write_problem_files(const HostProblem& p, const std::string& dir) {
   std::ofstream(dir + "/problem.json") << head << "\"arrays\":" << manifest << "}";
 }
 
+std::string read_text_file(const std::string& path) { return read_all(path); }
+
+double json_number(const std::string& text, const std::string& anchor, const std::string& key) {
+  return number(text, anchor, key);
+}
+
 }  // namespace drape

@@ -49,6 +49,11 @@ HostProblem reference_problem(int columns, const std::string& edit);
 // Reads a problem.json / problem.bin pair written by the reference's `oracle e7-generate` (or the oracle
 // restatement); f64 copies of the geometry arrays are used when present. Throws std::runtime_error.
 HostProblem read_problem_files(const std::string& dir);
+// The whole file as text (throws if it cannot be read).
+std::string read_text_file(const std::string& path);
+// The number at the first "key": after the first "anchor" of a JSON text (NaN if absent): the flat key scan the
+// reference reads problem.json with (jsonscan.rs:3-26).
+double json_number(const std::string& text, const std::string& anchor, const std::string& key);
 
 // Writes the same pair (the subset this GPU stage reads, plus f64 geometry).
 void write_problem_files(const HostProblem& p, const std::string& dir);

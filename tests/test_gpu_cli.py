@@ -1,0 +1,52 @@
+"""The `drape` command on the GPU (needs a B200): a cold solve of the reference's n17 base case with the rules
+of its problem.json writes the gpu-<mode>/ files run-e7.ts writes (state files readable by both), and a warm
+start from that equilibrium stays there; the learned preconditioner runs with the shipped weights."""
+import json
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from drape_b200 import api
+from drape_b200.build import CLI
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(*args):
+    p = subprocess.run([CLI, *args], capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr
+    return p
+
+
+def test_cold_then_warm_reference_case():
+    with tempfile.TemporaryDirectory() as t:
+        api.write_reference_problem(t, 17, "base")
+        _run("--case", t, "--mode", "cold")
+        out = os.path.join(t, "gpu-cold")
+        res = json.load(open(os.path.join(out, "gpu-result.json")))
+        assert res["schema"] == "e7-gpu/1" and res["stop"] == "tolerance", res
+        assert res["final_relative_residual"] <= 1e-8 * 1.0001
+        ptc = np.fromfile(os.path.join(out, "gpu-ptc.bin"), np.float64).reshape(-1, 7)
+        assert len(ptc) == res["accepted_steps"] and np.all(np.diff(ptc[:, 0]) > 0)
+        meta = json.load(open(os.path.join(out, "gpu-equilibrium.json")))
+        eq = np.fromfile(os.path.join(out, "gpu-equilibrium.bin"), np.float32)
+        assert meta["dtype"] == "f32" and eq.size == 3 * meta["vertices"] and meta["final_h"] > 0
+        states = np.fromfile(os.path.join(out, "gpu-states.bin"), np.float32)
+        assert np.array_equal(states[eq.size:], eq)
+        # warm start from the written equilibrium: already converged (f32 rounding of the state aside)
+        _run("--case", t, "--mode", "warm", "--start", os.path.join(out, "gpu-equilibrium"))
+        warm = json.load(open(os.path.join(t, "gpu-warm", "gpu-result.json")))
+        assert warm["stop"] == "tolerance" and warm["accepted_steps"] <= res["accepted_steps"], warm
+        eq2 = np.fromfile(os.path.join(t, "gpu-warm", "gpu-equilibrium.bin"), np.float32)
+        assert np.abs(eq2 - eq).max() <= 1e-3
+
+
+def test_learned_preconditioner_from_the_command():
+    with tempfile.TemporaryDirectory() as t:
+        api.write_reference_problem(t, 17, "base")
+        _run("--case", t, "--mode", "cold", "--preconditioner", "learned")
+        res = json.load(open(os.path.join(t, "gpu-cold", "gpu-result.json")))
+        assert res["preconditioner"] == "learned" and res["stop"] == "tolerance", res
