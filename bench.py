@@ -6,8 +6,9 @@ nu = 0.3, t = 5e-4 m, k_b = 1e-5 N m, IPC d_hat = 2e-3 m, kappa = 1e3; PTC from 
 |grad E_s| <= 1e-6 N, PCG rtol 1e-6, <= 2000 iterations. One step = one full cold solve to the converged state.
 Direction solver (--preconditioner): learned (default: the multilevel V-cycle flexible PCG with the shipped
 network's fine smoother), multilevel (spectral Jacobi smoothing), jacobi (the reference's block-Jacobi PCG).
---compare adds one device-timed solve with each of the other two on the same workload (the learned-vs-Jacobi
-comparison of the metric). Synthetic scene (the reference ships no dataset; seeded jitter, seed 0).
+--compare jacobi (default) adds one device-timed block-Jacobi solve of the same workload after the timed steps, the
+learned-vs-Jacobi comparison of the metric (all: also multilevel and learned; none: skip). Synthetic scene (the
+reference ships no dataset; seeded jitter, seed 0).
 
 value: seconds per converged solve with the problem resident in HBM (CUDA-event-timed solve, max over ranks).
 e2e:   the same through the C ABI from host arrays: drape_create (host->device copies) + solve + drape_get_state
@@ -135,7 +136,7 @@ def run_gpu(args):
         return api.default_options(pcg_max_iterations=args.pcg_max, max_steps=args.max_steps,
                                    preconditioner={"jacobi": 0, "multilevel": 1, "learned": 2}[name])
 
-    net = api.Network.trained(device=local) if args.preconditioner == "learned" or args.compare else None
+    net = api.Network.trained(device=local) if args.preconditioner == "learned" or args.compare == "all" else None
     # Host arrays for the end-to-end leg (built outside every timed region).
     pdir = tempfile.mkdtemp(prefix="drape_bench_")
     api.write_sheet_problem(pdir, args.n, seed=args.seed, plane=bool(args.plane))
@@ -210,8 +211,9 @@ def run_gpu(args):
         bytes_per_iter = multilevel_bytes_per_iteration(args.n, R, B)
     achieved = (bytes_per_iter * last["pcg_iterations"]) / (last["ms_pcg"] / 1e3) / 1e9 if last["ms_pcg"] > 0 else 0.0
     comparison = {}
-    if args.compare:
-        for other in ("jacobi", "multilevel", "learned"):
+    others = {"none": (), "jacobi": ("jacobi",), "all": ("jacobi", "multilevel", "learned")}[args.compare]
+    if others:  # every rank runs the same comparison solves (replicas; one_step holds the barriers), rank 0 reports
+        for other in others:
             if other == args.preconditioner:
                 continue
             log_o, s_o, _, _ = one_step(other)
@@ -221,6 +223,8 @@ def run_gpu(args):
                                  "pcg_per_newton": log_o["pcg_iterations"] / max(1, log_o["newton_iterations"]),
                                  "fallbacks_to_jacobi": log_o["fallbacks"], "converged": log_o["reason"] == "tolerance",
                                  "final_residual_N": log_o["final_residual"]}
+        if "jacobi" in comparison:
+            comparison["jacobi_seconds_over_this"] = comparison["jacobi"]["seconds"] / t
     out = {
         "metric": METRIC, "value": t, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -326,7 +330,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--preconditioner", default="learned", choices=["jacobi", "multilevel", "learned"])
-    ap.add_argument("--compare", action="store_true")
+    ap.add_argument("--compare", default="jacobi", choices=["none", "jacobi", "all"],
+                    help="after the timed steps, one device-timed solve of the same workload with each other solver")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

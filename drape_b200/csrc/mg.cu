@@ -833,12 +833,6 @@ int mg_level_count(int n) {
   return n <= kMgCoarsestMax ? levels : 1;
 }
 
-cudaError_t mg_fine_jacobi_smoother(const MgDevice& d, float omega, cudaStream_t s) {
-  const int R = d.fine.R;
-  jacobi_smoother_kernel<true><<<(R + 255) / 256, 256, 0, s>>>(d.fine, d.lv[0], omega);
-  return cudaGetLastError();
-}
-
 namespace {
 
 // Reproducible start vector of the power method: components uniform in [-1, 1) from a hash of the index.
@@ -934,12 +928,6 @@ __global__ void scale_smoother_kernel(float* S, int count, const float* omega) {
 }
 
 }  // namespace
-
-int mg_power_ctas(const MgDevice& d, int first, int end) {
-  int c = 0;
-  for (int l = first; l < end; ++l) c += row_grid(d.lv[l].rows);
-  return c;
-}
 
 cudaError_t mg_setup(const MgDevice& d, float omega, bool fine_smoother, bool reuse_omega, cudaStream_t s) {
   if (d.levels < 2) return cudaErrorInvalidValue;

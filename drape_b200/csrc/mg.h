@@ -70,7 +70,6 @@ struct MgDevice {
   MgLevel lv[kMgMaxLevels];
   float* coarse_inv = nullptr;   // dense f32 inverse of the coarsest operator, [m][m], m = 3 rows
   float* omega = nullptr;        // [kMgMaxLevels] damping of each level's Jacobi smoother (set-up output)
-  double* coarse_work = nullptr; // f64 [m][2m] Gauss-Jordan work space
   // flexible PCG vectors (level 0, float4 rows)
   const float4* b = nullptr;
   float4* x = nullptr;
@@ -83,7 +82,7 @@ struct MgDevice {
 };
 
 constexpr int kMgRowsPerCta = 32;  // level-0 row kernels: 8 lanes per row, 256 threads
-constexpr int kMgPartials = 4096;  // capacity of each partial array (R <= 131072 rows)
+constexpr int kMgPartials = 4096;  // capacity of each partial array (the power method's: R < 24 x 4096 rows)
 
 // Number of levels for an n x n grid (1 if it cannot be coarsened).
 int mg_level_count(int n);
@@ -98,10 +97,6 @@ int mg_level_count(int n);
 // change little from one Newton update to the next).
 constexpr int kMgPowerSteps = 10;
 cudaError_t mg_setup(const MgDevice& d, float omega, bool fine_smoother, bool reuse_omega, cudaStream_t s);
-// CTAs of the level row kernels summed over levels [first, end) (the power method's partial sums).
-int mg_power_ctas(const MgDevice& d, int first, int end);
-// Smoothers omega * D^{-1} at level 0 only.
-cudaError_t mg_fine_jacobi_smoother(const MgDevice& d, float omega, cudaStream_t s);
 
 // Flexible PCG: clear the state and start from x = 0, r = b.
 cudaError_t mg_pcg_init(const MgDevice& d, float tol2, int max_iterations, int stall_window, cudaStream_t s);
