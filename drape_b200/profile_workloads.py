@@ -3,7 +3,7 @@
     python -m drape_b200.profile_workloads cycle   [--n 129] [--steps 20]   # multilevel V-cycle and PCG iteration
     python -m drape_b200.profile_workloads network [--n 129] [--steps 20]   # preconditioner network forward
     python -m drape_b200.profile_workloads spmv    [--drapes 128]          # batched and n257 BSR SpMV, autotuned
-    python -m drape_b200.profile_workloads solve   [--n 129] [--preconditioner learned] [--out state.npy]
+    python -m drape_b200.profile_workloads solve   [--n 129] [--preconditioner learned] [--out state.npy] [--budget s]
 
 spmv builds the batched configuration: `drapes` sheets with n drawn from {33, 49, 65, 97, 129}, sphere radius
 U(0.15, 0.35) m, E log-uniform in [1e5, 2e6] Pa (master seed 7), each assembled on the GPU at its start state
@@ -108,6 +108,7 @@ def main(argv=None):
     ap.add_argument("--preconditioner", default="learned", choices=["jacobi", "multilevel", "learned"])
     ap.add_argument("--out", default=None, help="solve: .npy file for the converged positions")
     ap.add_argument("--absolute", type=float, default=1e-6, help="solve: stop at |grad E_s| <= this (N)")
+    ap.add_argument("--budget", type=float, default=0.0, help="solve: the solver's own time budget, s (0: none)")
     ap.add_argument("--n", type=int, default=129)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--drapes", type=int, default=128)
@@ -119,13 +120,14 @@ def main(argv=None):
         # the bench scene's full cold solve; the converged positions go to --out for an f64 error check
         pre = {"jacobi": 0, "multilevel": 1, "learned": 2}[args.preconditioner]
         d = api.Drape.sheet(args.n, seed=0, plane=True,
-                            options=api.default_options(preconditioner=pre, equilibrium_absolute=args.absolute))
+                            options=api.default_options(preconditioner=pre, equilibrium_absolute=args.absolute,
+                                                        time_budget_s=args.budget))
         if pre == 2:
             d.set_network(api.Network.trained())
-        log = d.solve_equilibrium()
+        log = d.solve_equilibrium(check=False)
         if args.out:
             np.save(args.out, d.state)
-        print(json.dumps({k: log[k] for k in ("reason", "ptc_steps", "newton_iterations", "pcg_iterations",
+        print(json.dumps({k: log[k] for k in ("reason", "ptc_steps", "newton_iterations", "pcg_iterations", "fallbacks",
                                               "final_residual", "device_seconds", "static_energy")}), flush=True)
         return 0
     d, blocks, b = system(args.n, args.steps)
