@@ -373,6 +373,29 @@ def spmv_benchmark(row_ptr, col_idx, values, x, launches=20, lanes_per_row=8, th
     return (ms.value, y) if result else ms.value
 
 
+def solve_batch(drapes, workers=16, check=True):
+    """Solves the drapes (distinct `Drape` objects) concurrently from their current states (drape_solve_batch):
+    `workers` host threads, each solving one drape at a time on that drape's own stream. Returns (logs, seconds,
+    total_seconds): one run-log dict per drape (with its "status"), each drape's host solve time, and the batch's."""
+    lib = load()
+    lib.drape_solve_batch.argtypes = [P, ctypes.c_int32, ctypes.c_int32, P, P, P, P]
+    n = len(drapes)
+    handles = (P * n)(*[d.h for d in drapes])
+    logs = (RunLog * n)()
+    status = np.zeros(n, np.int32)
+    seconds = np.zeros(n, np.float64)
+    total = ctypes.c_double()
+    st = lib.drape_solve_batch(handles, n, workers, logs, _ptr(status), _ptr(seconds), ctypes.byref(total))
+    if check and st != 0:
+        raise DrapeError(st, lib.drape_last_error(None).decode())
+    out = []
+    for i in range(n):
+        d = logs[i].as_dict()
+        d["status"] = int(status[i])
+        out.append(d)
+    return out, seconds, total.value
+
+
 NETWORK_PARAMETERS = 34177
 NETWORK_FILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "preconditioner_network.bin")
 

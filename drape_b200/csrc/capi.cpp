@@ -1,9 +1,13 @@
 // extern "C" boundary of libdrape_b200.so (declarations and reference citations: include/drape_b200.h).
+#include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <vector>
 #include <memory>
 #include <string>
+#include <thread>
 
 #include "../../include/drape_b200.h"
 #include "context.h"
@@ -256,6 +260,51 @@ drape_status drape_solve_equilibrium(drape_ctx* ctx, const double* start, double
     if (reason == 3) return fail(ctx, "time budget exhausted", DRAPE_E_TIMEOUT);
     return DRAPE_OK;
   });
+}
+
+drape_status drape_solve_batch(drape_ctx* const* ctxs, int32_t count, int32_t workers, drape_run_log* logs,
+                               drape_status* statuses, double* solve_seconds, double* total_seconds) {
+  if (!ctxs || count < 1 || workers < 1)
+    return fail(nullptr, "drape_solve_batch: contexts is null, or count or workers is below 1", DRAPE_E_ARG);
+  std::vector<drape_ctx*> sorted(ctxs, ctxs + count);
+  for (int i = 0; i < count; ++i)
+    if (!ctxs[i] || !ctxs[i]->impl)
+      return fail(nullptr, "drape_solve_batch: context " + std::to_string(i) + " is null or destroyed", DRAPE_E_STATE);
+  std::sort(sorted.begin(), sorted.end());
+  if (std::adjacent_find(sorted.begin(), sorted.end()) != sorted.end())
+    return fail(nullptr, "drape_solve_batch: a context appears twice (one context solves on one thread)", DRAPE_E_ARG);
+  std::vector<drape_status> status(count, DRAPE_OK);
+  std::vector<double> seconds(count, 0.0);
+  std::atomic<int> next{0};
+  auto work = [&] {
+    for (int i = next++; i < count; i = next++) {
+      drape::Context& c = *ctxs[i]->impl;
+      drape_run_log local{};
+      const auto t0 = std::chrono::steady_clock::now();
+      try {
+        drape::check(cudaSetDevice(c.device()), "cudaSetDevice");
+        c.set_blocking_sync(true);
+        status[i] = drape_solve_equilibrium(ctxs[i], nullptr, 0.0, logs ? logs + i : &local);
+        c.set_blocking_sync(false);
+      } catch (const std::exception& e) {
+        c.last_error = e.what();
+        status[i] = DRAPE_E_CUDA;
+      }
+      seconds[i] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+  };
+  const auto t_start = std::chrono::steady_clock::now();
+  std::vector<std::thread> pool;
+  const int threads = std::min(workers, count);
+  for (int t = 0; t < threads; ++t) pool.emplace_back(work);
+  for (auto& t : pool) t.join();
+  if (total_seconds) *total_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+  if (statuses) std::copy(status.begin(), status.end(), statuses);
+  if (solve_seconds) std::copy(seconds.begin(), seconds.end(), solve_seconds);
+  for (int i = 0; i < count; ++i)
+    if (status[i] != DRAPE_OK)
+      return fail(nullptr, "drape_solve_batch: drape " + std::to_string(i) + ": " + ctxs[i]->impl->last_error, status[i]);
+  return DRAPE_OK;
 }
 
 drape_status drape_step_records(const drape_ctx* cctx, drape_step_record* out, int32_t capacity, int32_t* count) {

@@ -91,6 +91,7 @@ Context::~Context() {
   if (stream_) cudaStreamSynchronize(stream_);
   for (auto& e : ev_)
     if (e) cudaEventDestroy(e);
+  if (sync_event_) cudaEventDestroy(sync_event_);
   if (pinned_) cudaFreeHost(pinned_);
   if (pinned_state_) cudaFreeHost(pinned_state_);
   if (pinned_mg_) cudaFreeHost(pinned_mg_);
@@ -277,7 +278,24 @@ void Context::configure_pcg() {
   check(cudaMemsetAsync(pcg_timing_.ptr, 0, 8 * sizeof(long long), stream_), "memset");
 }
 
-void Context::sync() { check(cudaStreamSynchronize(stream_), "stream synchronize"); }
+void Context::sync() { wait_stream(); }
+
+void Context::wait_stream() const {
+  if (!blocking_sync_) {
+    check(cudaStreamSynchronize(stream_), "stream synchronize");
+    return;
+  }
+  check(cudaEventRecord(sync_event_, stream_), "event");
+  check(cudaEventSynchronize(sync_event_), "event synchronize");
+}
+
+void Context::set_blocking_sync(bool on) {
+  if (on && !sync_event_) {
+    check(cudaSetDevice(device_), "cudaSetDevice");
+    check(cudaEventCreateWithFlags(&sync_event_, cudaEventBlockingSync | cudaEventDisableTiming), "cudaEventCreate");
+  }
+  blocking_sync_ = on;
+}
 
 double Context::read_scalar(int slot) {
   check(cudaMemcpyAsync(pinned_ + slot, scalars_.ptr + slot, sizeof(double), cudaMemcpyDeviceToHost, stream_), "read");
@@ -297,7 +315,7 @@ void Context::set_positions(const double* xyz) {
 
 void Context::get_positions(double* xyz) const {
   x_.download(xyz, 3 * size_t(host_.V), stream_);
-  check(cudaStreamSynchronize(stream_), "stream synchronize");
+  wait_stream();
 }
 
 double Context::assemble(const double* x, double inv_h2, double mu, int mode, bool hessian) {

@@ -130,11 +130,18 @@ class Context {
   void network_train_host(Network& net, int tuples, const float* const* blocks, const double* const* rhs,
                           const double* const* solutions, int steps, double lr, double* losses);
 
+  // ---- concurrent solves of many contexts (one host thread each)
+  int device() const { return device_; }
+  // With `on`, every wait for this context's stream blocks its host thread on an event (cudaEventBlockingSync)
+  // instead of spinning in cudaStreamSynchronize, so that many solving threads share the host cores.
+  void set_blocking_sync(bool on);
+
   std::string last_error;
 
  private:
   void upload_problem();
   void sync();
+  void wait_stream() const;
   double read_scalar(int slot);
   double assemble(const double* x, double inv_h2, double mu, int mode, bool hessian);
   double reduce_partials(int n, int op, int slot);
@@ -155,6 +162,8 @@ class Context {
   drape_options opt_;
   int device_ = 0;
   cudaStream_t stream_ = nullptr;
+  cudaEvent_t sync_event_ = nullptr;  // set_blocking_sync's event (null: cudaStreamSynchronize)
+  bool blocking_sync_ = false;
   DevProblem dp_{};
   double gravity_load_ = 0.0, final_h_ = 0.0;
   PcgLaunch pcg_cfg_;

@@ -972,7 +972,11 @@ cudaError_t mg_setup(const MgDevice& d, float omega, bool fine_smoother, bool re
   const MgLevel& top = d.lv[d.levels - 1];
   const int m = 3 * top.rows;
   const size_t smem = size_t(m) * 2 * m * sizeof(double);
-  if ((e = cudaFuncSetAttribute(coarse_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))) != cudaSuccess)
+  // The ceiling is one process-wide setting: the largest coarsest level's size for every call, so that concurrent
+  // set-ups of different hierarchies never lower it under another's launch.
+  constexpr int kCoarseSmemMax = 3 * kMgCoarsestRowsMax * 2 * 3 * kMgCoarsestRowsMax * int(sizeof(double));
+  if ((e = cudaFuncSetAttribute(coarse_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kCoarseSmemMax)) !=
+      cudaSuccess)
     return e;
   coarse_inverse_kernel<<<1, 1024, smem, s>>>(top, d.coarse_inv, d.error);
   return cudaGetLastError();

@@ -470,6 +470,20 @@ const void* pcg_fn(int lpr, bool msmem) {
   return nullptr;
 }
 
+// Raises the kernel's dynamic shared-memory ceiling to all that the device allows beside the kernel's static shared
+// memory. The ceiling is one setting per kernel for the whole process: setting it to this fixed value, rather than
+// to each launch's own size, keeps host threads that launch the kernel concurrently for drapes of different sizes
+// from lowering it between another thread's set and launch.
+cudaError_t allow_dynamic_smem(const void* fn) {
+  int dev = 0, optin = 0;
+  cudaError_t e;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) != cudaSuccess) return e;
+  cudaFuncAttributes fa{};
+  if ((e = cudaFuncGetAttributes(&fa, fn)) != cudaSuccess) return e;
+  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - int(fa.sharedSizeBytes));
+}
+
 }  // namespace
 
 size_t pcg_smem_bytes(int cap_rows, int cap_blocks, bool msmem) {
@@ -483,7 +497,7 @@ int pcg_max_grid(int threads, int lanes_per_row, size_t smem, bool msmem) {
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess) return 0;
+  if (allow_dynamic_smem(fn) != cudaSuccess) return 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess) return 0;
   return sms * per_sm;
 }
@@ -491,7 +505,7 @@ int pcg_max_grid(int threads, int lanes_per_row, size_t smem, bool msmem) {
 cudaError_t launch_pcg(const PcgArgs& a, const PcgLaunch& cfg, cudaStream_t s) {
   const void* fn = pcg_fn(cfg.lanes_per_row, cfg.matrix_in_smem);
   if (!fn || cfg.threads % 32 != 0 || cfg.threads > 1024 || cfg.grid < 1) return cudaErrorInvalidValue;
-  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(cfg.smem));
+  cudaError_t e = allow_dynamic_smem(fn);
   if (e != cudaSuccess) return e;
   PcgArgs args = a;
   void* params[] = {&args};

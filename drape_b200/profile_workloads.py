@@ -4,6 +4,10 @@
     python -m drape_b200.profile_workloads network [--n 129] [--steps 20]   # preconditioner network forward
     python -m drape_b200.profile_workloads spmv    [--drapes 128]          # batched and n257 BSR SpMV, autotuned
     python -m drape_b200.profile_workloads solve   [--n 129] [--preconditioner learned] [--out state.npy] [--budget s]
+    python -m drape_b200.profile_workloads batch   [--drapes 128] [--workers 32] [--budget s]   # concurrent solves
+
+batch solves the same `drapes` sheets cold (learned preconditioner unless --preconditioner says otherwise) through
+drape_solve_batch, `workers` at a time, and reports solves/s and the p50/p99 of the per-drape solve times.
 
 spmv builds the batched configuration: `drapes` sheets with n drawn from {33, 49, 65, 97, 129}, sphere radius
 U(0.15, 0.35) m, E log-uniform in [1e5, 2e6] Pa (master seed 7), each assembled on the GPU at its start state
@@ -19,6 +23,7 @@ assemble the projected (SPD) PTC system at that state, and then:
 import argparse
 import ctypes
 import json
+import os
 import sys
 
 import numpy as np
@@ -52,16 +57,58 @@ def sheet_matrix(n, seed, radius, young):
     return arr["row_ptr"].astype(np.int64), arr["col_idx"].astype(np.int64), blocks
 
 
+def batch_scenes(drapes):
+    """(columns, seed, sphere radius, E) of the batched configuration's drapes, master seed 7."""
+    rng = np.random.default_rng(7)
+    out = []
+    for _ in range(drapes):
+        n = int(rng.choice([33, 49, 65, 97, 129]))
+        out.append((n, int(rng.integers(1, 1 << 30)), float(rng.uniform(0.15, 0.35)),
+                    float(np.exp(rng.uniform(np.log(1e5), np.log(2e6))))))
+    return out
+
+
+def batch_workload(drapes, workers, budget, preconditioner):
+    """Every drape of the batched configuration solved cold to |grad E_s| <= 1e-6 N, `workers` at a time."""
+    net = api.Network.trained() if preconditioner == 2 else None
+    ds = []
+    for n, seed, radius, young in batch_scenes(drapes):
+        d = api.Drape.sheet(n, seed=seed, radius=radius, young=young, plane=True,
+                            options=api.default_options(preconditioner=preconditioner, time_budget_s=budget))
+        if net is not None:
+            d.set_network(net)
+        ds.append(d)
+    logs, seconds, total = api.solve_batch(ds, workers, check=False)
+    sizes = [s[0] for s in batch_scenes(drapes)]
+    done = [i for i, g in enumerate(logs) if g["status"] == 0]
+    per_n = {}
+    for n in sorted(set(sizes)):
+        idx = [i for i in range(drapes) if sizes[i] == n]
+        per_n[str(n)] = {"drapes": len(idx), "median_s": float(np.median(seconds[idx])),
+                         "median_newton": float(np.median([logs[i]["newton_iterations"] for i in idx])),
+                         "pcg_per_newton": sum(logs[i]["pcg_iterations"] for i in idx) /
+                         max(1, sum(logs[i]["newton_iterations"] for i in idx))}
+    reasons = {}
+    for g in logs:
+        reasons[g["reason"]] = reasons.get(g["reason"], 0) + 1
+    out = {"workload": "batch", "drapes": drapes, "workers": workers, "preconditioner": preconditioner,
+           "budget_s": budget, "solved": len(done), "total_s": total, "solves_per_s": len(done) / total,
+           "p50_s": float(np.percentile(seconds, 50)), "p99_s": float(np.percentile(seconds, 99)),
+           "max_s": float(seconds.max()), "sum_device_s": float(sum(g["device_seconds"] for g in logs)),
+           "newton": int(sum(g["newton_iterations"] for g in logs)), "pcg": int(sum(g["pcg_iterations"] for g in logs)),
+           "fallbacks": int(sum(g["fallbacks"] for g in logs)), "reasons": reasons, "per_columns": per_n}
+    for d in ds:
+        d.close()
+    return out
+
+
 def spmv_workload(drapes):
     import json as _json
     import os
-    rng = np.random.default_rng(7)
     parts, offset = [], 0
     sizes = []
-    for _ in range(drapes):
-        n = int(rng.choice([33, 49, 65, 97, 129]))
-        rp, ci, blk = sheet_matrix(n, int(rng.integers(1, 1 << 30)), float(rng.uniform(0.15, 0.35)),
-                                   float(np.exp(rng.uniform(np.log(1e5), np.log(2e6)))))
+    for n, seed, radius, young in batch_scenes(drapes):
+        rp, ci, blk = sheet_matrix(n, seed, radius, young)
         parts.append((rp, ci + offset, blk))
         offset += len(rp) - 1
         sizes.append(n)
@@ -104,17 +151,25 @@ def spmv_workload(drapes):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("workload", choices=["cycle", "network", "spmv", "solve"])
+    ap.add_argument("workload", choices=["cycle", "network", "spmv", "solve", "batch"])
+    ap.add_argument("--workers", type=int, default=32, help="batch: drapes solved at a time")
     ap.add_argument("--preconditioner", default="learned", choices=["jacobi", "multilevel", "learned"])
     ap.add_argument("--out", default=None, help="solve: .npy file for the converged positions")
     ap.add_argument("--absolute", type=float, default=1e-6, help="solve: stop at |grad E_s| <= this (N)")
-    ap.add_argument("--budget", type=float, default=0.0, help="solve: the solver's own time budget, s (0: none)")
+    ap.add_argument("--budget", type=float, default=0.0,
+                    help="solve, batch: the solver's own time budget per drape, s (0: none)")
     ap.add_argument("--n", type=int, default=129)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--drapes", type=int, default=128)
     args = ap.parse_args(argv)
     if args.workload == "spmv":
         print(json.dumps(spmv_workload(args.drapes)), flush=True)
+        return 0
+    if args.workload == "batch":
+        # more hardware queues than the default 8, for streams of many drapes (read when CUDA starts)
+        os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+        pre = {"jacobi": 0, "multilevel": 1, "learned": 2}[args.preconditioner]
+        print(json.dumps(batch_workload(args.drapes, args.workers, args.budget, pre)), flush=True)
         return 0
     if args.workload == "solve":
         # the bench scene's full cold solve; the converged positions go to --out for an f64 error check
@@ -127,7 +182,7 @@ def main(argv=None):
         log = d.solve_equilibrium(check=False)
         if args.out:
             np.save(args.out, d.state)
-        print(json.dumps({k: log[k] for k in ("reason", "ptc_steps", "newton_iterations", "pcg_iterations", "fallbacks",
+        print(json.dumps({k: log[k] for k in ("reason", "ptc_steps", "newton_iterations", "pcg_iterations", "fallbacks", "ms_pcg",
                                               "final_residual", "device_seconds", "static_energy")}), flush=True)
         return 0
     d, blocks, b = system(args.n, args.steps)

@@ -117,3 +117,11 @@ def test_creating_a_context_without_a_device_fails_loudly(lib):
         pytest.skip("a GPU is present")
     with pytest.raises(api.DrapeError):
         api.Drape.sheet(9)
+
+
+def test_batch_solve_rejects_an_empty_batch(lib):
+    # argument checks of drape_solve_batch happen on the host, before any context or thread is touched
+    with pytest.raises(api.DrapeError) as e:
+        api.solve_batch([])
+    assert e.value.status == 1
+    assert "count or workers" in str(e.value)
