@@ -78,6 +78,18 @@ class StepRecord(ctypes.Structure):
                 ("min_distance", ctypes.c_double)]
 
 
+class NewtonRecord(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int32) for k in ("step", "iteration", "pcg_iterations", "pcg_status", "halvings",
+                                              "status", "retries", "pad")] + \
+               [(k, ctypes.c_double) for k in ("relative_residual", "linear_residual", "step_length", "eta", "mu",
+                                               "alpha_max", "delta_sum", "slope", "norm_squared")]
+
+
+class AttemptRecord(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int32) for k in ("step", "attempt", "reason", "record_start", "record_end", "pad")] + \
+               [("h", ctypes.c_double)]
+
+
 def load():
     """Loads the CUDA library (raises if it has not been built: `python -m drape_b200.build`)."""
     global _lib
@@ -267,6 +279,22 @@ class Drape:
         recs = (StepRecord * max(n.value, 1))()
         self._check(self.lib.drape_step_records(self.h, recs, n.value, ctypes.byref(n)))
         return [{k: getattr(r, k) for k, _ in StepRecord._fields_} for r in recs[: n.value]]
+
+    def _records(self, fn, cls):
+        fn.argtypes = [P, P, ctypes.c_int32, P]
+        n = ctypes.c_int32()
+        self._check(fn(self.h, None, 0, ctypes.byref(n)))
+        recs = (cls * max(n.value, 1))()
+        self._check(fn(self.h, recs, n.value, ctypes.byref(n)))
+        return [{k: getattr(r, k) for k, _ in cls._fields_ if k != "pad"} for r in recs[: n.value]]
+
+    def newton_records(self):
+        """The last solve's Newton iterates (drape_newton_records; gpu-iterations.bin / gpu-robust.bin rows)."""
+        return self._records(self.lib.drape_newton_records, NewtonRecord)
+
+    def attempt_records(self):
+        """The last solve's attempts (drape_attempt_records; gpu-attempts.bin rows)."""
+        return self._records(self.lib.drape_attempt_records, AttemptRecord)
 
     def assemble(self, x, x_hat=None, h=0.0, mu=0.0, mode=0, curvature=False, blocks=True):
         g = np.zeros(3 * self.R)

@@ -317,6 +317,27 @@ drape_status drape_step_records(const drape_ctx* cctx, drape_step_record* out, i
   });
 }
 
+drape_status drape_newton_records(const drape_ctx* cctx, drape_newton_record* out, int32_t capacity, int32_t* count) {
+  auto* ctx = const_cast<drape_ctx*>(cctx);
+  return guarded(ctx, [&](drape::Context& c) {
+    const auto& s = c.newton_records();
+    if (count) *count = int32_t(s.size());
+    for (int32_t i = 0; out && i < capacity && i < int32_t(s.size()); ++i) out[i] = s[size_t(i)];
+    return DRAPE_OK;
+  });
+}
+
+drape_status drape_attempt_records(const drape_ctx* cctx, drape_attempt_record* out, int32_t capacity,
+                                   int32_t* count) {
+  auto* ctx = const_cast<drape_ctx*>(cctx);
+  return guarded(ctx, [&](drape::Context& c) {
+    const auto& s = c.attempt_records();
+    if (count) *count = int32_t(s.size());
+    for (int32_t i = 0; out && i < capacity && i < int32_t(s.size()); ++i) out[i] = s[size_t(i)];
+    return DRAPE_OK;
+  });
+}
+
 drape_status drape_assemble(drape_ctx* ctx, const double* x, const double* x_hat, double h, double mu, int32_t mode,
                             int32_t curvature, double* grad, float* blocks) {
   return guarded(ctx, [&](drape::Context& c) {

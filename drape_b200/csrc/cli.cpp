@@ -12,7 +12,10 @@
 //   gpu-ptc.bin                   f64 [accepted steps][7]: step, h, residual, inner, rejected, pcgIterations, minDistance
 //   gpu-equilibrium.{json,bin}    the equilibrium as an f32 state file with its final_h
 //   gpu-states.bin                f32: the start state, then the equilibrium
-//   gpu-iterations.bin, gpu-robust.bin, gpu-attempts.bin: empty (per-Newton and per-attempt records are not kept)
+//   gpu-iterations.bin            f64 [Newton iterates][9]: the reference's RECORD_FIELDS (outputs.ts:8)
+//   gpu-robust.bin                f64 [Newton iterates][16]: EXTRA_FIELDS (outputs.ts:9-10), NaN where this solver
+//                                 has no counterpart (update/step norms, resolution, limiting vertex, noise tests)
+//   gpu-attempts.bin              f64 [attempts][6]: step, attempt, h, reason, recordStart, recordEnd
 // Exit status: 0 when the solve ran to a stop rule, 1 on an error, 2 on a usage error.
 #include <sys/stat.h>
 #include <unistd.h>
@@ -219,13 +222,45 @@ int main(int argc, char** argv) {
                            double(r.pcg_iterations), r.min_distance};
     ptc.insert(ptc.end(), row, row + 7);
   }
+  // per-Newton and per-attempt tables (outputs.ts:8-10, run-e7.ts:94-98): f64 rows, NaN where the reference's
+  // field has no counterpart in this solver or no value on the iterate (the last iterate takes no solve)
+  const double nan = std::nan("");
+  int32_t n_rec = 0, n_att = 0;
+  drape_newton_records(ctx, nullptr, 0, &n_rec);
+  drape_attempt_records(ctx, nullptr, 0, &n_att);
+  std::vector<drape_newton_record> nrec(size_t(n_rec > 0 ? n_rec : 1));
+  std::vector<drape_attempt_record> arec(size_t(n_att > 0 ? n_att : 1));
+  drape_newton_records(ctx, nrec.data(), n_rec, &n_rec);
+  drape_attempt_records(ctx, arec.data(), n_att, &n_att);
+  std::vector<double> iterations, robust, attempts;
+  for (int i = 0; i < n_rec; ++i) {
+    const drape_newton_record& r = nrec[size_t(i)];
+    const bool solved = r.pcg_iterations >= 0;
+    const double it_row[9] = {double(r.step), double(r.iteration), r.relative_residual,
+                              solved ? double(r.pcg_iterations) : nan, solved ? double(r.pcg_status) : nan,
+                              solved ? r.linear_residual : nan, r.step_length,
+                              r.halvings >= 0 ? double(r.halvings) : nan, double(r.status)};
+    iterations.insert(iterations.end(), it_row, it_row + 9);
+    // eta, mu, updateInf, stepInf, retries, resolution, alphaMax, limitingVertex, minDistance, deltaSum, deltaAbs,
+    // noiseOnly, slope, slopeExact, normSquared, normSquaredExact
+    const double rb_row[16] = {r.eta, r.mu, nan, nan, solved ? double(r.retries) : nan, nan, r.alpha_max, nan, nan,
+                               r.delta_sum, nan, nan, r.slope, nan, r.norm_squared, nan};
+    robust.insert(robust.end(), rb_row, rb_row + 16);
+  }
+  for (int i = 0; i < n_att; ++i) {
+    const drape_attempt_record& r = arec[size_t(i)];
+    const double row[6] = {double(r.step), double(r.attempt), r.h, double(r.reason), double(r.record_start),
+                           double(r.record_end)};
+    attempts.insert(attempts.end(), row, row + 6);
+  }
   std::vector<float> eq(x.begin(), x.end()), states(x0.begin(), x0.end());
   states.insert(states.end(), eq.begin(), eq.end());
   bool ok = write_bytes(out + "/gpu-ptc.bin", ptc.data(), ptc.size() * sizeof(double)) &&
             write_bytes(out + "/gpu-equilibrium.bin", eq.data(), eq.size() * sizeof(float)) &&
             write_bytes(out + "/gpu-states.bin", states.data(), states.size() * sizeof(float)) &&
-            write_bytes(out + "/gpu-iterations.bin", nullptr, 0) && write_bytes(out + "/gpu-robust.bin", nullptr, 0) &&
-            write_bytes(out + "/gpu-attempts.bin", nullptr, 0);
+            write_bytes(out + "/gpu-iterations.bin", iterations.data(), iterations.size() * sizeof(double)) &&
+            write_bytes(out + "/gpu-robust.bin", robust.data(), robust.size() * sizeof(double)) &&
+            write_bytes(out + "/gpu-attempts.bin", attempts.data(), attempts.size() * sizeof(double));
   {
     std::ofstream f(out + "/gpu-equilibrium.json");
     char buf[256];
@@ -250,13 +285,12 @@ int main(int argc, char** argv) {
         "  \"final_relative_residual\": %.17g,\n  \"trajectory_ms\": %.6f,\n  \"ms_per_step\": %.6f,\n"
         "  \"device_ms\": %.6f,\n  \"phase_ms_per_step\": {\"assembly\": %.6f, \"pcg\": %.6f, \"line_search\": %.6f, "
         "\"ccd\": %.6f, \"other\": %.6f},\n  \"kernel_launches\": %d,\n  \"fallbacks_to_jacobi\": %d,\n"
-        "  \"record_tables\": \"gpu-iterations.bin, gpu-robust.bin and gpu-attempts.bin are empty: per-Newton and "
-        "per-attempt records are not kept\"\n}\n",
+        "  \"newton_records\": %d,\n  \"attempt_records\": %d\n}\n",
         prop.name, a.mode.c_str(), a.preconditioner.c_str(), int(drape::json_number(text, "", "grid_columns")), stop,
         o.max_steps, log.ptc_steps, log.rejected_attempts, log.newton_iterations, log.pcg_iterations, log.final_h,
         log.final_residual, log.final_relative_residual, 1e3 * log.seconds, 1e3 * log.seconds / steps,
         1e3 * log.device_seconds, log.ms_assembly / steps, log.ms_pcg / steps, log.ms_line_search / steps,
-        log.ms_ccd / steps, log.ms_other / steps, log.kernel_launches, log.fallbacks);
+        log.ms_ccd / steps, log.ms_other / steps, log.kernel_launches, log.fallbacks, n_rec, n_att);
     f << buf;
     ok = ok && bool(f);
   }

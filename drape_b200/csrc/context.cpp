@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 
 namespace drape {
 
@@ -420,29 +421,52 @@ AttemptResult Context::attempt(double h, double scale) {
     check(cudaMemcpyAsync(x_.ptr, xn_.ptr, nv * sizeof(double), cudaMemcpyDeviceToDevice, stream_), "start");
   }
   double mu = 0.0, eta = opt_.forcing ? 1e-2 : opt_.pcg_rtol, prev_norm = 0.0;
+  constexpr double kNaN = std::numeric_limits<double>::quiet_NaN();
   for (int it = 0;; ++it) {
     double norm = t_phase(kAssembly, [&] { return assemble(x_.ptr, inv_h2, mu, 0, true); });
     double rel = norm / scale;
+    // this iterate's record (robust-newton.ts records): completed below as the iterate proceeds
+    drape_newton_record rec{};
+    rec.step = record_step_;
+    rec.iteration = it;
+    rec.pcg_iterations = -1;
+    rec.halvings = -1;
+    rec.relative_residual = rel;
+    rec.norm_squared = norm * norm;
+    rec.linear_residual = rec.step_length = rec.eta = rec.alpha_max = rec.delta_sum = rec.slope = kNaN;
+    rec.mu = mu;
+    auto finish = [&](int status) {
+      rec.status = status;
+      records_.push_back(rec);
+    };
     if (!std::isfinite(rel)) {
+      finish(6);
       res.non_finite = true;
       return res;
     }
     if (rel <= opt_.inner_tolerance) {
+      finish(1);
       res.status = 0;
       return res;
     }
     if (it == opt_.inner_max) {
+      finish(2);
       res.status = 1;
       return res;
     }
     if (opt_.forcing) eta = it == 0 ? 1e-2 : next_forcing(eta, norm / prev_norm);
     prev_norm = norm;
+    rec.eta = eta;
+    rec.pcg_iterations = 0;
     double slope = 0.0;
     for (;;) {
       res.max_mu = std::max(res.max_mu, mu);
       kcheck(launch_rhs(host_.R, g_.ptr, b_.ptr, stream_), "rhs");
       PcgResult pr = direction_solve(eta, opt_.pcg_max_iterations);
       res.pcg_iterations += pr.iterations;
+      rec.pcg_iterations += pr.iterations;
+      rec.pcg_status = pr.status;
+      rec.linear_residual = pr.relative;
       check(cudaMemcpyAsync(sol_.ptr, px_.ptr, sizeof(float4) * host_.R, cudaMemcpyDeviceToDevice, stream_), "copy");
       if (opt_.refine && pr.status != kPcgBreakdown) {
         kcheck(launch_refine_residual(host_.R, row_ptr_.ptr, col_idx_.ptr, DevBsr{a0_.ptr, a1_.ptr, a2_.ptr}, g_.ptr,
@@ -450,6 +474,7 @@ AttemptResult Context::attempt(double h, double scale) {
               "refine");
         PcgResult pc = direction_solve(opt_.refine_rtol, opt_.pcg_max_iterations);
         res.pcg_iterations += pc.iterations;
+        rec.pcg_iterations += pc.iterations;
         if (pc.status != kPcgBreakdown) kcheck(launch_add_rows(host_.R, sol_.ptr, px_.ptr, stream_), "add");
       }
       if (host_.R < host_.V)  // fixed vertices keep a zero direction
@@ -457,17 +482,22 @@ AttemptResult Context::attempt(double h, double scale) {
       kcheck(launch_scatter_direction(dp_, sol_.ptr, d_.ptr, stream_), "scatter");
       kcheck(launch_slope(dp_, g_.ptr, d_.ptr, partial_.ptr, kReduceGrid, stream_), "slope");
       slope = reduce_partials(kReduceGrid, 0, kSlope);
+      rec.slope = slope;
       bool failed = pr.status == kPcgBreakdown || !(slope < 0.0);
       if (!failed) break;
       if (mu >= 1e3) {
+        finish(5);
         res.status = 3;
         return res;
       }
       mu = raise_mu(mu);
       res.mu_retries++;
+      rec.retries++;
+      rec.mu = mu;
       t_phase(kAssembly, [&] { return assemble(x_.ptr, inv_h2, mu, 0, true); });
     }
     double amax = t_phase(kCcd, [&] { return max_step(x_.ptr, d_.ptr); });
+    rec.alpha_max = amax;
     int halvings = -1;
     double alpha = 0.0;
     t_phase(kLineSearch, [&] {
@@ -477,15 +507,20 @@ AttemptResult Context::attempt(double h, double scale) {
         if (delta <= opt_.armijo * a * slope) {
           halvings = k;
           alpha = a;
+          rec.delta_sum = delta;
           break;
         }
       }
       return 0;
     });
     if (halvings < 0) {
+      finish(3);
       res.status = 2;
       return res;
     }
+    rec.halvings = halvings;
+    rec.step_length = alpha;
+    finish(0);
     kcheck(launch_axpy(int(nv), x_.ptr, alpha, d_.ptr, x_.ptr, stream_), "advance");
     res.updates++;
     res.halvings += halvings;
@@ -506,6 +541,8 @@ int Context::solve_equilibrium(const double* start, double h0, drape_run_log* lo
   std::memset(mg_outcome_, 0, sizeof mg_outcome_);
   mg_iterations_ = 0;
   steps_.clear();
+  records_.clear();
+  attempts_.clear();
   check(cudaEventRecord(ev_[4], stream_), "event");
   drape_run_log out{};
   out.gravity_load = L;
@@ -537,18 +574,40 @@ int Context::solve_equilibrium(const double* start, double h0, drape_run_log* lo
     AttemptResult res;
     double h_try = h;
     int rejected = 0;
+    record_step_ = int(steps_.size()) + 1;
+    auto log_attempt = [&](int index, double ht, int reason, int start) {
+      drape_attempt_record a{};
+      a.step = record_step_;
+      a.attempt = index;
+      a.reason = reason;
+      a.record_start = start;
+      a.record_end = int(records_.size());
+      a.h = ht;
+      attempts_.push_back(a);
+    };
+    // attempt outcome as the reference's REJECTION code (drape-e7.ts:11)
+    auto reason_of = [](const AttemptResult& a) {
+      if (a.non_finite) return 3;
+      if (a.updates == 0 && a.status == 3) return 1;
+      if (a.updates == 0 && a.status == 2) return 2;
+      return 0;
+    };
     for (; rejected <= opt_.max_rejections; ++rejected) {
       h_try = std::max(h * std::pow(opt_.shrink, rejected), h_floor);
+      int start = int(records_.size());
       res = attempt(h_try, r);
       bool failed = res.non_finite || (res.updates == 0 && (res.status == 2 || res.status == 3));
       if (!failed && opt_.curvature && res.status == 3 && res.updates > 0) {
         // mu-cap trigger: solve again without the b' d2d barrier term (drape-e7.ts:113-123).
+        log_attempt(rejected, h_try, 4, start);
+        start = int(records_.size());
         opt_.curvature = 0;
         AttemptResult again = attempt(h_try, r);
         opt_.curvature = 1;
         res = again;
         failed = res.non_finite || (res.updates == 0 && (res.status == 2 || res.status == 3));
       }
+      log_attempt(rejected, h_try, reason_of(res), start);
       if (!failed) {
         accepted = true;
         break;

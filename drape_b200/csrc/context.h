@@ -97,6 +97,8 @@ class Context {
   double static_energy();                          // E_s(x) at the current state
   int solve_equilibrium(const double* start, double h0, drape_run_log* log);
   const std::vector<drape_step_record>& steps() const { return steps_; }
+  const std::vector<drape_newton_record>& newton_records() const { return records_; }
+  const std::vector<drape_attempt_record>& attempt_records() const { return attempts_; }
 
   // Stand-alone timed SpMV of the assembled matrix (roofline measurement): average ms per launch.
   float time_spmv(int launches, int lanes_per_row, int threads);
@@ -239,6 +241,9 @@ class Context {
   PcgSyncHeader* pinned_state_ = nullptr;
   cudaEvent_t ev_[8] = {};
   std::vector<drape_step_record> steps_;
+  std::vector<drape_newton_record> records_;
+  std::vector<drape_attempt_record> attempts_;
+  int record_step_ = 0;  // PTC step the Newton records of the running attempt belong to
   double phase_ms_[6] = {};
   int partial_grid_ = 0;
 };

@@ -110,6 +110,26 @@ typedef struct {
   double h, residual, min_distance;
 } drape_step_record;
 
+/* One Newton iterate of a solve: the reference's IterationRecord and the RobustRecord fields this solver has
+ * (newton.ts:12-22, robust-newton.ts; gpu-iterations.bin and gpu-robust.bin rows, outputs.ts:8-10). The last iterate
+ * of an attempt takes no solve: pcg_iterations = -1 there (the reference's NaN). status: 0 running (an update was
+ * taken), 1 converged, 2 iteration limit, 3 line search failed, 5 regularisation (mu) cap (newton.ts:8), 6 non-finite
+ * residual. */
+typedef struct {
+  int32_t step, iteration, pcg_iterations, pcg_status, halvings, status, retries, pad;
+  double relative_residual, linear_residual, step_length; /* |g| / |g(x_n)|, PCG recursive residual, alpha */
+  double eta, mu, alpha_max, delta_sum, slope, norm_squared; /* forcing, regularisation, CCD bound, accepted
+                                                                 energy change, g.d, |g|^2 */
+} drape_newton_record;
+
+/* One attempt at a step size (AttemptLog, drape-e7.ts:26-32; gpu-attempts.bin rows): its Newton records are
+ * [record_start, record_end) of drape_newton_records. reason (drape-e7.ts:11): 0 accepted, 1 regularisation cap,
+ * 2 line search failed, 3 non-finite, 4 curvature retry (superseded by a run without the barrier's b'd2d term). */
+typedef struct {
+  int32_t step, attempt, reason, record_start, record_end, pad;
+  double h;
+} drape_attempt_record;
+
 /* Library version string. */
 const char* drape_version(void);
 
@@ -169,6 +189,10 @@ drape_status drape_solve_batch(drape_ctx* const* ctxs, int32_t count, int32_t wo
                                drape_status* statuses, double* solve_seconds, double* total_seconds);
 /* Copies up to `capacity` accepted-step records of the last solve; returns their total count in *count. */
 drape_status drape_step_records(const drape_ctx* ctx, drape_step_record* out, int32_t capacity, int32_t* count);
+/* The same for the last solve's Newton iterates (ctx.records of robust-newton.ts, gpu-iterations.bin and
+ * gpu-robust.bin) and its attempts (drape-e7.ts:116,138, gpu-attempts.bin). */
+drape_status drape_newton_records(const drape_ctx* ctx, drape_newton_record* out, int32_t capacity, int32_t* count);
+drape_status drape_attempt_records(const drape_ctx* ctx, drape_attempt_record* out, int32_t capacity, int32_t* count);
 
 /* Kernel-level entry points on host buffers (the parity checks of run-e7.ts:140-145 --checks):
  * g = grad Phi(x) with x_hat and step h (mode 0; Phi = (1/2h^2)(x - x_hat)^T M (x - x_hat) + Pi) or

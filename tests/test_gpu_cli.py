@@ -36,6 +36,25 @@ def test_cold_then_warm_reference_case():
         assert meta["dtype"] == "f32" and eq.size == 3 * meta["vertices"] and meta["final_h"] > 0
         states = np.fromfile(os.path.join(out, "gpu-states.bin"), np.float32)
         assert np.array_equal(states[eq.size:], eq)
+        # per-Newton and per-attempt tables: every accepted attempt's records add up to its gpu-ptc.bin row
+        it = np.fromfile(os.path.join(out, "gpu-iterations.bin"), np.float64).reshape(-1, 9)
+        rb = np.fromfile(os.path.join(out, "gpu-robust.bin"), np.float64).reshape(-1, 16)
+        at = np.fromfile(os.path.join(out, "gpu-attempts.bin"), np.float64).reshape(-1, 6)
+        assert len(it) == len(rb) == res["newton_records"] > 0 and len(at) == res["attempt_records"]
+        assert np.all(at[:, 4] <= at[:, 5]) and at[-1, 5] == len(it) and np.all(at[1:, 4] == at[:-1, 5])
+        accepted = at[at[:, 3] == 0]
+        assert len(accepted) == res["accepted_steps"] and np.array_equal(accepted[:, 0], ptc[:, 0])
+        for a, p in zip(accepted, ptc):
+            seg = it[int(a[4]):int(a[5])]
+            assert np.all(seg[:, 0] == p[0]) and np.array_equal(seg[:, 1], np.arange(len(seg)))
+            assert int((seg[:, 8] == 0).sum()) == p[3]  # updates = the step's inner count
+            assert int(np.nansum(seg[:, 3])) == p[5]    # PCG iterations of the step
+            # the last iterate ends the attempt: converged or at the limit without a solve, or a failed search
+            assert seg[-1, 8] != 0 and (np.isnan(seg[-1, 3]) or seg[-1, 8] in (3, 5))
+            assert a[2] == p[1]
+        upd = it[:, 8] == 0
+        assert np.all(it[upd, 6] >= 0) and np.all(it[upd, 6] <= rb[upd, 6])  # 0 <= alpha <= alpha_max
+        assert np.all(rb[upd, 12] < 0) and np.all(rb[upd, 9] <= 0)          # descent slope, Armijo decrease
         # warm start from the written equilibrium: already converged (f32 rounding of the state aside)
         _run("--case", t, "--mode", "warm", "--start", os.path.join(out, "gpu-equilibrium"))
         warm = json.load(open(os.path.join(t, "gpu-warm", "gpu-result.json")))
