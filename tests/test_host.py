@@ -130,12 +130,12 @@ def test_batch_solve_rejects_an_empty_batch(lib):
 def test_record_structs_match_the_header(tmp_path):
     """The ctypes views of the record structs have the C layout (sizes from the header, compiled here)."""
     src = tmp_path / "sizes.c"
-    src.write_text('#include <stdio.h>\n#include "drape_b200.h"\nint main(void) { printf("%zu %zu %zu %zu\\n", '
+    src.write_text('#include <stdio.h>\n#include "drape_b200.h"\nint main(void) { printf("%zu %zu %zu %zu %zu\\n", '
                    'sizeof(drape_newton_record), sizeof(drape_attempt_record), sizeof(drape_step_record), '
-                   'sizeof(drape_options)); return 0; }\n')
+                   'sizeof(drape_options), sizeof(drape_run_log)); return 0; }\n')
     exe = tmp_path / "sizes"
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
     sizes = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     import ctypes
     assert sizes == [ctypes.sizeof(api.NewtonRecord), ctypes.sizeof(api.AttemptRecord),
-                     ctypes.sizeof(api.StepRecord), ctypes.sizeof(api.Options)]
+                     ctypes.sizeof(api.StepRecord), ctypes.sizeof(api.Options), ctypes.sizeof(api.RunLog)]
