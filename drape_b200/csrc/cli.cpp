@@ -275,7 +275,7 @@ int main(int argc, char** argv) {
   const int steps = log.ptc_steps > 0 ? log.ptc_steps : 1;
   {
     std::ofstream f(out + "/gpu-result.json");
-    char buf[4096];
+    char buf[8192];
     std::snprintf(
         buf, sizeof buf,
         "{\n  \"schema\": \"e7-gpu/1\",\n  \"backend\": \"drape_b200-cuda\",\n  \"adapter\": \"%s\",\n  \"mode\": \"%s\",\n"
@@ -285,7 +285,14 @@ int main(int argc, char** argv) {
         "  \"final_relative_residual\": %.17g,\n  \"trajectory_ms\": %.6f,\n  \"ms_per_step\": %.6f,\n"
         "  \"device_ms\": %.6f,\n  \"phase_ms_per_step\": {\"assembly\": %.6f, \"pcg\": %.6f, \"line_search\": %.6f, "
         "\"ccd\": %.6f, \"other\": %.6f},\n  \"kernel_launches\": %d,\n  \"fallbacks_to_jacobi\": %d,\n"
-        "  \"newton_records\": %d,\n  \"attempt_records\": %d\n}\n",
+        "  \"newton_records\": %d,\n  \"attempt_records\": %d,\n"
+        // the column names of gpu-iterations.bin and gpu-robust.bin (outputs.ts:8-10; e4_compare.rs:61-70 reads the
+        // robust table by these names)
+        "  \"record_fields\": [\"step\", \"iteration\", \"relativeResidual\", \"pcgIterations\", \"pcgStatus\", "
+        "\"linearResidual\", \"stepLength\", \"halvings\", \"status\"],\n"
+        "  \"robust_fields\": [\"eta\", \"mu\", \"updateInf\", \"stepInf\", \"retries\", \"resolution\", \"alphaMax\", "
+        "\"limitingVertex\", \"minDistance\", \"deltaSum\", \"deltaAbs\", \"noiseOnly\", \"slope\", \"slopeExact\", "
+        "\"normSquared\", \"normSquaredExact\"]\n}\n",
         prop.name, a.mode.c_str(), a.preconditioner.c_str(), int(drape::json_number(text, "", "grid_columns")), stop,
         o.max_steps, log.ptc_steps, log.rejected_attempts, log.newton_iterations, log.pcg_iterations, log.final_h,
         log.final_residual, log.final_relative_residual, 1e3 * log.seconds, 1e3 * log.seconds / steps,

@@ -11,6 +11,7 @@ import pytest
 
 from drape_b200 import api
 from drape_b200.build import CLI
+from tests import e7_replays
 
 pytestmark = pytest.mark.gpu
 
@@ -55,6 +56,12 @@ def test_cold_then_warm_reference_case():
         upd = it[:, 8] == 0
         assert np.all(it[upd, 6] >= 0) and np.all(it[upd, 6] <= rb[upd, 6])  # 0 <= alpha <= alpha_max
         assert np.all(rb[upd, 12] < 0) and np.all(rb[upd, 9] <= 0)          # descent slope, Armijo decrease
+        # the reference comparer's replays of these tables (e7_compare.rs:240-248)
+        problem = json.load(open(os.path.join(t, "problem.json")))
+        _, fields, it2, rb2, at2, ptc2 = e7_replays.read_run(out)
+        assert e7_replays.forcing_replay(it2, rb2, fields, at2) <= 1e-5
+        assert e7_replays.controller_replay(problem, ptc2)
+        assert e7_replays.rejection_replay(it2, at2)
         # warm start from the written equilibrium: already converged (f32 rounding of the state aside)
         _run("--case", t, "--mode", "warm", "--start", os.path.join(out, "gpu-equilibrium"))
         warm = json.load(open(os.path.join(t, "gpu-warm", "gpu-result.json")))
