@@ -346,6 +346,25 @@ class Drape:
         self._check(self.lib.drape_max_step(self.h, _ptr(_f64(x)), _ptr(_f64(d)), ctypes.byref(out)))
         return out.value
 
+    def element_terms(self, x, exact=True):
+        """(grad [9T + 12H], hess [81T + 144H]) f32 element terms at x in the reference's per-element layout."""
+        fn = self.lib.drape_element_terms
+        fn.argtypes = [P, P, ctypes.c_int32, P, P]
+        g = np.zeros(9 * self.T + 12 * self.H, np.float32)
+        hs = np.zeros(81 * self.T + 144 * self.H, np.float32)
+        self._check(fn(self.h, _ptr(_f64(x)), int(exact), _ptr(g), _ptr(hs)))
+        return g, hs
+
+    def row_terms(self, x, x_hat, row_mass=None, mu=0.0, contact=False, curvature=True):
+        """(grad [3R], hess [9R]) f32 per-row inertia (row_mass: mass over h^2 per row) and barrier terms."""
+        fn = self.lib.drape_row_terms
+        fn.argtypes = [P, P, P, P, ctypes.c_double, ctypes.c_int32, ctypes.c_int32, P, P]
+        g = np.zeros(3 * self.R, np.float32)
+        hs = np.zeros(9 * self.R, np.float32)
+        self._check(fn(self.h, _ptr(_f64(x)), _ptr(_f64(x_hat)), _ptr(_f64(row_mass)), mu, int(contact), int(curvature),
+                       _ptr(g), _ptr(hs)))
+        return g, hs
+
     def static_residual(self, x=None):
         out = ctypes.c_double()
         self._check(self.lib.drape_static_residual(self.h, _ptr(_f64(x)), ctypes.byref(out)))

@@ -20,7 +20,8 @@ CLI = os.path.join(PKG, "drape")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc" if os.path.exists("/usr/local/cuda/bin/nvcc") else "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall", "-I", os.path.join(ROOT, "include")]
-LIB_SOURCES = ["elem.cu", "pcg.cu", "mg.cu", "nn.cu", "problem.cpp", "context.cpp", "capi.cpp", "noalloc.cu"]
+LIB_SOURCES = ["elem.cu", "pcg.cu", "mg.cu", "nn.cu", "checks.cu", "problem.cpp", "context.cpp", "capi.cpp",
+               "noalloc.cu"]
 CLI_SOURCES = ["cli.cpp"]
 
 

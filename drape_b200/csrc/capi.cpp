@@ -572,6 +572,23 @@ drape_status drape_static_energy(drape_ctx* ctx, const double* x, double* out) {
   });
 }
 
+drape_status drape_element_terms(drape_ctx* ctx, const double* x, int32_t exact, float* grad, float* hess) {
+  return guarded(ctx, [&](drape::Context& c) {
+    if (!x) return fail(ctx, "x is null", DRAPE_E_ARG);
+    c.element_terms_host(x, exact, grad, hess);
+    return DRAPE_OK;
+  });
+}
+
+drape_status drape_row_terms(drape_ctx* ctx, const double* x, const double* x_hat, const double* row_mass, double mu,
+                             int32_t contact, int32_t curvature, float* grad, float* hess) {
+  return guarded(ctx, [&](drape::Context& c) {
+    if (!x || !x_hat) return fail(ctx, "x and x_hat are required", DRAPE_E_ARG);
+    c.row_terms_host(x, x_hat, row_mass, mu, contact, curvature, grad, hess);
+    return DRAPE_OK;
+  });
+}
+
 drape_status drape_time_spmv(drape_ctx* ctx, int32_t launches, int32_t lanes_per_row, int32_t threads, float* ms) {
   return guarded(ctx, [&](drape::Context& c) {
     if (launches < 1 || !ms || threads < 32 || threads % 32 || threads > 1024) return fail(ctx, "invalid arguments", DRAPE_E_ARG);

@@ -2,7 +2,7 @@
 // flags: engine/gpu/src/node/run-e7.ts:37-43; its outputs: run-e7.ts:93-107, state-files.ts).
 //
 //   drape --case <dir> [--mode cold|warm|prolong] [--start <state prefix>]
-//         [--preconditioner jacobi|multilevel|learned] [--network <weights file>] [--device <n>]
+//         [--preconditioner jacobi|multilevel|learned] [--network <weights file>] [--device <n>] [--checks]
 //   environment: E7_BUDGET_S (time budget of the solve, s), E7_PROGRESS (one stderr line per accepted step)
 //
 // Reads <dir>/problem.json + problem.bin (`oracle e7-generate`), solves to equilibrium with the rules of the
@@ -16,6 +16,11 @@
 //   gpu-robust.bin                f64 [Newton iterates][16]: EXTRA_FIELDS (outputs.ts:9-10), NaN where this solver
 //                                 has no counterpart (update/step norms, resolution, limiting vertex, noise tests)
 //   gpu-attempts.bin              f64 [attempts][6]: step, attempt, h, reason, recordStart, recordEnd
+// and with --checks, before the solve (run-e7.ts:81-91, 140-145; the reference's probe runs are not made):
+//   gpu-kernel.bin                f32: exact element gradient [9T + 12H] and Hessian [81T + 144H], the projected
+//                                 ones, then the row terms [3R + 9R] at kernel_state, x_hat = rest, mu = kernel_mu
+//   gpu-contact-kernel.bin        f32 [3R + 9R]: the barrier row terms alone at contact_state
+//   gpu-inertia-h.bin             f32: the inertia row terms at kernel_state for h = 1/240, 0.1, 1 s
 // Exit status: 0 when the solve ran to a stop rule, 1 on an error, 2 on a usage error.
 #include <sys/stat.h>
 #include <unistd.h>
@@ -37,11 +42,12 @@ namespace {
 
 const char* kUsage =
     "usage: drape --case <case dir> [--mode cold|warm|prolong] [--start <state prefix>]\n"
-    "             [--preconditioner jacobi|multilevel|learned] [--network <weights>] [--device <n>]\n";
+    "             [--preconditioner jacobi|multilevel|learned] [--network <weights>] [--device <n>] [--checks]\n";
 
 struct Args {
   std::string dir, mode = "cold", start, preconditioner = "jacobi", network;
   int device = 0;
+  bool checks = false;
 };
 
 bool parse(int argc, char** argv, Args* a, std::string* err) {
@@ -59,6 +65,7 @@ bool parse(int argc, char** argv, Args* a, std::string* err) {
               : k == "--preconditioner" ? value(&a->preconditioner)
               : k == "--network" ? value(&a->network)
               : k == "--device" ? (value(&dev) && (a->device = std::atoi(dev.c_str()), true))
+              : k == "--checks" ? (a->checks = true, true)
                                 : false;
     if (!ok) {
       *err = "unknown or incomplete option " + k;
@@ -113,6 +120,74 @@ bool write_bytes(const std::string& path, const void* data, size_t n) {
 double rule(const std::string& text, const char* block, const char* key, double fallback) {
   const double v = drape::json_number(text, block, key);
   return std::isfinite(v) ? v : fallback;
+}
+
+// run-e7.ts --checks (runChecks, run-e7.ts:140-145; writeChecks, 81-91): the element and row terms at the problem's
+// check states, in the reference's layouts. Needs kernel_state, rest_positions, row_mass (and contact_state for the
+// contact file) in problem.bin, and the robust block's kernel_mu.
+bool write_checks(drape_ctx* ctx, const std::string& dir, const std::string& text, const std::string& out,
+                  const int64_t sizes[6], std::string* err) {
+  const size_t V = size_t(sizes[0]), T = size_t(sizes[1]), H = size_t(sizes[2]), R = size_t(sizes[3]);
+  std::vector<double> kernel_state, contact_state, rest, row_mass, unit_mass, colliders;
+  try {
+    kernel_state = drape::read_problem_array(dir, "kernel_state");
+    contact_state = drape::read_problem_array(dir, "contact_state");
+    rest = drape::read_problem_array(dir, "rest_positions");
+    row_mass = drape::read_problem_array(dir, "row_mass");
+    unit_mass = drape::read_problem_array(dir, "row_unit_mass_f64");
+    if (unit_mass.empty()) unit_mass = drape::read_problem_array(dir, "row_unit_mass");
+    colliders = drape::read_problem_array(dir, "colliders");
+  } catch (const std::exception& e) {
+    *err = e.what();
+    return false;
+  }
+  const double kernel_mu = drape::json_number(text, "robust", "kernel_mu");
+  if (kernel_state.size() != 3 * V || rest.size() != 3 * V || row_mass.size() != R || unit_mass.size() != R ||
+      !std::isfinite(kernel_mu)) {
+    *err = "--checks needs kernel_state, rest_positions, row_mass and row_unit_mass in problem.bin and "
+           "robust.kernel_mu in problem.json";
+    return false;
+  }
+  auto fail = [&](const char* what) {
+    *err = std::string(what) + ": " + drape_last_error(ctx);
+    return false;
+  };
+  std::vector<float> kernel, g(9 * T + 12 * H), h(81 * T + 144 * H), rg(3 * R), rh(9 * R);
+  for (int exact = 1; exact >= 0; --exact) {
+    if (drape_element_terms(ctx, kernel_state.data(), exact, g.data(), h.data()) != DRAPE_OK)
+      return fail("element terms");
+    kernel.insert(kernel.end(), g.begin(), g.end());
+    kernel.insert(kernel.end(), h.begin(), h.end());
+  }
+  if (drape_row_terms(ctx, kernel_state.data(), rest.data(), row_mass.data(), kernel_mu, 0, 1, rg.data(),
+                      rh.data()) != DRAPE_OK)
+    return fail("row terms");
+  kernel.insert(kernel.end(), rg.begin(), rg.end());
+  kernel.insert(kernel.end(), rh.begin(), rh.end());
+  bool ok = write_bytes(out + "/gpu-kernel.bin", kernel.data(), kernel.size() * sizeof(float));
+  if (contact_state.size() == 3 * V) {
+    // header word 3 of the collider array switches the barrier's curvature term off (contact-host.ts:92-97)
+    const int curvature = colliders.size() > 3 && colliders[3] != 0.0 ? 0 : 1;
+    if (drape_row_terms(ctx, contact_state.data(), contact_state.data(), nullptr, 0.0, 1, curvature, rg.data(),
+                        rh.data()) != DRAPE_OK)
+      return fail("contact terms");
+    std::vector<float> contact(rg.begin(), rg.end());
+    contact.insert(contact.end(), rh.begin(), rh.end());
+    ok = ok && write_bytes(out + "/gpu-contact-kernel.bin", contact.data(), contact.size() * sizeof(float));
+  }
+  std::vector<float> inertia;
+  for (double size : {1.0 / 240.0, 0.1, 1.0}) {
+    std::vector<double> mass(R);
+    for (size_t r = 0; r < R; ++r) mass[r] = double(float(unit_mass[r] / (size * size)));
+    if (drape_row_terms(ctx, kernel_state.data(), rest.data(), mass.data(), 0.0, 0, 1, rg.data(), rh.data()) !=
+        DRAPE_OK)
+      return fail("inertia terms");
+    inertia.insert(inertia.end(), rg.begin(), rg.end());
+    inertia.insert(inertia.end(), rh.begin(), rh.end());
+  }
+  ok = ok && write_bytes(out + "/gpu-inertia-h.bin", inertia.data(), inertia.size() * sizeof(float));
+  if (!ok) *err = "cannot write the check files in " + out;
+  return ok;
 }
 
 }  // namespace
@@ -194,6 +269,14 @@ int main(int argc, char** argv) {
       return 1;
     }
   }
+  const std::string out = a.dir + "/gpu-" + a.mode;
+  ::mkdir(out.c_str(), 0755);
+  if (a.checks && !write_checks(ctx, a.dir, text, out, sizes, &err)) {
+    std::fprintf(stderr, "drape: %s\n", err.c_str());
+    drape_destroy(ctx);
+    drape_network_destroy(net);
+    return 1;
+  }
   std::vector<double> x0(3 * V);
   drape_get_state(ctx, x0.data(), nullptr);
   if (!start.empty()) x0 = start;
@@ -213,8 +296,6 @@ int main(int argc, char** argv) {
   std::vector<drape_step_record> recs(size_t(count > 0 ? count : 1));
   drape_step_records(ctx, recs.data(), count, &count);
 
-  const std::string out = a.dir + "/gpu-" + a.mode;
-  ::mkdir(out.c_str(), 0755);
   std::vector<double> ptc;
   for (int i = 0; i < count; ++i) {
     const drape_step_record& r = recs[size_t(i)];

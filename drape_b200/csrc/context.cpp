@@ -759,6 +759,39 @@ double Context::max_step_host(const double* x, const double* d) {
   return max_step(xt_.ptr, d_.ptr);
 }
 
+void Context::element_terms_host(const double* x, int exact, float* grad, float* hess) {
+  xt_.upload(x, 3 * size_t(host_.V), stream_);
+  const size_t ng = 9 * size_t(host_.T) + 12 * size_t(host_.H), nh = 81 * size_t(host_.T) + 144 * size_t(host_.H);
+  DeviceArray<float> g, h;
+  g.alloc(ng);
+  h.alloc(nh);
+  kcheck(launch_element_terms(dp_, xt_.ptr, exact, g.ptr, h.ptr, stream_), "element terms");
+  if (grad) g.download(grad, ng, stream_);
+  if (hess) h.download(hess, nh, stream_);
+  sync();
+}
+
+void Context::row_terms_host(const double* x, const double* x_hat, const double* row_mass, double mu, int contact,
+                             int curvature, float* grad, float* hess) {
+  const size_t nv = 3 * size_t(host_.V), R = size_t(host_.R);
+  xt_.upload(x, nv, stream_);
+  d_.upload(x_hat, nv, stream_);
+  DeviceArray<double> m;
+  if (row_mass) {
+    m.alloc(R);
+    m.upload(row_mass, R, stream_);
+  }
+  DeviceArray<float> g, h;
+  g.alloc(3 * R);
+  h.alloc(9 * R);
+  kcheck(launch_row_terms(dp_, xt_.ptr, d_.ptr, row_mass ? m.ptr : nullptr, mu, contact, curvature, g.ptr, h.ptr,
+                          stream_),
+         "row terms");
+  if (grad) g.download(grad, 3 * R, stream_);
+  if (hess) h.download(hess, 9 * R, stream_);
+  sync();
+}
+
 double Context::static_energy_host(const double* x) {
   xt_.upload(x, 3 * size_t(host_.V), stream_);
   kcheck(launch_static_energy(dp_, xt_.ptr, partial_.ptr, kReduceGrid, stream_), "static_energy");

@@ -90,6 +90,10 @@ class Context {
   double energy_change_host(const double* x, const double* x_hat, double h, const double* d, double alpha, int mode);
   double max_step_host(const double* x, const double* d);
   double static_energy_host(const double* x);
+  // Kernel checks in the reference's per-element layout (checks.cu): element terms at x; row terms at x, x_hat.
+  void element_terms_host(const double* x, int exact, float* grad, float* hess);
+  void row_terms_host(const double* x, const double* x_hat, const double* row_mass, double mu, int contact,
+                      int curvature, float* grad, float* hess);
 
   // ---- device-resident operations
   double gravity_load() const { return gravity_load_; }

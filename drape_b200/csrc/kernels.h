@@ -117,4 +117,10 @@ cudaError_t launch_refine_residual(int R, const int* row_ptr, const int* col_idx
 // d += e (float4 rows).
 cudaError_t launch_add_rows(int R, float4* d, const float4* e, cudaStream_t s);
 
+// Kernel checks (checks.cu): element terms in the reference's per-element layout and per-row inertia/barrier terms.
+cudaError_t launch_element_terms(const DevProblem& p, const double* x, int exact, float* grad, float* hess,
+                                 cudaStream_t s);
+cudaError_t launch_row_terms(const DevProblem& p, const double* x, const double* x_hat, const double* row_mass,
+                             double mu, int contact, int curvature, float* grad, float* hess, cudaStream_t s);
+
 }  // namespace drape

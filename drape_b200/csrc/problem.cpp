@@ -377,6 +377,14 @@ HostProblem read_problem_files(const std::string& dir) {
   return p;
 }
 
+std::vector<double> read_problem_array(const std::string& dir, const std::string& name) {
+  std::string text = read_all(dir + "/problem.json");
+  const size_t at = text.find("\"arrays\"");
+  if (at == std::string::npos) return {};
+  Manifest m{text.substr(at), read_all(dir + "/problem.bin")};
+  return m.get<double>(name, false);
+}
+
 void write_problem_files(const HostProblem& p, const std::string& dir) {
   mkdir(dir.c_str(), 0755);
   std::string bytes, manifest = "[";

@@ -49,6 +49,9 @@ HostProblem reference_problem(int columns, const std::string& edit);
 // Reads a problem.json / problem.bin pair written by the reference's `oracle e7-generate` (or the oracle
 // restatement); f64 copies of the geometry arrays are used when present. Throws std::runtime_error.
 HostProblem read_problem_files(const std::string& dir);
+// One named array of a problem.bin as f64 (empty when the manifest has no such array): the check states
+// kernel_state and contact_state and the per-row row_mass of the reference's files (e3_generate.rs:93-98).
+std::vector<double> read_problem_array(const std::string& dir, const std::string& name);
 // The whole file as text (throws if it cannot be read).
 std::string read_text_file(const std::string& path);
 // The number at the first "key": after the first "anchor" of a JSON text (NaN if absent): the flat key scan the

@@ -216,6 +216,20 @@ drape_status drape_max_step(drape_ctx* ctx, const double* x, const double* d, do
  * e7_ptc.rs:43-51). */
 drape_status drape_static_residual(drape_ctx* ctx, const double* x, double* out);
 drape_status drape_static_energy(drape_ctx* ctx, const double* x, double* out);
+/* Element terms at x (3V f64) in the reference's per-element layout, f32 (each may be NULL): grad [9T + 12H] with
+ * triangle e at 9e + 3k + i and hinge h at 9T + 12h + 3k + i; hess [81T + 144H] with triangle block (k, l) at
+ * 81e + 9(3k + l) and hinge block (k, l) at 81T + 144h + 9(4k + l), 3x3 row-major. exact 1: StVK stress and the
+ * hinge's 2c(grad grad^T + theta d2 theta); 0: positive-part stress in the geometric term and Gauss-Newton hinge
+ * (replaces the exactElements / projectedElements passes of evaluateDrapeKernels, drape-step.ts:83-97;
+ * membrane_element.wgsl, hinge_element.wgsl). */
+drape_status drape_element_terms(drape_ctx* ctx, const double* x, int32_t exact, float* grad, float* hess);
+/* Row terms at x with prediction x_hat (3V f64 each), f32 (each may be NULL): grad [3R] = m_r (x - x_hat) +
+ * sum b'(d) n, hess [9R] = m_r (1 + mu) I + sum b''(d) n n^T + b'(d) kappa (I - n n^T) over the active colliders
+ * when `contact` (the kappa term when `curvature`), with row_mass [R] the per-row mass over h^2 (NULL: 0)
+ * (replaces the inertia pass of evaluateKernelsWithInertia, evaluateContactKernel and evaluateInertiaAtSteps,
+ * drape-e4.ts:108-120, contact-host.ts:76-90, drape-e7.ts:203-218; inertia.wgsl). */
+drape_status drape_row_terms(drape_ctx* ctx, const double* x, const double* x_hat, const double* row_mass, double mu,
+                             int32_t contact, int32_t curvature, float* grad, float* hess);
 
 /* The multilevel preconditioner (no counterpart in the reference): z = M r, one V-cycle for the given f32 blocks
  * (NULL: the last assembled matrix) and rhs r (3R f64, rounded to f32); z is 3R f64. */
