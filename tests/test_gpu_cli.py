@@ -57,10 +57,14 @@ def test_cold_then_warm_reference_case():
         assert np.all(it[upd, 6] >= 0) and np.all(it[upd, 6] <= rb[upd, 6])  # 0 <= alpha <= alpha_max
         assert np.all(rb[upd, 12] < 0) and np.all(rb[upd, 9] <= 0)          # descent slope, Armijo decrease
         # the reference comparer's replays of these tables (e7_compare.rs:240-248)
-        problem = json.load(open(os.path.join(t, "problem.json")))
+        # the command's step rules: the problem's "ptc" block over the library defaults it falls back to
+        o = api.default_options()
+        rules = {"growth": o.growth, "shrink": o.shrink, "inner_max_iterations": o.inner_max, "h0": o.h0,
+                 "h_min_factor": o.h_min_factor, "h_max": o.h_max}
+        rules.update(json.load(open(os.path.join(t, "problem.json"))).get("ptc", {}))
         _, fields, it2, rb2, at2, ptc2 = e7_replays.read_run(out)
         assert e7_replays.forcing_replay(it2, rb2, fields, at2) <= 1e-5
-        assert e7_replays.controller_replay(problem, ptc2)
+        assert e7_replays.controller_replay({"ptc": rules}, ptc2)
         assert e7_replays.rejection_replay(it2, at2)
         # warm start from the written equilibrium: already converged (f32 rounding of the state aside)
         _run("--case", t, "--mode", "warm", "--start", os.path.join(out, "gpu-equilibrium"))
