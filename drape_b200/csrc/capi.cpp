@@ -327,6 +327,23 @@ drape_status drape_newton_records(const drape_ctx* cctx, drape_newton_record* ou
   });
 }
 
+drape_status drape_keep_states(drape_ctx* ctx, int32_t keep) {
+  return guarded(ctx, [&](drape::Context& c) {
+    c.set_keep_states(keep != 0);
+    return DRAPE_OK;
+  });
+}
+
+drape_status drape_step_states(const drape_ctx* cctx, float* out, int64_t capacity, int64_t* count) {
+  auto* ctx = const_cast<drape_ctx*>(cctx);
+  return guarded(ctx, [&](drape::Context& c) {
+    const auto& s = c.step_states();
+    if (count) *count = int64_t(s.size());
+    if (out && capacity > 0) std::copy(s.begin(), s.begin() + std::min<int64_t>(capacity, int64_t(s.size())), out);
+    return DRAPE_OK;
+  });
+}
+
 drape_status drape_attempt_records(const drape_ctx* cctx, drape_attempt_record* out, int32_t capacity,
                                    int32_t* count) {
   auto* ctx = const_cast<drape_ctx*>(cctx);

@@ -11,7 +11,8 @@
 //   gpu-result.json               schema e7-gpu/1: the run-e7.ts fields this solver records
 //   gpu-ptc.bin                   f64 [accepted steps][7]: step, h, residual, inner, rejected, pcgIterations, minDistance
 //   gpu-equilibrium.{json,bin}    the equilibrium as an f32 state file with its final_h
-//   gpu-states.bin                f32: the start state, then the equilibrium
+//   gpu-states.bin                f32: the start state, then every accepted state (grids of <= 65 columns) or
+//                                 the equilibrium alone
 //   gpu-iterations.bin            f64 [Newton iterates][9]: the reference's RECORD_FIELDS (outputs.ts:8)
 //   gpu-robust.bin                f64 [Newton iterates][16]: EXTRA_FIELDS (outputs.ts:9-10), NaN where this solver
 //                                 has no counterpart (update/step norms, resolution, limiting vertex, noise tests)
@@ -269,6 +270,9 @@ int main(int argc, char** argv) {
       return 1;
     }
   }
+  // every accepted state is kept for grids of at most 65 columns (run-e7.ts:29,133)
+  const bool keep_states = drape::json_number(text, "", "grid_columns") <= 65;
+  drape_keep_states(ctx, keep_states ? 1 : 0);
   const std::string out = a.dir + "/gpu-" + a.mode;
   ::mkdir(out.c_str(), 0755);
   if (a.checks && !write_checks(ctx, a.dir, text, out, sizes, &err)) {
@@ -334,8 +338,17 @@ int main(int argc, char** argv) {
                            double(r.record_end)};
     attempts.insert(attempts.end(), row, row + 6);
   }
+  // the start state, then every accepted state (small grids) or the equilibrium alone (drape-e7.ts:159,175-178)
   std::vector<float> eq(x.begin(), x.end()), states(x0.begin(), x0.end());
-  states.insert(states.end(), eq.begin(), eq.end());
+  if (keep_states) {
+    int64_t n_states = 0;
+    drape_step_states(ctx, nullptr, 0, &n_states);
+    std::vector<float> kept(size_t(n_states > 0 ? n_states : 1));
+    drape_step_states(ctx, kept.data(), n_states, &n_states);
+    states.insert(states.end(), kept.begin(), kept.begin() + n_states);
+  } else {
+    states.insert(states.end(), eq.begin(), eq.end());
+  }
   bool ok = write_bytes(out + "/gpu-ptc.bin", ptc.data(), ptc.size() * sizeof(double)) &&
             write_bytes(out + "/gpu-equilibrium.bin", eq.data(), eq.size() * sizeof(float)) &&
             write_bytes(out + "/gpu-states.bin", states.data(), states.size() * sizeof(float)) &&

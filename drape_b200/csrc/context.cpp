@@ -543,6 +543,7 @@ int Context::solve_equilibrium(const double* start, double h0, drape_run_log* lo
   steps_.clear();
   records_.clear();
   attempts_.clear();
+  states_.clear();
   check(cudaEventRecord(ev_[4], stream_), "event");
   drape_run_log out{};
   out.gravity_load = L;
@@ -629,6 +630,12 @@ int Context::solve_equilibrium(const double* start, double h0, drape_run_log* lo
     kcheck(launch_min_distance(dp_, x_.ptr, partial_.ptr, kReduceGrid, stream_), "min_distance");
     rec.min_distance = reduce_partials(kReduceGrid, 1, kMinDist);
     steps_.push_back(rec);
+    if (keep_states_) {  // the accepted state in f32 (drape-e7.ts:175)
+      std::vector<double> xs(nv);
+      x_.download(xs.data(), nv, stream_);
+      sync();
+      states_.insert(states_.end(), xs.begin(), xs.end());
+    }
     out.newton_iterations += res.updates;
     out.pcg_iterations += res.pcg_iterations;
     out.mu_retries += res.mu_retries;

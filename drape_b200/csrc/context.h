@@ -103,6 +103,9 @@ class Context {
   const std::vector<drape_step_record>& steps() const { return steps_; }
   const std::vector<drape_newton_record>& newton_records() const { return records_; }
   const std::vector<drape_attempt_record>& attempt_records() const { return attempts_; }
+  // With `on`, every accepted PTC state of a solve is kept in f32 (3V floats per step, in step order).
+  void set_keep_states(bool on) { keep_states_ = on; }
+  const std::vector<float>& step_states() const { return states_; }
 
   // Stand-alone timed SpMV of the assembled matrix (roofline measurement): average ms per launch.
   float time_spmv(int launches, int lanes_per_row, int threads);
@@ -247,6 +250,8 @@ class Context {
   std::vector<drape_step_record> steps_;
   std::vector<drape_newton_record> records_;
   std::vector<drape_attempt_record> attempts_;
+  bool keep_states_ = false;
+  std::vector<float> states_;
   int record_step_ = 0;  // PTC step the Newton records of the running attempt belong to
   double phase_ms_[6] = {};
   int partial_grid_ = 0;

@@ -193,6 +193,12 @@ drape_status drape_step_records(const drape_ctx* ctx, drape_step_record* out, in
  * gpu-robust.bin) and its attempts (drape-e7.ts:116,138, gpu-attempts.bin). */
 drape_status drape_newton_records(const drape_ctx* ctx, drape_newton_record* out, int32_t capacity, int32_t* count);
 drape_status drape_attempt_records(const drape_ctx* ctx, drape_attempt_record* out, int32_t capacity, int32_t* count);
+/* keep = 1: later solves keep every accepted PTC state (f32), the reference's keepStates (drape-e7.ts:156-178, on
+ * for grids of at most 65 columns, run-e7.ts:29,133). drape_step_states copies up to `capacity` floats of the last
+ * solve's states (3V per accepted step, in step order; the start state is not among them) and returns their total
+ * count in *count. */
+drape_status drape_keep_states(drape_ctx* ctx, int32_t keep);
+drape_status drape_step_states(const drape_ctx* ctx, float* out, int64_t capacity, int64_t* count);
 
 /* Kernel-level entry points on host buffers (the parity checks of run-e7.ts:140-145 --checks):
  * g = grad Phi(x) with x_hat and step h (mode 0; Phi = (1/2h^2)(x - x_hat)^T M (x - x_hat) + Pi) or

@@ -36,7 +36,9 @@ def test_cold_then_warm_reference_case():
         eq = np.fromfile(os.path.join(out, "gpu-equilibrium.bin"), np.float32)
         assert meta["dtype"] == "f32" and eq.size == 3 * meta["vertices"] and meta["final_h"] > 0
         states = np.fromfile(os.path.join(out, "gpu-states.bin"), np.float32)
-        assert np.array_equal(states[eq.size:], eq)
+        # n17 <= 65 columns: the start, then every accepted state; the last is the equilibrium
+        assert states.size == (res["accepted_steps"] + 1) * eq.size
+        assert np.array_equal(states[-eq.size:], eq)
         # per-Newton and per-attempt tables: every accepted attempt's records add up to its gpu-ptc.bin row
         it = np.fromfile(os.path.join(out, "gpu-iterations.bin"), np.float64).reshape(-1, 9)
         rb = np.fromfile(os.path.join(out, "gpu-robust.bin"), np.float64).reshape(-1, 16)
