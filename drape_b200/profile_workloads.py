@@ -5,6 +5,7 @@
     python -m drape_b200.profile_workloads spmv    [--drapes 128]          # batched and n257 BSR SpMV, autotuned
     python -m drape_b200.profile_workloads solve   [--n 129] [--preconditioner learned] [--out state.npy] [--budget s]
     python -m drape_b200.profile_workloads batch   [--drapes 128] [--workers 32] [--budget s]   # concurrent solves
+    torchrun --nproc-per-node N -m drape_b200.profile_workloads batch ...   # the drapes split over N GPUs
 
 batch solves the same `drapes` sheets cold (learned preconditioner unless --preconditioner says otherwise) through
 drape_solve_batch, `workers` at a time, and reports solves/s and the p50/p99 of the per-drape solve times.
@@ -28,7 +29,7 @@ import sys
 
 import numpy as np
 
-from drape_b200 import api
+from drape_b200 import api, batch_shards
 
 GRAVITY = np.array([0.0, -9.81, 0.0])
 
@@ -69,37 +70,61 @@ def batch_scenes(drapes):
 
 
 def batch_workload(drapes, workers, budget, preconditioner):
-    """Every drape of the batched configuration solved cold to |grad E_s| <= 1e-6 N, `workers` at a time."""
-    net = api.Network.trained() if preconditioner == 2 else None
+    """Every drape of the batched configuration solved cold to |grad E_s| <= 1e-6 N, `workers` at a time. Under
+    torchrun (WORLD_SIZE > 1, one process per GPU) each rank solves its row-balanced share on its own GPU
+    (drape_b200.batch_shards) and the ranks combine only their results; rank 0 returns the job's line."""
+    world, rank = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    scenes = batch_scenes(drapes)
+    mine = batch_shards.partition([n * n for n, _, _, _ in scenes], world)[rank]
+    dist, device = None, None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as td
+
+        torch.cuda.set_device(local)
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=600 + 2 * budget))
+        dist, device = td, f"cuda:{local}"
+    net = api.Network.trained(device=local) if preconditioner == 2 else None
     ds = []
-    for n, seed, radius, young in batch_scenes(drapes):
-        d = api.Drape.sheet(n, seed=seed, radius=radius, young=young, plane=True,
+    for i in mine:
+        n, seed, radius, young = scenes[i]
+        d = api.Drape.sheet(n, seed=seed, radius=radius, young=young, plane=True, device=local,
                             options=api.default_options(preconditioner=preconditioner, time_budget_s=budget))
         if net is not None:
             d.set_network(net)
         ds.append(d)
-    logs, seconds, total = api.solve_batch(ds, workers, check=False)
-    sizes = [s[0] for s in batch_scenes(drapes)]
-    done = [i for i, g in enumerate(logs) if g["status"] == 0]
+    logs, seconds, total = api.solve_batch(ds, workers, check=False) if ds else ([], np.zeros(0), 0.0)
+    local_counts = {"solved": sum(g["status"] == 0 for g in logs), "newton": sum(g["newton_iterations"] for g in logs),
+                    "pcg": sum(g["pcg_iterations"] for g in logs), "fallbacks": sum(g["fallbacks"] for g in logs),
+                    "sum_device_s": sum(g["device_seconds"] for g in logs)}
+    for g in logs:
+        key = "reason_" + g["reason"]
+        local_counts[key] = local_counts.get(key, 0) + 1
+    for k in ("reason_tolerance", "reason_cap", "reason_stalled", "reason_time_budget"):
+        local_counts.setdefault(k, 0)
+    total, counts, seconds_all = batch_shards.combine(total, local_counts, seconds, mine, drapes, dist, device)
+    for d in ds:
+        d.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    sizes = [s[0] for s in scenes]
     per_n = {}
     for n in sorted(set(sizes)):
         idx = [i for i in range(drapes) if sizes[i] == n]
-        per_n[str(n)] = {"drapes": len(idx), "median_s": float(np.median(seconds[idx])),
-                         "median_newton": float(np.median([logs[i]["newton_iterations"] for i in idx])),
-                         "pcg_per_newton": sum(logs[i]["pcg_iterations"] for i in idx) /
-                         max(1, sum(logs[i]["newton_iterations"] for i in idx))}
-    reasons = {}
-    for g in logs:
-        reasons[g["reason"]] = reasons.get(g["reason"], 0) + 1
-    out = {"workload": "batch", "drapes": drapes, "workers": workers, "preconditioner": preconditioner,
-           "budget_s": budget, "solved": len(done), "total_s": total, "solves_per_s": len(done) / total,
-           "p50_s": float(np.percentile(seconds, 50)), "p99_s": float(np.percentile(seconds, 99)),
-           "max_s": float(seconds.max()), "sum_device_s": float(sum(g["device_seconds"] for g in logs)),
-           "newton": int(sum(g["newton_iterations"] for g in logs)), "pcg": int(sum(g["pcg_iterations"] for g in logs)),
-           "fallbacks": int(sum(g["fallbacks"] for g in logs)), "reasons": reasons, "per_columns": per_n}
-    for d in ds:
-        d.close()
-    return out
+        per_n[str(n)] = {"drapes": len(idx), "median_s": float(np.median(seconds_all[idx]))}
+    solved = int(round(counts["solved"]))
+    return {"workload": "batch", "drapes": drapes, "workers": workers, "n_gpus": world,
+            "preconditioner": preconditioner, "budget_s": budget, "solved": solved, "total_s": total,
+            "solves_per_s": solved / total if total > 0 else 0.0,
+            "p50_s": float(np.percentile(seconds_all, 50)), "p99_s": float(np.percentile(seconds_all, 99)),
+            "max_s": float(seconds_all.max()), "sum_device_s": counts["sum_device_s"],
+            "newton": int(round(counts["newton"])), "pcg": int(round(counts["pcg"])),
+            "fallbacks": int(round(counts["fallbacks"])),
+            "reasons": {k[len("reason_"):]: int(round(v)) for k, v in counts.items() if k.startswith("reason_") and v},
+            "per_columns": per_n}
 
 
 def spmv_workload(drapes):
@@ -169,7 +194,9 @@ def main(argv=None):
         # more hardware queues than the default 8, for streams of many drapes (read when CUDA starts)
         os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
         pre = {"jacobi": 0, "multilevel": 1, "learned": 2}[args.preconditioner]
-        print(json.dumps(batch_workload(args.drapes, args.workers, args.budget, pre)), flush=True)
+        out = batch_workload(args.drapes, args.workers, args.budget, pre)
+        if int(os.environ.get("RANK", "0")) == 0:
+            print(json.dumps(out), flush=True)
         return 0
     if args.workload == "solve":
         # the bench scene's full cold solve; the converged positions go to --out for an f64 error check
@@ -182,8 +209,9 @@ def main(argv=None):
         log = d.solve_equilibrium(check=False)
         if args.out:
             np.save(args.out, d.state)
-        print(json.dumps({k: log[k] for k in ("reason", "ptc_steps", "newton_iterations", "pcg_iterations", "fallbacks", "ms_pcg",
-                                              "final_residual", "device_seconds", "static_energy")}), flush=True)
+        keys = ("reason", "ptc_steps", "newton_iterations", "pcg_iterations", "fallbacks", "ms_pcg", "final_residual",
+                "device_seconds", "static_energy")
+        print(json.dumps({k: log[k] for k in keys}), flush=True)
         return 0
     d, blocks, b = system(args.n, args.steps)
     lib = api.load()
