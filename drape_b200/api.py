@@ -82,7 +82,7 @@ class NewtonRecord(ctypes.Structure):
     _fields_ = [(k, ctypes.c_int32) for k in ("step", "iteration", "pcg_iterations", "pcg_status", "halvings",
                                               "status", "retries", "pad")] + \
                [(k, ctypes.c_double) for k in ("relative_residual", "linear_residual", "step_length", "eta", "mu",
-                                               "alpha_max", "delta_sum", "slope", "norm_squared")]
+                                               "alpha_max", "delta_sum", "slope", "norm_squared", "resolution")]
 
 
 class AttemptRecord(ctypes.Structure):
@@ -295,6 +295,39 @@ class Drape:
     def attempt_records(self):
         """The last solve's attempts (drape_attempt_records; gpu-attempts.bin rows)."""
         return self._records(self.lib.drape_attempt_records, AttemptRecord)
+
+    def keep_states(self, keep=True):
+        """Later solves keep every accepted state (drape_keep_states); step_states() returns them, [steps, 3V] f32."""
+        self.lib.drape_keep_states.argtypes = [P, ctypes.c_int32]
+        self._check(self.lib.drape_keep_states(self.h, int(keep)))
+
+    def step_states(self):
+        fn = self.lib.drape_step_states
+        fn.argtypes = [P, P, ctypes.c_int64, P]
+        n = ctypes.c_int64()
+        self._check(fn(self.h, None, 0, ctypes.byref(n)))
+        out = np.zeros(n.value, np.float32)
+        self._check(fn(self.h, _ptr(out), n.value, ctypes.byref(n)))
+        return out.reshape(-1, 3 * self.V)
+
+    def probe(self, probes):
+        """PTC probes (drape_probe_begin / drape_probe_step): one logged Newton attempt per (step, h, positions).
+        Returns (Newton records, iterates [n, 3V] f32, direction pairs [m, 2, 3V] f32, trials [k, 8] f64)."""
+        lib = self.lib
+        lib.drape_probe_begin.argtypes = [P]
+        lib.drape_probe_step.argtypes = [P, P, ctypes.c_double, ctypes.c_int32]
+        lib.drape_probe_logs.argtypes = [P, P, ctypes.c_int64, P, P, ctypes.c_int64, P, P, ctypes.c_int64, P]
+        self._check(lib.drape_probe_begin(self.h))
+        for step, h, x in probes:
+            self._check(lib.drape_probe_step(self.h, _ptr(_f64(x)), h, int(step)))
+        ni, nd, nt = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        self._check(lib.drape_probe_logs(self.h, None, 0, ctypes.byref(ni), None, 0, ctypes.byref(nd), None, 0,
+                                         ctypes.byref(nt)))
+        it, dr, tr = np.zeros(ni.value, np.float32), np.zeros(nd.value, np.float32), np.zeros(nt.value)
+        self._check(lib.drape_probe_logs(self.h, _ptr(it), ni.value, ctypes.byref(ni), _ptr(dr), nd.value,
+                                         ctypes.byref(nd), _ptr(tr), nt.value, ctypes.byref(nt)))
+        return (self.newton_records(), it.reshape(-1, 3 * self.V), dr.reshape(-1, 2, 3 * self.V),
+                tr.reshape(-1, 8))
 
     def assemble(self, x, x_hat=None, h=0.0, mu=0.0, mode=0, curvature=False, blocks=True):
         g = np.zeros(3 * self.R)

@@ -327,6 +327,38 @@ drape_status drape_newton_records(const drape_ctx* cctx, drape_newton_record* ou
   });
 }
 
+drape_status drape_probe_begin(drape_ctx* ctx) {
+  return guarded(ctx, [&](drape::Context& c) {
+    c.probe_begin();
+    return DRAPE_OK;
+  });
+}
+
+drape_status drape_probe_step(drape_ctx* ctx, const double* xyz, double h, int32_t step) {
+  return guarded(ctx, [&](drape::Context& c) {
+    if (!xyz || !(h > 0)) return fail(ctx, "drape_probe_step needs positions and h > 0", DRAPE_E_ARG);
+    c.probe_step(xyz, h, step);
+    return DRAPE_OK;
+  });
+}
+
+drape_status drape_probe_logs(const drape_ctx* cctx, float* iterates, int64_t iterates_capacity,
+                              int64_t* iterates_count, float* directions, int64_t directions_capacity,
+                              int64_t* directions_count, double* trials, int64_t trials_capacity,
+                              int64_t* trials_count) {
+  auto* ctx = const_cast<drape_ctx*>(cctx);
+  return guarded(ctx, [&](drape::Context& c) {
+    auto copy = [](const auto& v, auto* out, int64_t cap, int64_t* count) {
+      if (count) *count = int64_t(v.size());
+      if (out && cap > 0) std::copy(v.begin(), v.begin() + std::min<int64_t>(cap, int64_t(v.size())), out);
+    };
+    copy(c.probe_iterates(), iterates, iterates_capacity, iterates_count);
+    copy(c.probe_directions(), directions, directions_capacity, directions_count);
+    copy(c.probe_trials(), trials, trials_capacity, trials_count);
+    return DRAPE_OK;
+  });
+}
+
 drape_status drape_keep_states(drape_ctx* ctx, int32_t keep) {
   return guarded(ctx, [&](drape::Context& c) {
     c.set_keep_states(keep != 0);

@@ -17,11 +17,13 @@
 //   gpu-robust.bin                f64 [Newton iterates][16]: EXTRA_FIELDS (outputs.ts:9-10), NaN where this solver
 //                                 has no counterpart (update/step norms, resolution, limiting vertex, noise tests)
 //   gpu-attempts.bin              f64 [attempts][6]: step, attempt, h, reason, recordStart, recordEnd
-// and with --checks, before the solve (run-e7.ts:81-91, 140-145; the reference's probe runs are not made):
+// and with --checks, before the solve (run-e7.ts:81-91, 140-152):
 //   gpu-kernel.bin                f32: exact element gradient [9T + 12H] and Hessian [81T + 144H], the projected
 //                                 ones, then the row terms [3R + 9R] at kernel_state, x_hat = rest, mu = kernel_mu
 //   gpu-contact-kernel.bin        f32 [3R + 9R]: the barrier row terms alone at contact_state
 //   gpu-inertia-h.bin             f32: the inertia row terms at kernel_state for h = 1/240, 0.1, 1 s
+//   gpu-probe-{iterations,robust}.bin, gpu-probe-iterates.bin, gpu-probe-directions.bin, gpu-probe-search.bin:
+//                                 the PTC probes of the case's probes.json / probes.bin, when it has them
 // Exit status: 0 when the solve ran to a stop rule, 1 on an error, 2 on a usage error.
 #include <sys/stat.h>
 #include <unistd.h>
@@ -118,6 +120,36 @@ bool write_bytes(const std::string& path, const void* data, size_t n) {
   return bool(f);
 }
 
+// gpu-<prefix>iterations.bin (RECORD_FIELDS) and gpu-<prefix>robust.bin (EXTRA_FIELDS) of the context's Newton records
+// (writeRun, outputs.ts:24-28): f64 rows, NaN where the reference's field has no counterpart in this solver or no
+// value on the iterate (the last iterate of an attempt takes no solve).
+bool write_run_tables(drape_ctx* ctx, const std::string& out, const std::string& prefix, int32_t* count) {
+  const double nan = std::nan("");
+  int32_t n = 0;
+  drape_newton_records(ctx, nullptr, 0, &n);
+  std::vector<drape_newton_record> rec(size_t(n > 0 ? n : 1));
+  drape_newton_records(ctx, rec.data(), n, &n);
+  std::vector<double> iterations, robust;
+  for (int i = 0; i < n; ++i) {
+    const drape_newton_record& r = rec[size_t(i)];
+    const bool solved = r.pcg_iterations >= 0;
+    const double it_row[9] = {double(r.step), double(r.iteration), r.relative_residual,
+                              solved ? double(r.pcg_iterations) : nan, solved ? double(r.pcg_status) : nan,
+                              solved ? r.linear_residual : nan, r.step_length,
+                              r.halvings >= 0 ? double(r.halvings) : nan, double(r.status)};
+    iterations.insert(iterations.end(), it_row, it_row + 9);
+    // eta, mu, updateInf, stepInf, retries, resolution, alphaMax, limitingVertex, minDistance, deltaSum, deltaAbs,
+    // noiseOnly, slope, slopeExact, normSquared, normSquaredExact
+    const double rb_row[16] = {r.eta, r.mu, nan, nan, solved ? double(r.retries) : nan, r.resolution, r.alpha_max,
+                               nan, nan, r.delta_sum, nan, nan, r.slope, nan, r.norm_squared, nan};
+    robust.insert(robust.end(), rb_row, rb_row + 16);
+  }
+  *count = n;
+  const std::string base = out + "/gpu-" + prefix;
+  return write_bytes(base + "iterations.bin", iterations.data(), iterations.size() * sizeof(double)) &&
+         write_bytes(base + "robust.bin", robust.data(), robust.size() * sizeof(double));
+}
+
 double rule(const std::string& text, const char* block, const char* key, double fallback) {
   const double v = drape::json_number(text, block, key);
   return std::isfinite(v) ? v : fallback;
@@ -187,7 +219,42 @@ bool write_checks(drape_ctx* ctx, const std::string& dir, const std::string& tex
     inertia.insert(inertia.end(), rh.begin(), rh.end());
   }
   ok = ok && write_bytes(out + "/gpu-inertia-h.bin", inertia.data(), inertia.size() * sizeof(float));
-  if (!ok) *err = "cannot write the check files in " + out;
+  if (!ok) {
+    *err = "cannot write the check files in " + out;
+    return false;
+  }
+  // PTC probes when the case has them (probes.json / probes.bin of the oracle's cold base solves; run-e7.ts:65-79,
+  // 146-152): one logged Newton attempt from each probed f32 state with its h
+  std::ifstream probes_json(dir + "/probes.json");
+  if (!probes_json) return true;
+  std::vector<double> steps, hs, positions;
+  try {
+    steps = drape::read_named_array(dir + "/probes.json", dir + "/probes.bin", "probe_steps");
+    hs = drape::read_named_array(dir + "/probes.json", dir + "/probes.bin", "probe_h");
+    positions = drape::read_named_array(dir + "/probes.json", dir + "/probes.bin", "probe_positions");
+  } catch (const std::exception& e) {
+    *err = e.what();
+    return false;
+  }
+  if (hs.size() != steps.size() || positions.size() != 3 * V * steps.size()) {
+    *err = "probes.bin: probe_steps, probe_h and probe_positions disagree";
+    return false;
+  }
+  if (drape_probe_begin(ctx) != DRAPE_OK) return fail("probes");
+  for (size_t k = 0; k < steps.size(); ++k)
+    if (drape_probe_step(ctx, positions.data() + 3 * V * k, hs[k], int32_t(steps[k])) != DRAPE_OK)
+      return fail("probe");
+  int64_t ni = 0, nd = 0, nt = 0;
+  drape_probe_logs(ctx, nullptr, 0, &ni, nullptr, 0, &nd, nullptr, 0, &nt);
+  std::vector<float> iterates(static_cast<size_t>(ni)), directions(static_cast<size_t>(nd));
+  std::vector<double> trials(static_cast<size_t>(nt));
+  drape_probe_logs(ctx, iterates.data(), ni, &ni, directions.data(), nd, &nd, trials.data(), nt, &nt);
+  int32_t n_rec = 0;
+  ok = write_run_tables(ctx, out, "probe-", &n_rec) &&
+       write_bytes(out + "/gpu-probe-iterates.bin", iterates.data(), iterates.size() * sizeof(float)) &&
+       write_bytes(out + "/gpu-probe-directions.bin", directions.data(), directions.size() * sizeof(float)) &&
+       write_bytes(out + "/gpu-probe-search.bin", trials.data(), trials.size() * sizeof(double));
+  if (!ok) *err = "cannot write the probe files in " + out;
   return ok;
 }
 
@@ -307,31 +374,12 @@ int main(int argc, char** argv) {
                            double(r.pcg_iterations), r.min_distance};
     ptc.insert(ptc.end(), row, row + 7);
   }
-  // per-Newton and per-attempt tables (outputs.ts:8-10, run-e7.ts:94-98): f64 rows, NaN where the reference's
-  // field has no counterpart in this solver or no value on the iterate (the last iterate takes no solve)
-  const double nan = std::nan("");
-  int32_t n_rec = 0, n_att = 0;
-  drape_newton_records(ctx, nullptr, 0, &n_rec);
+  // per-attempt table (run-e7.ts:98); the per-Newton tables are written with the others below
+  int32_t n_att = 0;
   drape_attempt_records(ctx, nullptr, 0, &n_att);
-  std::vector<drape_newton_record> nrec(size_t(n_rec > 0 ? n_rec : 1));
   std::vector<drape_attempt_record> arec(size_t(n_att > 0 ? n_att : 1));
-  drape_newton_records(ctx, nrec.data(), n_rec, &n_rec);
   drape_attempt_records(ctx, arec.data(), n_att, &n_att);
-  std::vector<double> iterations, robust, attempts;
-  for (int i = 0; i < n_rec; ++i) {
-    const drape_newton_record& r = nrec[size_t(i)];
-    const bool solved = r.pcg_iterations >= 0;
-    const double it_row[9] = {double(r.step), double(r.iteration), r.relative_residual,
-                              solved ? double(r.pcg_iterations) : nan, solved ? double(r.pcg_status) : nan,
-                              solved ? r.linear_residual : nan, r.step_length,
-                              r.halvings >= 0 ? double(r.halvings) : nan, double(r.status)};
-    iterations.insert(iterations.end(), it_row, it_row + 9);
-    // eta, mu, updateInf, stepInf, retries, resolution, alphaMax, limitingVertex, minDistance, deltaSum, deltaAbs,
-    // noiseOnly, slope, slopeExact, normSquared, normSquaredExact
-    const double rb_row[16] = {r.eta, r.mu, nan, nan, solved ? double(r.retries) : nan, nan, r.alpha_max, nan, nan,
-                               r.delta_sum, nan, nan, r.slope, nan, r.norm_squared, nan};
-    robust.insert(robust.end(), rb_row, rb_row + 16);
-  }
+  std::vector<double> attempts;
   for (int i = 0; i < n_att; ++i) {
     const drape_attempt_record& r = arec[size_t(i)];
     const double row[6] = {double(r.step), double(r.attempt), r.h, double(r.reason), double(r.record_start),
@@ -352,9 +400,9 @@ int main(int argc, char** argv) {
   bool ok = write_bytes(out + "/gpu-ptc.bin", ptc.data(), ptc.size() * sizeof(double)) &&
             write_bytes(out + "/gpu-equilibrium.bin", eq.data(), eq.size() * sizeof(float)) &&
             write_bytes(out + "/gpu-states.bin", states.data(), states.size() * sizeof(float)) &&
-            write_bytes(out + "/gpu-iterations.bin", iterations.data(), iterations.size() * sizeof(double)) &&
-            write_bytes(out + "/gpu-robust.bin", robust.data(), robust.size() * sizeof(double)) &&
             write_bytes(out + "/gpu-attempts.bin", attempts.data(), attempts.size() * sizeof(double));
+  int32_t n_rec = 0;
+  ok = ok && write_run_tables(ctx, out, "", &n_rec);
   {
     std::ofstream f(out + "/gpu-equilibrium.json");
     char buf[256];

@@ -434,9 +434,11 @@ AttemptResult Context::attempt(double h, double scale) {
     rec.relative_residual = rel;
     rec.norm_squared = norm * norm;
     rec.linear_residual = rec.step_length = rec.eta = rec.alpha_max = rec.delta_sum = rec.slope = kNaN;
+    rec.resolution = kNaN;
     rec.mu = mu;
     auto finish = [&](int status) {
       rec.status = status;
+      if (probe_log_) log_probe_iterate(rec);
       records_.push_back(rec);
     };
     if (!std::isfinite(rel)) {
@@ -504,6 +506,11 @@ AttemptResult Context::attempt(double h, double scale) {
       for (int k = 0; k <= opt_.max_halvings; ++k) {
         double a = amax * std::ldexp(1.0, -k);
         double delta = energy_change(x_.ptr, d_.ptr, a, inv_h2, 0);
+        if (probe_log_) {  // TRIAL_FIELDS: step, iteration, halving, alpha, sum, abs, slope, accepted
+          const double row[8] = {double(record_step_), double(it), double(k), a, delta, kNaN, slope,
+                                 delta <= opt_.armijo * a * slope ? 1.0 : 0.0};
+          probe_trials_.insert(probe_trials_.end(), row, row + 8);
+        }
         if (delta <= opt_.armijo * a * slope) {
           halvings = k;
           alpha = a;
@@ -526,6 +533,56 @@ AttemptResult Context::attempt(double h, double scale) {
     res.halvings += halvings;
     mu = halvings == 0 ? relax_mu(mu) : mu;
   }
+}
+
+// The iterate x_k in f32, its f32 spacing (2^(exponent of max |x_i| over the rows' vertices - 23), e4_rules.rs:35-39)
+// and, after a direction solve, the pair (x_k, d_k) in f32.
+void Context::log_probe_iterate(drape_newton_record& rec) {
+  const size_t nv = 3 * size_t(host_.V);
+  std::vector<double> xs(nv), ds;
+  x_.download(xs.data(), nv, stream_);
+  if (rec.pcg_iterations >= 0) {
+    ds.resize(nv);
+    d_.download(ds.data(), nv, stream_);
+  }
+  sync();
+  double largest = 0.0;
+  for (int r = 0; r < host_.R; ++r)
+    for (int c = 0; c < 3; ++c) largest = std::max(largest, std::fabs(xs[3 * size_t(host_.row_vertex[r]) + c]));
+  const float m = float(largest);
+  uint32_t bits;
+  std::memcpy(&bits, &m, sizeof bits);
+  rec.resolution = std::ldexp(1.0, int((bits >> 23) & 0xffu) - 127 - 23);
+  probe_iterates_.insert(probe_iterates_.end(), xs.begin(), xs.end());
+  if (rec.pcg_iterations >= 0) {
+    probe_directions_.insert(probe_directions_.end(), xs.begin(), xs.end());
+    probe_directions_.insert(probe_directions_.end(), ds.begin(), ds.end());
+  }
+}
+
+void Context::probe_begin() {
+  records_.clear();
+  attempts_.clear();
+  probe_iterates_.clear();
+  probe_directions_.clear();
+  probe_trials_.clear();
+}
+
+// runPtcProbes (drape-e7.ts:190-200): x_n = x, x_hat = x_n + h^2 g, scale = |grad E_s(x_n)|, one attempt.
+void Context::probe_step(const double* x, double h, int step) {
+  set_positions(x);
+  check(cudaMemcpyAsync(xn_.ptr, x_.ptr, 3 * size_t(host_.V) * sizeof(double), cudaMemcpyDeviceToDevice, stream_),
+        "save");
+  const double scale = static_residual();
+  record_step_ = step;
+  probe_log_ = true;
+  try {
+    attempt(h, scale);
+  } catch (...) {
+    probe_log_ = false;
+    throw;
+  }
+  probe_log_ = false;
 }
 
 int Context::solve_equilibrium(const double* start, double h0, drape_run_log* log) {

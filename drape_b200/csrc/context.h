@@ -106,6 +106,13 @@ class Context {
   // With `on`, every accepted PTC state of a solve is kept in f32 (3V floats per step, in step order).
   void set_keep_states(bool on) { keep_states_ = on; }
   const std::vector<float>& step_states() const { return states_; }
+  // PTC probes: one logged Newton attempt of step `step` from x with step size h (records, iterates, directions,
+  // line-search trials); probe_begin clears the records and the logs.
+  void probe_begin();
+  void probe_step(const double* x, double h, int step);
+  const std::vector<float>& probe_iterates() const { return probe_iterates_; }
+  const std::vector<float>& probe_directions() const { return probe_directions_; }
+  const std::vector<double>& probe_trials() const { return probe_trials_; }
 
   // Stand-alone timed SpMV of the assembled matrix (roofline measurement): average ms per launch.
   float time_spmv(int launches, int lanes_per_row, int threads);
@@ -252,6 +259,10 @@ class Context {
   std::vector<drape_attempt_record> attempts_;
   bool keep_states_ = false;
   std::vector<float> states_;
+  bool probe_log_ = false;
+  std::vector<float> probe_iterates_, probe_directions_;
+  std::vector<double> probe_trials_;
+  void log_probe_iterate(drape_newton_record& rec);
   int record_step_ = 0;  // PTC step the Newton records of the running attempt belong to
   double phase_ms_[6] = {};
   int partial_grid_ = 0;

@@ -377,12 +377,17 @@ HostProblem read_problem_files(const std::string& dir) {
   return p;
 }
 
-std::vector<double> read_problem_array(const std::string& dir, const std::string& name) {
-  std::string text = read_all(dir + "/problem.json");
+std::vector<double> read_named_array(const std::string& json_path, const std::string& bin_path,
+                                     const std::string& name) {
+  std::string text = read_all(json_path);
   const size_t at = text.find("\"arrays\"");
   if (at == std::string::npos) return {};
-  Manifest m{text.substr(at), read_all(dir + "/problem.bin")};
+  Manifest m{text.substr(at), read_all(bin_path)};
   return m.get<double>(name, false);
+}
+
+std::vector<double> read_problem_array(const std::string& dir, const std::string& name) {
+  return read_named_array(dir + "/problem.json", dir + "/problem.bin", name);
 }
 
 void write_problem_files(const HostProblem& p, const std::string& dir) {

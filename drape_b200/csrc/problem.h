@@ -52,6 +52,9 @@ HostProblem read_problem_files(const std::string& dir);
 // One named array of a problem.bin as f64 (empty when the manifest has no such array): the check states
 // kernel_state and contact_state and the per-row row_mass of the reference's files (e3_generate.rs:93-98).
 std::vector<double> read_problem_array(const std::string& dir, const std::string& name);
+// The same from any manifest / binary pair in that layout (the oracle's probes.json / probes.bin, io.rs:5-55).
+std::vector<double> read_named_array(const std::string& json_path, const std::string& bin_path,
+                                     const std::string& name);
 // The whole file as text (throws if it cannot be read).
 std::string read_text_file(const std::string& path);
 // The number at the first "key": after the first "anchor" of a JSON text (NaN if absent): the flat key scan the

@@ -120,6 +120,7 @@ typedef struct {
   double relative_residual, linear_residual, step_length; /* |g| / |g(x_n)|, PCG recursive residual, alpha */
   double eta, mu, alpha_max, delta_sum, slope, norm_squared; /* forcing, regularisation, CCD bound, accepted
                                                                  energy change, g.d, |g|^2 */
+  double resolution; /* probe runs: f32 spacing of the iterate's largest |x| (e4_rules.rs:35-39); else NaN */
 } drape_newton_record;
 
 /* One attempt at a step size (AttemptLog, drape-e7.ts:26-32; gpu-attempts.bin rows): its Newton records are
@@ -198,6 +199,17 @@ drape_status drape_attempt_records(const drape_ctx* ctx, drape_attempt_record* o
  * solve's states (3V per accepted step, in step order; the start state is not among them) and returns their total
  * count in *count. */
 drape_status drape_keep_states(drape_ctx* ctx, int32_t keep);
+/* PTC probes (runPtcProbes, drape-e7.ts:190-200; run-e7.ts:146-152): drape_probe_begin clears the Newton records and
+ * the probe logs; each drape_probe_step runs one Newton attempt of PTC step `step` from `xyz` (3V f64) with step size
+ * h, recording its Newton iterates (drape_newton_records) and logging, per iterate, its positions (f32 3V), per
+ * update the pair (positions, direction) (f32 2 x 3V) and per line-search trial the row (step, iteration, halving,
+ * alpha, energy-change sum, NaN, g.d, accepted 0/1) (f64 8; TRIAL_FIELDS of outputs.ts:11). drape_probe_logs copies
+ * up to the given capacities (floats / doubles, each buffer may be NULL) and returns the totals. */
+drape_status drape_probe_begin(drape_ctx* ctx);
+drape_status drape_probe_step(drape_ctx* ctx, const double* xyz, double h, int32_t step);
+drape_status drape_probe_logs(const drape_ctx* ctx, float* iterates, int64_t iterates_capacity, int64_t* iterates_count,
+                              float* directions, int64_t directions_capacity, int64_t* directions_count,
+                              double* trials, int64_t trials_capacity, int64_t* trials_count);
 drape_status drape_step_states(const drape_ctx* ctx, float* out, int64_t capacity, int64_t* count);
 
 /* Kernel-level entry points on host buffers (the parity checks of run-e7.ts:140-145 --checks):

@@ -1,6 +1,8 @@
 """The reference comparer's replays of a GPU run's record tables, restated in Python (test checker only): the
 Eisenstat-Walker forcing replay (engine/oracle/src/e4_compare.rs:87-95 with e4_rules.rs:8-30), the PTC step-size
-controller replay (e7_compare.rs:111-121) and the rejection replay (e7_compare.rs:128-136). The tables are the
+controller replay (e7_compare.rs:111-121), the rejection replay (e7_compare.rs:128-136) and the probe replays:
+alpha_max (e5_compare.rs:70-101), resolution (e5_compare.rs:103-110) and line-search acceptance
+(e6_compare.rs:40-62). The tables are the
 gpu-<mode>/ files the `drape` command writes (gpu-iterations.bin, gpu-robust.bin by the names in gpu-result.json's
 "robust_fields", gpu-attempts.bin, gpu-ptc.bin)."""
 import json
@@ -78,3 +80,38 @@ def rejection_replay(it, at):
         if not ok:
             return False
     return True
+
+
+def f32_spacing(max_abs):
+    """e4_rules.rs:35-39: 2^(exponent of max_abs as f32 - 23)."""
+    bits = int(np.array([max_abs], np.float32).view(np.uint32)[0])
+    return 2.0 ** (((bits >> 23) & 0xFF) - 127 - 23)
+
+
+def resolution_replay(it, rb, fields, iterates, free_rows):
+    """Every probe update's recorded resolution equals f32_spacing(max |x_i|) over the free vertices' coordinates."""
+    col = fields.index("resolution")
+    for k, x in enumerate(iterates):
+        if not np.isfinite(it[k, 3]):
+            continue
+        largest = np.abs(x.reshape(-1, 3)[free_rows]).max()
+        if f32_spacing(float(largest)) != rb[k, col]:
+            return False
+    return True
+
+
+def alpha_errors(it, rb, fields, directions, max_step):
+    """Relative errors of the recorded alpha_max against the f64 CCD rule `max_step(x, d)` at each update's recorded
+    f32 (x, d) pair (the reference's tolerance is max(1e-5, 8 eps32 cond) with cond the limiting sphere's |q|/d0)."""
+    col = fields.index("alphaMax")
+    updates = np.flatnonzero(np.isfinite(it[:, 3]))
+    assert len(updates) == len(directions), (len(updates), len(directions))
+    return [abs(max_step(pair[0].astype(np.float64), pair[1].astype(np.float64)) - rb[k, col]) / rb[k, col]
+            for k, pair in zip(updates, directions)]
+
+
+def acceptance_replay(trials, armijo):
+    """Each trial's accept decision replayed from its recorded numbers: plain Armijo sum <= f32(c alpha g.d) (the
+    noise term needs the absolute change sum, which this solver does not record)."""
+    plain = (armijo * trials[:, 3] * trials[:, 6]).astype(np.float32).astype(np.float64)
+    return bool(np.all((trials[:, 4] <= plain) == (trials[:, 7] == 1.0)))
