@@ -164,8 +164,7 @@ constexpr int kGalerkinEntries = 9 * kMgStencil;  // a row couples within 2 vert
 struct GalerkinEntry {
   double m[9];
   double w;
-  int j;
-  int pad;
+  int jx, jy;  // the fine column's grid coordinates (jx < 0: outside the grid)
 };
 
 template <bool kSrcBsr>
@@ -213,7 +212,9 @@ __global__ void __launch_bounds__(32 * kGalerkinWarps) galerkin_kernel(MgFine fi
       E.w = wi;
       if (kSrcBsr) {
         const int k = sf + t;
-        E.j = fine.col_idx[k];
+        const int j = fine.col_idx[k];
+        E.jx = j % nf;
+        E.jy = j / nf;
         float m[9];
         load_block(fine.A, k, m);
 #pragma unroll
@@ -221,7 +222,8 @@ __global__ void __launch_bounds__(32 * kGalerkinWarps) galerkin_kernel(MgFine fi
       } else {
         int j;
         const bool in = stencil_neighbour(nf, si % nf, si / nf, t, &j);
-        E.j = in ? j : -1;
+        E.jx = in ? j % nf : -1;
+        E.jy = in ? j / nf : -1;
 #pragma unroll
         for (int e = 0; e < 9; ++e) E.m[e] = in ? src.A64[(t * 9 + e) * src.rows + si] : 0.0;
       }
@@ -237,8 +239,8 @@ __global__ void __launch_bounds__(32 * kGalerkinWarps) galerkin_kernel(MgFine fi
       const int JX = J % nc, JY = J / nc;
       for (int t = 0; t < total; ++t) {
         const GalerkinEntry& E = L[t];
-        if (E.j < 0) continue;
-        const double wj = w1d(E.j % nf, JX) * w1d(E.j / nf, JY);
+        if (E.jx < 0) continue;
+        const double wj = w1d(E.jx, JX) * w1d(E.jy, JY);
         if (wj == 0.0) continue;
         const double w = E.w * wj;
 #pragma unroll
@@ -344,12 +346,16 @@ __global__ void __launch_bounds__(1024) coarse_inverse_kernel(MgLevel lv, float*
     const int p = s_piv;
     const double d = M[p * w + k];
     const double rd = d != 0.0 ? 1.0 / d : 0.0;
-    for (int c = threadIdx.x; c < w; c += blockDim.x) s_row[c] = M[p * w + c] * rd;
+    // Columns left of k are already eliminated: zero in the pivot row, so no row changes there. Only columns
+    // k .. 2m - 1 are touched (rows by warp, columns by lane).
+    for (int c = k + threadIdx.x; c < w; c += blockDim.x) s_row[c] = M[p * w + c] * rd;
     for (int i = threadIdx.x; i < m; i += blockDim.x) s_fac[i] = i == p ? 0.0 : M[i * w + k];
     __syncthreads();
-    for (int t = threadIdx.x; t < m * w; t += blockDim.x) {
-      const int i = t / w, c = t % w;
-      M[t] = i == p ? s_row[c] : M[t] - s_fac[i] * s_row[c];
+    const int warps = blockDim.x >> 5;
+    for (int i = warp; i < m; i += warps) {
+      double* row = M + i * w;
+      const double f = s_fac[i];
+      for (int c = k + lane; c < w; c += 32) row[c] = i == p ? s_row[c] : row[c] - f * s_row[c];
     }
     __syncthreads();
   }
