@@ -342,17 +342,18 @@ int main(int argc, char** argv) {
   drape_keep_states(ctx, keep_states ? 1 : 0);
   const std::string out = a.dir + "/gpu-" + a.mode;
   ::mkdir(out.c_str(), 0755);
+  // the solve's start, taken before the checks: the probe runs move the context's state
+  std::vector<double> x0(3 * V);
+  drape_get_state(ctx, x0.data(), nullptr);
+  if (!start.empty()) x0 = start;
   if (a.checks && !write_checks(ctx, a.dir, text, out, sizes, &err)) {
     std::fprintf(stderr, "drape: %s\n", err.c_str());
     drape_destroy(ctx);
     drape_network_destroy(net);
     return 1;
   }
-  std::vector<double> x0(3 * V);
-  drape_get_state(ctx, x0.data(), nullptr);
-  if (!start.empty()) x0 = start;
   drape_run_log log{};
-  const drape_status st = drape_solve_equilibrium(ctx, start.empty() ? nullptr : start.data(), h0, &log);
+  const drape_status st = drape_solve_equilibrium(ctx, x0.data(), h0, &log);
   if (st != DRAPE_OK && st != DRAPE_E_DIVERGED && st != DRAPE_E_TIMEOUT) {
     std::fprintf(stderr, "drape: %s\n", drape_last_error(ctx));
     drape_destroy(ctx);

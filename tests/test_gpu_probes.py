@@ -72,3 +72,12 @@ def test_probe_files_pass_the_probe_replays():
         errors = e7_replays.alpha_errors(it, rb, fields, pairs, oracle.max_step)
         assert max(errors) <= 1e-4, max(errors)
         assert e7_replays.acceptance_replay(trials, api.default_options().armijo)
+        # the checks and probes leave the cold solve alone: the same equilibrium as a run without --checks
+        with tempfile.TemporaryDirectory() as t2:
+            for name in ("problem.json", "problem.bin"):
+                open(os.path.join(t2, name), "wb").write(open(os.path.join(t, name), "rb").read())
+            p2 = subprocess.run([CLI, "--case", t2, "--mode", "cold"], capture_output=True, text=True, timeout=600)
+            assert p2.returncode == 0, p2.stderr
+            eq1 = np.fromfile(os.path.join(out, "gpu-equilibrium.bin"), np.float32)
+            eq2 = np.fromfile(os.path.join(t2, "gpu-cold", "gpu-equilibrium.bin"), np.float32)
+            assert np.array_equal(eq1, eq2)
