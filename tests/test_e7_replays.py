@@ -61,3 +61,44 @@ def test_forcing_rule_bounds():
     assert rp.next_forcing(1e-2, 1e-6) == 1e-7  # floored
     assert abs(rp.next_forcing(1e-2, 0.1) - 0.9 * 0.01) < 1e-18  # 0.9 ratio^2, no safeguard below 0.1
     assert rp.next_forcing(0.4, 1e-3) == 1e-2  # the safeguard 0.9 x 0.16 > 0.1 keeps eta up, then the cap
+
+
+def test_probe_replays_on_made_up_records():
+    """The probe replays (alpha, resolution, acceptance) pass on consistent made-up logs and catch planted errors."""
+    V = 2
+    x0 = np.array([0.1, 0.2, -0.3, 1.5, 0.0, 0.25], np.float32)
+    x1 = np.array([0.1, 0.2, -0.3, 0.7, 0.0, 0.25], np.float32)
+    d = np.full(6, 0.01, np.float32)
+    it = np.full((3, 9), np.nan)
+    it[:, 0] = 4
+    it[:, 1] = [0, 1, 2]
+    it[:2, 3] = 7  # two updates, the last iterate takes no solve
+    fields = FIELDS
+    rb = np.full((3, 16), np.nan)
+    rb[0, 5] = rp.f32_spacing(1.5)
+    rb[1, 5] = rp.f32_spacing(0.7)
+    rb[:2, 6] = [0.5, 0.25]
+    iterates = np.stack([x0, x1, x1])
+    pairs = np.stack([np.stack([x0, d]), np.stack([x1, d])])
+    free = np.arange(V)
+    assert rp.f32_spacing(1.5) == 2.0 ** -23 and rp.f32_spacing(0.7) == 2.0 ** -24
+    assert rp.resolution_replay(it, rb, fields, iterates, free)
+    bad = rb.copy()
+    bad[1, 5] *= 2
+    assert not rp.resolution_replay(it, bad, fields, iterates, free)
+    # alpha: the rule replayed exactly gives 0 error; a recorded alpha 1 % off is caught
+    rule = {0: 0.5, 1: 0.25}
+    calls = iter(range(2))
+    errors = rp.alpha_errors(it, rb, fields, pairs, lambda x, dd: rule[next(calls)])
+    assert max(errors) == 0.0
+    calls = iter(range(2))
+    off = rb.copy()
+    off[1, 6] *= 1.01
+    assert max(rp.alpha_errors(it, off, fields, pairs, lambda x, dd: rule[next(calls)])) > 1e-3
+    # acceptance: sum <= f32(c alpha slope) decides; a flipped decision is caught
+    trials = np.array([[4, 0, 0, 0.5, -1e-3, np.nan, -1.0, 1.0],
+                       [4, 1, 0, 0.25, 1e-3, np.nan, -1.0, 0.0]])
+    assert rp.acceptance_replay(trials, 1e-4)
+    flipped = trials.copy()
+    flipped[1, 7] = 1.0
+    assert not rp.acceptance_replay(flipped, 1e-4)

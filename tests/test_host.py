@@ -139,3 +139,36 @@ def test_record_structs_match_the_header(tmp_path):
     import ctypes
     assert sizes == [ctypes.sizeof(api.NewtonRecord), ctypes.sizeof(api.AttemptRecord),
                      ctypes.sizeof(api.StepRecord), ctypes.sizeof(api.Options), ctypes.sizeof(api.RunLog)]
+
+
+def test_named_array_reader_reads_probe_files(tmp_path):
+    """read_named_array (problem.cpp, compiled here with the host compiler) reads a probes.json / probes.bin pair in
+    the problem-file layout (u32 and f32 arrays at 8-byte-aligned offsets) and returns nothing for an absent name."""
+    import json
+
+    steps = np.array([3, 17], np.uint32)
+    h = np.array([1e-3, 0.25], np.float32)
+    pos = np.arange(12, dtype=np.float32) * 0.5
+    raw, arrays = bytearray(), []
+    for name, dtype, values in (("probe_steps", "u32", steps), ("probe_h", "f32", h), ("probe_positions", "f32", pos)):
+        while len(raw) % 8:
+            raw.append(0)
+        arrays.append({"name": name, "dtype": dtype, "length": int(values.size), "offset": len(raw)})
+        raw += values.tobytes()
+    (tmp_path / "probes.bin").write_bytes(bytes(raw))
+    (tmp_path / "probes.json").write_text(json.dumps({"arrays": arrays}, separators=(",", ":")))
+    src = tmp_path / "read.cpp"
+    src.write_text('#include <cstdio>\n#include "problem.h"\nint main(int, char** argv) {\n'
+                   '  for (const char* name : {"probe_steps", "probe_h", "probe_positions", "missing"}) {\n'
+                   '    auto v = drape::read_named_array(std::string(argv[1]) + "/probes.json", std::string(argv[1]) +'
+                   ' "/probes.bin", name);\n    std::printf("%s %zu", name, v.size());\n'
+                   '    for (double x : v) std::printf(" %.17g", x);\n    std::printf("\\n");\n  }\n}\n')
+    exe = tmp_path / "read"
+    subprocess.run(["g++", "-std=c++17", "-I", os.path.join(ROOT, "drape_b200", "csrc"), str(src),
+                    os.path.join(ROOT, "drape_b200", "csrc", "problem.cpp"), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe), str(tmp_path)], capture_output=True, text=True, check=True).stdout.splitlines()
+    got = {line.split()[0]: [float(v) for v in line.split()[2:]] for line in out}
+    assert got["probe_steps"] == [3.0, 17.0]
+    assert np.allclose(got["probe_h"], h.astype(np.float64), rtol=0, atol=0)
+    assert np.array_equal(got["probe_positions"], pos.astype(np.float64))
+    assert got["missing"] == []
