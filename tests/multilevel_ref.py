@@ -106,6 +106,33 @@ def block_apply(S, r, transpose=False):
     return (np.einsum("kji,kj->ki" if transpose else "kij,kj->ki", S, r3)).reshape(-1)
 
 
+def chebyshev_interval(omega):
+    """[lo, hi] of D^{-1} A that the spectral omega damps as degree-1 Chebyshev: omega = 2 / (lo + hi) with
+    hi = 1.1 lambda and lo = hi / 30."""
+    hi = 2.0 / (omega * (1.0 + 1.0 / 30.0))
+    return hi / 30.0, hi
+
+
+def chebyshev_apply(A, Dinv, r, lo, hi, degree):
+    """z = p(D^{-1} A) D^{-1} r: `degree` steps of block-Jacobi preconditioned Chebyshev iteration for A z = r from
+    z = 0 on the interval [lo, hi] (the three-term recurrence of Saad, Iterative Methods for Sparse Linear Systems,
+    2nd ed., Algorithm 12.1). Degree 1 is omega D^{-1} r with omega = 2 / (lo + hi); each further degree costs one
+    SpMV with A. A candidate fine smoother, checked here on the host ahead of a device kernel."""
+    theta, delta = 0.5 * (hi + lo), 0.5 * (hi - lo)
+    sigma = theta / delta
+    rho = 1.0 / sigma
+    d = block_apply(Dinv, r) / theta
+    z = d.copy()
+    res = r.copy()
+    for _ in range(degree - 1):
+        res = res - A @ d
+        rho_next = 1.0 / (2.0 * sigma - rho)
+        d = rho_next * rho * d + (2.0 * rho_next / delta) * block_apply(Dinv, res)
+        rho = rho_next
+        z = z + d
+    return z
+
+
 class Hierarchy:
     """omega > 0: fixed damping on every level; omega = None: spectral_omega per level (the device default)."""
 
