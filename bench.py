@@ -14,7 +14,9 @@ value: seconds per converged solve with the problem resident in HBM (CUDA-event-
 e2e:   the same through the C ABI from host arrays: drape_create (host->device copies) + solve + drape_get_state
        (device->host), wall clock on the host.
 --impl reference: the reference's CPU implementation of this path (the f64 oracle restatement; the Rust crate
-       cannot be built here), single-threaded like the reference, on a bounded sample of the same solve.
+       cannot be built here), single-threaded like the reference, on a bounded sample of the same solve: its
+       seconds per Newton iteration times the Newton iterations of the whole solve (FULL_SOLVE_NEWTON);
+       --full-solve times the oracle's whole solve instead.
 Multi-GPU: replicas only (one independent drape per rank, no collective on the data path).
 """
 import argparse
@@ -261,25 +263,50 @@ def run_gpu(args):
         print(json.dumps(out), flush=True)
 
 
+# Newton iterations of the whole cold solve of a bench workload, keyed by (n, plane, seed), and where the count
+# comes from: the f64 oracle's own whole solve (`python bench.py --impl reference --full-solve`, no CPU budget) where
+# it has been run, else the block-Jacobi GPU solve of the same workload (the reference's method, f32 PCG; 424 PTC
+# steps at n129).
+FULL_SOLVE_NEWTON = {(129, 1, 0): (3162, "the block-Jacobi GPU solve of this workload")}
+
+
+def full_newton_count(args, gpu_log=None):
+    """(Newton iterations of the whole solve, where the count comes from), or (None, ...) when neither the table
+    nor this run's GPU solve gives one."""
+    known = FULL_SOLVE_NEWTON.get((args.n, int(args.plane), args.seed))
+    if known is not None:
+        return known
+    if gpu_log:
+        return int(gpu_log["newton_iterations"]), "this run's GPU solve"
+    return None, "none"
+
+
 def cpu_baseline(args, gpu_log=None, budget_s=None):
     """The f64 oracle (port of the reference crate's method: exact tangent, LM, f64 block-Jacobi PCG rtol 1e-6
-    <= 2000 iterations, inner-count PTC from dt0 = 1e-3 s) on a bounded sample of the same solve: it runs PTC
-    steps until `budget_s` of CPU time has passed, and the full-solve time is its seconds per Newton iteration
-    times the Newton iterations of the full solve (the GPU's, when given, else the sample's rate over the
-    oracle's own PTC step cap is not extrapolated)."""
+    <= 2000 iterations, inner-count PTC from dt0 = 1e-3 s) timed on the host. It runs the cold solve until `budget_s`
+    of CPU time has passed (0: to the end) and reports the whole solve's time as its seconds per Newton iteration
+    times the Newton iterations of the whole solve: the counted whole solve of this workload, else this run's
+    GPU solve. With neither, the solve runs to the end and its own time is the value."""
     from tests import oracle_py
 
     budget = budget_s if budget_s is not None else args.cpu_budget
+    full_newton, source = full_newton_count(args, gpu_log)
+    if full_newton is None:
+        budget = 0.0
     s = oracle_py.Scene("sheet", args.n, seed=args.seed, plane=bool(args.plane))
     # The cold solve, stopped at the first PTC step that ends past the CPU budget.
     _, st = s.ptc(h0=1e-3, doubling=False, absolute=1e-6, pcg=True, rtol=1e-6, maxit=2000, budget_s=budget)
     steps, elapsed, newton = int(st["steps"]), st["seconds"], int(st["newton"])
+    if budget == 0.0:
+        return {"value": elapsed, "unit": "s", "cores": 1, "kind": "port", "newton_iterations": newton,
+                "converged": bool(st["converged"]),
+                "sample": f"the whole n{args.n} solve ({steps} PTC steps, {newton} Newton iterations) on 1 host core",
+                "host_cpu": _cpu_model()}
     per_newton = elapsed / max(1, newton)
-    full_newton = gpu_log["newton_iterations"] if gpu_log else newton
     return {"value": per_newton * full_newton, "unit": "s", "cores": 1, "kind": "port",
             "sample": f"{steps} PTC steps ({newton} Newton iterations) of the n{args.n} solve in {elapsed:.1f} s on 1 "
                       f"host core; value = {per_newton:.3f} s per Newton iteration x {full_newton} Newton iterations "
-                      f"of the full solve",
+                      f"of the whole solve ({source})",
             "host_cpu": _cpu_model()}
 
 
@@ -301,8 +328,9 @@ def run_reference(args):
 
     oracle_py.build()
     results = []
-    for i in range(args.warmup + args.steps):
-        r = cpu_baseline(args, None, budget_s=args.cpu_budget)
+    budget = 0.0 if args.full_solve else args.cpu_budget
+    for i in range(args.warmup if args.full_solve else 0, args.warmup + args.steps):  # a full solve needs no warm-up
+        r = cpu_baseline(args, None, budget_s=budget)
         if i >= args.warmup:
             results.append(r)
     v = sum(r["value"] for r in results) / len(results)
@@ -313,6 +341,9 @@ def run_reference(args):
                                   f"(exact tangent, LM, block-Jacobi PCG rtol 1e-6 <= 2000)", "columns": args.n},
            "cpu_baseline": {"value": v, "unit": "s", "cores": 1, "kind": "port", "sample": results[-1]["sample"]},
            "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if "newton_iterations" in results[-1]:
+        out["newton_iterations"] = results[-1]["newton_iterations"]
+        out["converged"] = results[-1]["converged"]
     print(json.dumps(out), flush=True)
 
 
@@ -328,6 +359,8 @@ def main():
     ap.add_argument("--pcg-max", type=int, default=2000)
     ap.add_argument("--max-steps", type=int, default=1000)
     ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--full-solve", action="store_true",
+                    help="--impl reference: time the oracle's whole solve instead of a bounded sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--preconditioner", default="learned", choices=["jacobi", "multilevel", "learned"])
     ap.add_argument("--compare", default="jacobi", choices=["none", "jacobi", "all"],
