@@ -106,6 +106,18 @@ def block_apply(S, r, transpose=False):
     return (np.einsum("kji,kj->ki" if transpose else "kij,kj->ki", S, r3)).reshape(-1)
 
 
+def smoothed_prolongation(A, P, level, c=4.0 / 3.0):
+    """(I - omega_P D^{-1} A) P with omega_P = c / lambda, lambda the spectral estimate of lambda_max(D^{-1} A) that
+    spectral_omega uses (the prolongation smoothing of smoothed aggregation: Vanek, Mandel and Brezina, Computing
+    56 (1996), with its omega_P = 4 / (3 lambda)). A candidate coarse space, checked on the host ahead of a device
+    form."""
+    lam = 2.0 / (spectral_omega(A, level) * 1.1 * (1.0 + 1.0 / 30.0))
+    Dinv = jacobi_smoother(A, 1.0)
+    R = A.shape[0] // 3
+    Dm = sp.bsr_matrix((Dinv, np.arange(R), np.arange(R + 1)), shape=A.shape).tocsr()
+    return (P - (c / lam) * (Dm @ (A @ P))).tocsr()
+
+
 def chebyshev_interval(omega):
     """[lo, hi] of D^{-1} A that the spectral omega damps as degree-1 Chebyshev: omega = 2 / (lo + hi) with
     hi = 1.1 lambda and lo = hi / 30."""
@@ -136,7 +148,9 @@ def chebyshev_apply(A, Dinv, r, lo, hi, degree):
 class Hierarchy:
     """omega > 0: fixed damping on every level; omega = None: spectral_omega per level (the device default)."""
 
-    def __init__(self, A, n, omega=None, fine_smoother=None):
+    def __init__(self, A, n, omega=None, fine_smoother=None, smooth_prolongation=()):
+        """smooth_prolongation: levels whose prolongation is smoothed once (smoothed_prolongation; a candidate
+        coarse space, not the device's), () for the device's bilinear one everywhere."""
         self.cols = level_columns(n)
         if len(self.cols) < 2:
             raise ValueError("grid cannot be coarsened")
@@ -144,6 +158,8 @@ class Hierarchy:
         self.P = []
         for l in range(len(self.cols) - 1):
             P = prolongation(self.cols[l])
+            if l in smooth_prolongation:
+                P = smoothed_prolongation(self.A[-1], P, l)
             self.P.append(P)
             self.A.append((P.T @ self.A[-1] @ P).tocsr())
         self.omega = [omega if omega else spectral_omega(Al, l) for l, Al in enumerate(self.A[:-1])]
