@@ -2,8 +2,10 @@
 
 Workload: the 1.0 m sheet of n x n vertices (default n = 129: 16641 vertices, 32768 triangles, 48896 hinges,
 180993 BSR blocks) over a sphere of radius 0.25 m and a ground plane at y = -0.25 m, isotropic StVK E = 5e5 Pa,
-nu = 0.3, t = 5e-4 m, k_b = 1e-5 N m, IPC d_hat = 2e-3 m, kappa = 1e3; PTC from dt0 = 1e-3 s to
-|grad E_s| <= 1e-6 N, PCG rtol 1e-6, <= 2000 iterations. One step = one full cold solve to the converged state.
+nu = 0.3, t = 5e-4 m, k_b = 1e-5 N m, IPC d_hat = 2e-3 m, kappa = 1e3; PTC from dt0 = 1e-3 s, PCG rtol 1e-6,
+<= 2000 iterations. One step = one full cold solve to the converged state: |grad E_s| <= 1e-7 N (--absolute), the
+residual at which the converged state lies within 1e-4 m of the f64 equilibrium; the solve's time to the scene's
+1e-6 N Newton tolerance is reported beside it ("secondary": the same run, read from its step records).
 Direction solver (--preconditioner): learned (default: the multilevel V-cycle flexible PCG with the shipped
 network's fine smoother), multilevel (spectral Jacobi smoothing), jacobi (the reference's block-Jacobi PCG).
 --compare jacobi (default) adds one device-timed block-Jacobi solve of the same workload after the timed steps, the
@@ -13,15 +15,19 @@ reference ships no dataset; seeded jitter, seed 0).
 value: seconds per converged solve with the problem resident in HBM (CUDA-event-timed solve, max over ranks).
 e2e:   the same through the C ABI from host arrays: drape_create (host->device copies) + solve + drape_get_state
        (device->host), wall clock on the host.
+error: after the timed steps, the f64 oracle polishes the last converged state on the host (band-Cholesky Newton
+       to 1e-8 N) and the line gives the max vertex distance, the relative static-energy error and the f64 residual.
 --impl reference: the reference's CPU implementation of this path (the f64 oracle restatement; the Rust crate
-       cannot be built here), single-threaded like the reference, on a bounded sample of the same solve: its
-       seconds per Newton iteration times the Newton iterations of the whole solve (FULL_SOLVE_NEWTON);
-       --full-solve times the oracle's whole solve instead.
+       cannot be built here), single-threaded like the reference, on a bounded sample of the same solve, scaled
+       by the oracle's own whole solve of this workload (FULL_SOLVE: its time to the sample's step over its time
+       to the end, measured once on one core); --full-solve times the oracle's whole solve instead.
+--probe cycle|network|spmv|solve: the stand-alone workloads the profiles were captured on (see probe()).
 Multi-GPU: replicas only (one independent drape per rank, no collective on the data path).
 """
 import argparse
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -117,6 +123,19 @@ PRECOND = {"jacobi": "block-Jacobi PCG", "multilevel": "multilevel V-cycle flexi
            "learned": "multilevel V-cycle flexible PCG with the network-predicted fine smoother"}
 
 
+def tolerance_crossing(records, tolerance):
+    """The solve's figures at the first moment its |grad E_s| was <= `tolerance`, from the step records of a solve
+    run to a tighter tolerance (the solve is deterministic, so a solve stopped at `tolerance` ends exactly there):
+    host seconds, PTC steps, Newton and PCG iterations up to that moment; None if the solve never got there."""
+    for k, r in enumerate(records):
+        if r["residual"] <= tolerance:
+            done = records[:k]
+            return {"tolerance_N": tolerance, "seconds": done[-1]["seconds"] if done else 0.0, "ptc_steps": k,
+                    "newton_iterations": int(sum(d["inner"] for d in done)),
+                    "pcg_iterations": int(sum(d["pcg_iterations"] for d in done))}
+    return None
+
+
 def run_gpu(args):
     import numpy as np
     import torch
@@ -134,8 +153,10 @@ def run_gpu(args):
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
     def options_for(name):
         return api.default_options(pcg_max_iterations=args.pcg_max, max_steps=args.max_steps,
+                                   equilibrium_absolute=args.absolute,
                                    preconditioner={"jacobi": 0, "multilevel": 1, "learned": 2}[name])
 
     net = api.Network.trained(device=local) if args.preconditioner == "learned" or args.compare == "all" else None
@@ -173,19 +194,20 @@ def run_gpu(args):
         state = drape.state
         t1 = time.perf_counter()
         barrier()
+        records = drape.step_records()
         drape.close()
         # The solve's time: CUDA events recorded by the library on its stream at the start and end of the solve
         # (with a synchronize before the end event is read); the host decisions between launches are inside.
-        return log, log["device_seconds"], t1 - t0, state
+        return log, log["device_seconds"], t1 - t0, state, records
 
     for _ in range(args.warmup):
         one_step()
     logs, secs, e2e = [], [], []
     with ClockSampler(local) as clock:
         for _ in range(args.steps):
-            log, s, w, state = one_step()
+            log, s_dev, w, state, records = one_step()
             logs.append(log)
-            secs.append(s)
+            secs.append(s_dev)
             e2e.append(w)
     clocks = clock.summary()
     t = sum(secs) / len(secs)
@@ -211,29 +233,48 @@ def run_gpu(args):
     else:
         kernel = "multilevel flexible PCG iteration (restrict/tail/prolong/direction/update kernels, one graph)"
         bytes_per_iter = multilevel_bytes_per_iteration(args.n, R, B)
+        tpath = os.path.join(ROOT, "profiles", "multilevel_traffic.json")
+        if os.path.exists(tpath):
+            tr = json.load(open(tpath))
+            if tr.get("columns") == args.n:
+                # DRAM bytes of one flexible PCG iteration (the sum over its kernels, ncu capture of the stand-alone
+                # cycle workload, bench.py --probe cycle), expressed per launch of the solve graph like `achieved`.
+                traffic = tr["dram_bytes_per_iteration"] * last["pcg_iterations"] / max(1, last["pcg_launches"])
     achieved = (bytes_per_iter * last["pcg_iterations"]) / (last["ms_pcg"] / 1e3) / 1e9 if last["ms_pcg"] > 0 else 0.0
+    # Device-time equivalent of the secondary tolerance's host seconds (the solve's device/host time ratio).
+    scale = last["device_seconds"] / last["seconds"] if last["seconds"] > 0 else 1.0
+    secondary = tolerance_crossing(records, args.secondary)
+    if secondary:
+        secondary["device_seconds"] = secondary["seconds"] * scale
     comparison = {}
     others = {"none": (), "jacobi": ("jacobi",), "all": ("jacobi", "multilevel", "learned")}[args.compare]
     if others:  # every rank runs the same comparison solves (replicas; one_step holds the barriers), rank 0 reports
         for other in others:
             if other == args.preconditioner:
                 continue
-            log_o, s_o, _, _ = one_step(other)
+            log_o, s_o, _, _, rec_o = one_step(other)
+            sec_o = tolerance_crossing(rec_o, args.secondary)
+            if sec_o:
+                sec_o["device_seconds"] = sec_o["seconds"] * (log_o["device_seconds"] / max(log_o["seconds"], 1e-9))
             comparison[other] = {"seconds": s_o, "ptc_steps": log_o["ptc_steps"],
                                  "newton_iterations": log_o["newton_iterations"],
                                  "pcg_iterations": log_o["pcg_iterations"],
                                  "pcg_per_newton": log_o["pcg_iterations"] / max(1, log_o["newton_iterations"]),
                                  "fallbacks_to_jacobi": log_o["fallbacks"], "converged": log_o["reason"] == "tolerance",
-                                 "final_residual_N": log_o["final_residual"]}
+                                 "final_residual_N": log_o["final_residual"], "secondary": sec_o}
         if "jacobi" in comparison:
             comparison["jacobi_seconds_over_this"] = comparison["jacobi"]["seconds"] / t
+            if secondary and comparison["jacobi"]["secondary"]:
+                comparison["jacobi_over_this_at_secondary"] = (comparison["jacobi"]["secondary"]["device_seconds"] /
+                                                               max(secondary["device_seconds"], 1e-9))
     out = {
         "metric": METRIC, "value": t, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": f"sheet n{args.n} over sphere r=0.25 + ground plane y=-0.25, {PRECOND[args.preconditioner]}, "
-                               f"PTC dt0=1e-3 s to |grad E_s|<=1e-6 N", "columns": args.n, "rows": R, "blocks": B,
-                   "seed": args.seed, "preconditioner": args.preconditioner, "parallelism": f"replicas{world}",
+                               f"PTC dt0=1e-3 s to |grad E_s|<={args.absolute:g} N", "columns": args.n, "rows": R,
+                   "blocks": B, "seed": args.seed, "preconditioner": args.preconditioner,
+                   "tolerance_N": args.absolute, "parallelism": f"replicas{world}",
                    "l2": "flushed (512 MiB write) before every timed solve"},
         "solve": {"converged": last["reason"] == "tolerance", "reason": last["reason"],
                   "final_residual_N": last["final_residual"], "ptc_steps": last["ptc_steps"],
@@ -242,6 +283,7 @@ def run_gpu(args):
                   "rejected_attempts": last["rejected_attempts"], "static_energy_J": last["static_energy"],
                   "fallbacks_to_jacobi": last["fallbacks"], "mg_levels": last["mg_levels"],
                   "phase_ms": {k: last[k] for k in ("ms_assembly", "ms_pcg", "ms_line_search", "ms_ccd", "ms_other")}},
+        "secondary": secondary,
         "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(sum(l["kernel_launches"] for l in logs)),
         "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved,
@@ -256,58 +298,97 @@ def run_gpu(args):
         comparison["this_run"] = args.preconditioner
         out["comparison"] = comparison
     if rank == 0 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(args, last)
+        out["cpu_baseline"], out["error"] = cpu_leg(args, state)
     if dist:
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(out), flush=True)
 
 
-# Newton iterations of the whole cold solve of a bench workload, keyed by (n, plane, seed), and where the count
-# comes from: the f64 oracle's own whole solve (`python bench.py --impl reference --full-solve`, no CPU budget) where
-# it has been run, else the block-Jacobi GPU solve of the same workload (the reference's method, f32 PCG; 424 PTC
-# steps at n129).
-FULL_SOLVE_NEWTON = {(129, 1, 0): (3162, "the block-Jacobi GPU solve of this workload")}
+# The f64 oracle's own whole cold solve of a bench workload, keyed by (n, plane, seed, tolerance in N): its time,
+# counts, and its cumulative time at the end of each of its first PTC steps (the scale of a bounded sample). Run
+# once with `python bench.py --impl reference --full-solve --record` on one core of the build container (Intel Xeon
+# @ 2.7 GHz), not on the GPU box. None where it has not been run.
+FULL_SOLVE = {
+    (33, 1, 0, 1e-07): {
+        "seconds": 30.231,
+        "steps": 76,
+        "newton": 494,
+        "seconds_to_1e-6": 29.961,
+        "host": "Intel(R) Xeon(R) Processor @ 2.70GHz (build container), 1 core",
+        "seconds_at_step": [0.01, 0.02, 0.031, 0.043, 0.06, 0.084, 0.113, 0.366, 0.615, 0.985, 1.03, 1.23, 1.807,
+            1.884, 2.429, 3.55, 3.699, 4.047, 4.328, 4.616, 4.735, 5.064, 5.323, 5.359, 5.48, 5.856, 6.297, 6.353,
+            6.434, 7.072, 7.274, 7.783, 8.45, 8.944, 9.397, 9.626, 9.888, 9.924, 9.981, 10.312, 10.741, 10.832,
+            11.537, 11.771, 12.602, 12.872, 13.568, 13.943, 14.064, 14.433, 14.639, 14.923, 15.368, 16.065, 16.396,
+            16.661, 17.251, 18.468, 18.843, 19.546, 20.746, 21.452, 21.662, 22.632, 23.599, 24.356, 25.289, 25.68,
+            26.142, 26.613, 27.442, 28.568, 28.888, 29.68, 29.961, 30.231],
+    },
+}
 
 
-def full_newton_count(args, gpu_log=None):
-    """(Newton iterations of the whole solve, where the count comes from), or (None, ...) when neither the table
-    nor this run's GPU solve gives one."""
-    known = FULL_SOLVE_NEWTON.get((args.n, int(args.plane), args.seed))
-    if known is not None:
-        return known
-    if gpu_log:
-        return int(gpu_log["newton_iterations"]), "this run's GPU solve"
-    return None, "none"
-
-
-def cpu_baseline(args, gpu_log=None, budget_s=None):
-    """The f64 oracle (port of the reference crate's method: exact tangent, LM, f64 block-Jacobi PCG rtol 1e-6
-    <= 2000 iterations, inner-count PTC from dt0 = 1e-3 s) timed on the host. It runs the cold solve until `budget_s`
-    of CPU time has passed (0: to the end) and reports the whole solve's time as its seconds per Newton iteration
-    times the Newton iterations of the whole solve: the counted whole solve of this workload, else this run's
-    GPU solve. With neither, the solve runs to the end and its own time is the value."""
+def _oracle_solve(args, budget):
+    """The oracle's cold solve of the bench workload (port of the reference crate's method: exact tangent, LM, f64
+    block-Jacobi PCG rtol 1e-6 <= 2000 iterations, inner-count PTC from dt0 = 1e-3 s), stopped at the first PTC step
+    that ends past `budget` s (0: to the tolerance). Returns its statistics (oracle_py.Scene.ptc)."""
     from tests import oracle_py
 
-    budget = budget_s if budget_s is not None else args.cpu_budget
-    full_newton, source = full_newton_count(args, gpu_log)
-    if full_newton is None:
-        budget = 0.0
     s = oracle_py.Scene("sheet", args.n, seed=args.seed, plane=bool(args.plane))
-    # The cold solve, stopped at the first PTC step that ends past the CPU budget.
-    _, st = s.ptc(h0=1e-3, doubling=False, absolute=1e-6, pcg=True, rtol=1e-6, maxit=2000, budget_s=budget)
+    _, st = s.ptc(h0=1e-3, doubling=False, absolute=args.absolute, pcg=True, rtol=1e-6, maxit=2000, budget_s=budget)
+    return st
+
+
+def cpu_baseline(args, budget_s=None):
+    """The f64 oracle timed on this host, single-threaded like the reference crate: a bounded sample of the cold
+    solve (the PTC steps that end within `budget_s`), scaled by the oracle's own whole solve of this workload
+    (FULL_SOLVE: whole-solve seconds over its seconds to the same step). Without a whole-solve record (or with
+    budget 0) the solve runs to the end and its own time is the value."""
+    budget = budget_s if budget_s is not None else args.cpu_budget
+    key = (args.n, int(args.plane), args.seed, args.absolute)
+    whole = FULL_SOLVE.get(key)
+    if whole is None and args.n <= 33:
+        budget = 0.0  # small enough to run whole (n33: ~30 s on one core)
+    st = _oracle_solve(args, budget)
     steps, elapsed, newton = int(st["steps"]), st["seconds"], int(st["newton"])
+    base = {"unit": "s", "cores": 1, "kind": "port", "host_cpu": _cpu_model()}
+    if whole is None and budget != 0.0:
+        # No whole-solve record to scale by: the sample is reported as what it is, a lower bound.
+        return dict(base, value=elapsed, sample_only=True,
+                    sample=f"{steps} PTC steps ({newton} Newton iterations) of the n{args.n} solve in {elapsed:.1f} s "
+                           f"on 1 host core; no whole-solve record of this workload, so the value is the sample's "
+                           f"time alone (a lower bound of the whole solve's)")
     if budget == 0.0:
-        return {"value": elapsed, "unit": "s", "cores": 1, "kind": "port", "newton_iterations": newton,
-                "converged": bool(st["converged"]),
-                "sample": f"the whole n{args.n} solve ({steps} PTC steps, {newton} Newton iterations) on 1 host core",
-                "host_cpu": _cpu_model()}
-    per_newton = elapsed / max(1, newton)
-    return {"value": per_newton * full_newton, "unit": "s", "cores": 1, "kind": "port",
-            "sample": f"{steps} PTC steps ({newton} Newton iterations) of the n{args.n} solve in {elapsed:.1f} s on 1 "
-                      f"host core; value = {per_newton:.3f} s per Newton iteration x {full_newton} Newton iterations "
-                      f"of the whole solve ({source})",
-            "host_cpu": _cpu_model()}
+        return dict(base, value=elapsed, newton_iterations=newton, converged=bool(st["converged"]),
+                    sample=f"the whole n{args.n} solve to {args.absolute:g} N ({steps} PTC steps, {newton} Newton "
+                           f"iterations) on 1 host core")
+    at = whole["seconds_at_step"]
+    k = min(steps, len(at))
+    ratio = whole["seconds"] / at[k - 1]
+    return dict(base, value=elapsed * ratio, extrapolated=True,
+                sample=f"{steps} PTC steps ({newton} Newton iterations) of the n{args.n} solve in {elapsed:.1f} s on 1 "
+                       f"host core, x {ratio:.2f} = the oracle's own whole solve to {args.absolute:g} N "
+                       f"({whole['steps']} PTC steps, {whole['newton']} Newton iterations, {whole['seconds']:.0f} s on "
+                       f"{whole['host']}) over its first {k} steps ({at[k - 1]:.1f} s there)",
+                whole_solve_measured={"seconds": whole["seconds"], "ptc_steps": whole["steps"],
+                                      "newton_iterations": whole["newton"], "host": whole["host"],
+                                      "seconds_to_1e-6_N": whole.get("seconds_to_1e-6")})
+
+
+def cpu_leg(args, gpu_state):
+    """Rank 0, after the timed steps: the CPU baseline, and the f64 error of the last converged GPU state (the oracle
+    polishes it with band-Cholesky Newton to 1e-8 N; max vertex distance, relative static-energy error, the f64
+    residual at the GPU state)."""
+    from tests import oracle_py
+    from tests.polish_state import polished_error
+
+    oracle_py.build()
+    base = cpu_baseline(args)
+    t0 = time.perf_counter()
+    oracle = oracle_py.Scene("sheet", args.n, seed=args.seed, plane=bool(args.plane))
+    err, e_rel, r64, _, st = polished_error(oracle, gpu_state, require_converged=False)
+    error = {"max_vertex_m": err, "relative_energy": e_rel, "f64_residual_N": r64,
+             "polish_converged": bool(st["converged"]), "polish_newton": int(st["newton"]),
+             "polish_cpu_s": time.perf_counter() - t0, "bound_m": 1e-4, "within_bound": bool(err <= 1e-4)}
+    return base, error
 
 
 def _cpu_model():
@@ -330,7 +411,7 @@ def run_reference(args):
     results = []
     budget = 0.0 if args.full_solve else args.cpu_budget
     for i in range(args.warmup if args.full_solve else 0, args.warmup + args.steps):  # a full solve needs no warm-up
-        r = cpu_baseline(args, None, budget_s=budget)
+        r = cpu_baseline(args, budget_s=budget)
         if i >= args.warmup:
             results.append(r)
     v = sum(r["value"] for r in results) / len(results)
@@ -338,13 +419,143 @@ def run_reference(args):
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
            "config": {"workload": f"sheet n{args.n} over sphere r=0.25 + ground plane y=-0.25, f64 oracle port "
-                                  f"(exact tangent, LM, block-Jacobi PCG rtol 1e-6 <= 2000)", "columns": args.n},
-           "cpu_baseline": {"value": v, "unit": "s", "cores": 1, "kind": "port", "sample": results[-1]["sample"]},
+                                  f"(exact tangent, LM, block-Jacobi PCG rtol 1e-6 <= 2000), PTC dt0=1e-3 s to "
+                                  f"|grad E_s|<={args.absolute:g} N", "columns": args.n, "tolerance_N": args.absolute},
+           "cpu_baseline": {k: results[-1][k] for k in results[-1] if k != "value"} | {"value": v},
            "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if "newton_iterations" in results[-1]:
         out["newton_iterations"] = results[-1]["newton_iterations"]
         out["converged"] = results[-1]["converged"]
     print(json.dumps(out), flush=True)
+
+
+def record_full_solve(args):
+    """--impl reference --full-solve --record: the oracle's whole solve with per-step times (its progress lines),
+    printed as the FULL_SOLVE entry for this workload."""
+    from tests import oracle_py
+
+    oracle_py.build()
+    cmd = [sys.executable, "-c",
+           "import sys; sys.path.insert(0, %r); from tests import oracle_py; "
+           "s = oracle_py.Scene('sheet', %d, seed=%d, plane=%s); "
+           "s.ptc(h0=1e-3, doubling=False, absolute=%r, pcg=True, rtol=1e-6, maxit=2000, progress=True)"
+           % (ROOT, args.n, args.seed, bool(args.plane), args.absolute)]
+    proc = subprocess.run(cmd, stderr=subprocess.PIPE, text=True, check=True)
+    print(json.dumps(parse_progress(proc.stderr.splitlines(), _cpu_model())), flush=True)
+
+
+def parse_progress(lines, host):
+    """FULL_SOLVE entry from the oracle's progress lines ('state after K steps: residual R N at T s, N Newton
+    iterations'): cumulative seconds at the end of each of the first 200 steps, the whole solve, and the time at
+    which the residual first fell to 1e-6 N."""
+    pat = re.compile(r"state after (\d+) steps: residual ([0-9.eE+-]+) N at ([0-9.]+) s, (\d+) Newton")
+    at, t6, last = [], None, None
+    for line in lines:
+        m = pat.search(line)
+        if not m:
+            continue
+        k, r, sec, newton = int(m.group(1)), float(m.group(2)), float(m.group(3)), int(m.group(4))
+        if k >= 1 and len(at) < 200:
+            at.append(sec)
+        if t6 is None and r <= 1e-6:
+            t6 = sec
+        last = (k, sec, newton)
+    return {"seconds": last[1], "steps": last[0], "newton": last[2], "seconds_to_1e-6": t6, "host": host,
+            "seconds_at_step": at}
+
+
+def probe(args):
+    """Stand-alone workloads the profiles were captured on (ncu needs kernels outside the solve's conditional
+    graph, and small, repeatable cases):
+      cycle    PTC steps of the n x n sheet drape with the multilevel preconditioner, then the projected PTC system
+               at that state: stand-alone V-cycles and flexible PCG iterations on it (drape_time_multilevel), a
+               fine SpMV;
+      network  the same system: the shipped network's forward (drape_network_gradient) and one learned PCG solve;
+      spmv     `drapes` sheets of the batched configuration concatenated block-diagonally, and the n257 sheet's
+               matrix: every lanes-per-row x threads shape of the SpMV kernel timed, the fastest checked against
+               numpy and reported in algorithmic GB/s (40 B per block + 28 B per row) against the measured HBM peak;
+      solve    the bench scene's cold solve to --absolute; the converged positions go to --out (an .npy file)."""
+    import ctypes
+
+    import numpy as np
+
+    from drape_b200 import api
+    from drape_b200.scenes import GRAVITY, batch_scenes, sheet_matrix
+
+    pre = {"jacobi": 0, "multilevel": 1, "learned": 2}[args.preconditioner]
+    if args.probe == "solve":
+        d = api.Drape.sheet(args.n, seed=args.seed, plane=bool(args.plane),
+                            options=api.default_options(preconditioner=pre, equilibrium_absolute=args.absolute,
+                                                        time_budget_s=args.budget))
+        if pre == 2:
+            d.set_network(api.Network.trained())
+        log = d.solve_equilibrium(check=False)
+        if args.out:
+            np.save(args.out, d.state)
+        keys = ("reason", "ptc_steps", "newton_iterations", "pcg_iterations", "fallbacks", "ms_pcg", "final_residual",
+                "device_seconds", "static_energy")
+        return {k: log[k] for k in keys}
+    if args.probe == "spmv":
+        parts, offset = [], 0
+        for n, seed, radius, young in batch_scenes(args.drapes):
+            rp, ci, blk = sheet_matrix(n, seed, radius, young)
+            parts.append((rp, ci + offset, blk))
+            offset += len(rp) - 1
+        rp_all, base = [np.zeros(1, np.int64)], 0
+        for rp, _, _ in parts:
+            rp_all.append(rp[1:] + base)
+            base += rp[-1]
+        batch = (np.concatenate(rp_all), np.concatenate([p[1] for p in parts]), np.concatenate([p[2] for p in parts]))
+        peak = peaks()["hbm_gbs"]
+        out = {}
+        for name, (rp, ci, blk) in (("batched", batch), ("n257", sheet_matrix(257, 0, 0.25, 5e5))):
+            R, B = len(rp) - 1, len(ci)
+            x = np.random.default_rng(1).standard_normal(3 * R).astype(np.float32)
+            shapes = {f"{lanes}x{threads}": api.spmv_benchmark(rp, ci, blk, x, 20, lanes, threads)
+                      for lanes in (4, 8, 16, 32) for threads in (128, 256)}
+            best = min(shapes, key=shapes.get)
+            lanes, threads = (int(v) for v in best.split("x"))
+            ms, y = api.spmv_benchmark(rp, ci, blk, x, 20, lanes, threads, result=True)
+            rows = np.repeat(np.arange(R), np.diff(rp))
+            ref = np.zeros((R, 3))
+            np.add.at(ref, rows, np.einsum("kab,kb->ka", blk.reshape(-1, 3, 3).astype(np.float64),
+                                           x.reshape(-1, 3).astype(np.float64)[ci]))
+            bytes_ = 40 * B + 28 * R
+            out[name] = {"rows": R, "blocks": B, "algorithmic_MB": bytes_ / 1e6, "best_shape": best, "ms": ms,
+                         "GB_per_s": bytes_ / (ms * 1e-3) / 1e9, "fraction_of_peak": bytes_ / (ms * 1e-3) / 1e9 / peak,
+                         "peak_GB_per_s": peak,
+                         "relative_error_vs_numpy": float(np.linalg.norm(y - ref.reshape(-1)) / np.linalg.norm(ref)),
+                         "all_shapes_ms": shapes}
+        return out
+    d = api.Drape.sheet(args.n, seed=args.seed, plane=bool(args.plane),
+                        options=api.default_options(max_steps=args.probe_steps, preconditioner=1))
+    d.solve_equilibrium(check=False)
+    x, h = d.state, d.final_h()
+    d.set_options(api.default_options(tangent=1))
+    g, blocks = d.assemble(x, x_hat=x + h * h * np.tile(GRAVITY, d.V), h=h, mode=0, curvature=False)
+    b = -g
+    lib = api.load()
+    out = {"probe": args.probe, "columns": args.n, "ptc_steps": args.probe_steps}
+    if args.probe == "cycle":
+        d.set_options(api.default_options(preconditioner=1))
+        _, info = d.pcg(b, 1e-6, 2000, blocks=blocks)
+        out["pcg"] = info
+        lib.drape_time_multilevel.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]
+        tm = (ctypes.c_float * 3)()
+        for its in (20, 200):
+            assert lib.drape_time_multilevel(d.h, its, tm) == 0, lib.drape_last_error(d.h)
+            out[f"iterations_{its}"] = {"vcycle_ms": tm[0], "pcg_iteration_ms": tm[1], "pdl": tm[2]}
+        out["spmv_ms"] = d.time_spmv(200, 8, 256)
+    else:
+        net = api.Network.trained()
+        d.set_options(api.default_options(preconditioner=1))
+        sol, _ = d.pcg(b, 1e-8, 4000, blocks=blocks)
+        loss, _, fac = net.gradient(d, blocks, b, sol)
+        d.set_options(api.default_options(preconditioner=2))
+        d.set_network(net)
+        _, info = d.pcg(b, 1e-6, 2000, blocks=blocks)
+        out.update({"loss": loss, "factor_min": float(fac.min()), "factor_max": float(fac.max()), "pcg": info})
+    return out
 
 
 def main():
@@ -358,16 +569,32 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--pcg-max", type=int, default=2000)
     ap.add_argument("--max-steps", type=int, default=1000)
+    ap.add_argument("--absolute", type=float, default=1e-7, help="stop at |grad E_s| <= this (N)")
+    ap.add_argument("--secondary", type=float, default=1e-6,
+                    help="also report the time at which the solve first reached |grad E_s| <= this (N)")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--full-solve", action="store_true",
                     help="--impl reference: time the oracle's whole solve instead of a bounded sample")
+    ap.add_argument("--record", action="store_true",
+                    help="--impl reference --full-solve: print the FULL_SOLVE entry (per-step times) of the solve")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--preconditioner", default="learned", choices=["jacobi", "multilevel", "learned"])
     ap.add_argument("--compare", default="jacobi", choices=["none", "jacobi", "all"],
                     help="after the timed steps, one device-timed solve of the same workload with each other solver")
+    ap.add_argument("--probe", default=None, choices=["cycle", "network", "spmv", "solve"],
+                    help="run one stand-alone profiling workload instead of the benchmark (see probe())")
+    ap.add_argument("--probe-steps", type=int, default=20, help="--probe cycle/network: PTC steps before the system")
+    ap.add_argument("--drapes", type=int, default=128, help="--probe spmv: drapes of the batched configuration")
+    ap.add_argument("--budget", type=float, default=0.0, help="--probe solve: the solver's time budget, s")
+    ap.add_argument("--out", default=None, help="--probe solve: .npy file for the converged positions")
     args = ap.parse_args()
-    if args.impl == "reference":
-        run_reference(args)
+    if args.probe:
+        print(json.dumps(probe(args)), flush=True)
+    elif args.impl == "reference":
+        if args.full_solve and args.record:
+            record_full_solve(args)
+        else:
+            run_reference(args)
     else:
         run_gpu(args)
 

@@ -75,7 +75,7 @@ class ProblemView(ctypes.Structure):
 class StepRecord(ctypes.Structure):
     _fields_ = [("step", ctypes.c_int32), ("inner", ctypes.c_int32), ("rejected", ctypes.c_int32),
                 ("pcg_iterations", ctypes.c_int32), ("h", ctypes.c_double), ("residual", ctypes.c_double),
-                ("min_distance", ctypes.c_double)]
+                ("min_distance", ctypes.c_double), ("seconds", ctypes.c_double)]
 
 
 class NewtonRecord(ctypes.Structure):

@@ -686,6 +686,7 @@ int Context::solve_equilibrium(const double* start, double h0, drape_run_log* lo
     rec.pcg_iterations = res.pcg_iterations;
     kcheck(launch_min_distance(dp_, x_.ptr, partial_.ptr, kReduceGrid, stream_), "min_distance");
     rec.min_distance = reduce_partials(kReduceGrid, 1, kMinDist);
+    rec.seconds = elapsed();
     steps_.push_back(rec);
     if (keep_states_) {  // the accepted state in f32 (drape-e7.ts:175)
       std::vector<double> xs(nv);

@@ -8,16 +8,17 @@
 // solver as drape_pcg with its work space in one fixed, file-scope device array instead of allocations.
 //
 // The array is sized for kNoAllocMaxRows block rows (about 3.4 MB) and every GPU that loads the library keeps it
-// until the process exits. In host code `g_noalloc_scratch` names a host-side stand-in, not device memory: the
-// device address is obtained once per device with cudaGetSymbolAddress while that device is current, and only
-// that address is handed to kernels.
+// until the process exits. In host code `g_noalloc_scratch` names a host-side stand-in, not device memory: every
+// call looks up the device address with cudaGetSymbolAddress while the caller's device is current (a lookup in
+// the loaded module, no allocation), and only that address is handed to kernels. Looking it up on every call
+// instead of caching it keeps the address valid after cudaDeviceReset or when the caller makes another context
+// current on the same device.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
-#include <mutex>
 #include <string>
 
 #include "../../include/drape_b200.h"
@@ -46,10 +47,6 @@ constexpr size_t kSyncBytes = sizeof(drape::PcgSyncHeader) + 32 * size_t(kNoAllo
 constexpr size_t kScratchBytes = (kOffSync + kSyncBytes + 255) / 256 * 256;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
-
-// Device address of g_noalloc_scratch per device, resolved on the first call on that device.
-std::mutex g_setup_mutex;
-void* g_scratch_ptr[64] = {};
 
 // Position of each row's diagonal block; flags[0] = 1 when a row has none.
 __global__ void find_diagonal(int R, const int* row_ptr, const int* col_idx, int* diag_pos, int* flags) {
@@ -87,18 +84,16 @@ extern "C" drape_status drape_pcg_noalloc(int32_t rows, const int32_t* row_ptr, 
     return fail("drape_pcg_noalloc: a0, a1, rhs and x must be 16-byte aligned", DRAPE_E_ARG);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return fail("drape_pcg_noalloc: no current device", DRAPE_E_CUDA);
+  if (cudaGetDevice(&dev) != cudaSuccess) return fail("drape_pcg_noalloc: no current device", DRAPE_E_CUDA);
   unsigned char* base = nullptr;
   {
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[dev]) {
-      // Once per device, with that device current: the device address of the file-scope array.
-      void* p = nullptr;
-      cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-      if (e != cudaSuccess) return fail(std::string("drape_pcg_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e), DRAPE_E_CUDA);
-      g_scratch_ptr[dev] = p;
-    }
-    base = static_cast<unsigned char*>(g_scratch_ptr[dev]);
+    // The device address of the file-scope array in the current context (on the first call on a device this
+    // also loads the library's device code there, which is why that call should come before any stream capture).
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(std::string("drape_pcg_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e), DRAPE_E_CUDA);
+    base = static_cast<unsigned char*>(p);
   }
   // Launch shape: as the context's, with the matrix read from global memory (no per-CTA block capacity needed).
   int sms = 0;
@@ -111,9 +106,12 @@ extern "C" drape_status drape_pcg_noalloc(int32_t rows, const int32_t* row_ptr, 
   cfg.lanes_per_row = kLanes;
   cfg.matrix_in_smem = false;
   cfg.smem = drape::pcg_smem_bytes(cap_rows, 0, false);
-  const int fit = drape::pcg_max_grid(kThreads, kLanes, cfg.smem, false);
-  if (fit <= 0) return fail("drape_pcg_noalloc: the PCG kernel does not fit on this device", DRAPE_E_CUDA);
-  if (grid > fit) {
+  // Fewer CTAs hold more rows each and so need more shared memory, which can lower the co-resident count again:
+  // shrink until the grid fits the occupancy at its own shared-memory size.
+  for (;;) {
+    const int fit = drape::pcg_max_grid(kThreads, kLanes, cfg.smem, false);
+    if (fit <= 0) return fail("drape_pcg_noalloc: the PCG kernel does not fit on this device", DRAPE_E_CUDA);
+    if (grid <= fit) break;
     grid = fit;
     cap_rows = (rows + grid - 1) / grid + 1;
     cfg.smem = drape::pcg_smem_bytes(cap_rows, 0, false);

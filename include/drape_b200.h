@@ -104,10 +104,13 @@ typedef struct {
   int32_t pad;
 } drape_run_log;
 
-/* One accepted PTC step (gpu-ptc.bin columns, run-e7.ts:96). */
+/* One accepted PTC step (gpu-ptc.bin columns, run-e7.ts:96). residual is |grad E_s| at the step's start;
+ * seconds is the solve's host time at the step's end (the solve synchronizes its stream there), so a solve run to
+ * a tight tolerance also tells when it passed a looser one: the first step whose starting residual is below that
+ * tolerance starts at the previous step's `seconds`. */
 typedef struct {
   int32_t step, inner, rejected, pcg_iterations;
-  double h, residual, min_distance;
+  double h, residual, min_distance, seconds;
 } drape_step_record;
 
 /* One Newton iterate of a solve: the reference's IterationRecord and the RobustRecord fields this solver has
@@ -316,10 +319,13 @@ drape_status drape_network_train(drape_ctx* ctx, drape_network* net, int32_t tup
  *   a0, a1 [4B] and a2 [B]          blocks as the assembly writes them: a0 = (m00,m01,m02,m10),
  *                                   a1 = (m11,m12,m20,m21), a2 = m22 (a0, a1 16-byte aligned)
  *   rhs, x [4 * rows]               one 16-byte row each (x, y, z, unused); x receives the solution from 0
- * info = [iterations, status (1 converged, 2 iteration limit, 3 breakdown)], relative = sqrt(rr/rr0) (host).
- * The first call on a device looks up the array's device address (cudaGetSymbolAddress) and should come before
- * any stream capture. Calls share the one array and run on `stream` (NULL: the default stream) and return after
- * synchronizing it; calls that overlap on the GPU (other host threads, other streams) race on the array. */
+ * info (host, may be NULL) = int32_t[3]: [iterations, status (1 converged, 2 iteration limit, 3 breakdown),
+ * residual replacements]; relative (host, may be NULL) = sqrt(rr/rr0).
+ * Every call looks up the array's device address in the current context (cudaGetSymbolAddress; no allocation),
+ * so the address stays right after cudaDeviceReset or a context switch. The first call on a device also loads
+ * the library's device code there and should come before any stream capture. Calls share the one array and run
+ * on `stream` (NULL: the default stream) and return after synchronizing it; calls that overlap on the GPU (other
+ * host threads, other streams) race on the array. */
 #define DRAPE_NOALLOC_MAX_ROWS 65536
 drape_status drape_pcg_noalloc(int32_t rows, const int32_t* row_ptr, const int32_t* col_idx, const float* a0,
                                const float* a1, const float* a2, const float* rhs, float* x, double rtol,

@@ -494,10 +494,14 @@ PtcRun ptc_solve(const Drape& d, std::vector<Vec3> start, double h_start, const 
   run.states.push_back(std::move(start));
   std::vector<Vec3> x = run.states.back();
   auto t0 = std::chrono::steady_clock::now();
+  int newton_total = 0;
   for (;;) {
     run.final_residual = vector_norm(static_gradient(d, x));
-    if (rules.time_budget_s > 0 &&
-        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > rules.time_budget_s) {
+    double elapsed = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (progress)
+      std::fprintf(stderr, "state after %zu steps: residual %.6e N at %.3f s, %d Newton iterations\n", run.steps.size(),
+                   run.final_residual, elapsed, newton_total);
+    if (rules.time_budget_s > 0 && elapsed > rules.time_budget_s) {
       run.reason = "time_budget";
       break;
     }
@@ -517,6 +521,7 @@ PtcRun ptc_solve(const Drape& d, std::vector<Vec3> start, double h_start, const 
       std::fprintf(stderr, "ptc step %zu h=%.3e r/L=%.3e inner=%d rejected=%d mu=%g pcg=%d\n", run.steps.size() + 1,
                    step.h, run.final_residual / load, step.inner_iterations, step.rejected_attempts, step.max_mu,
                    step.pcg_iterations);
+    newton_total += step.inner_iterations;
     run.steps.push_back(step);
     x = std::move(next);
     if (keep_states)

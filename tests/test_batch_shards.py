@@ -7,7 +7,7 @@ import pytest
 import torch.multiprocessing as mp
 
 from drape_b200 import batch_shards
-from drape_b200.profile_workloads import batch_scenes
+from drape_b200.scenes import batch_scenes
 
 
 def test_partition_covers_every_drape_once_and_balances_rows():

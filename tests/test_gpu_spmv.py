@@ -4,7 +4,7 @@ import numpy as np
 import pytest
 
 from drape_b200 import api
-from drape_b200.profile_workloads import sheet_matrix
+from drape_b200.scenes import sheet_matrix
 
 pytestmark = pytest.mark.gpu
 
