@@ -38,6 +38,7 @@ class Options(ctypes.Structure):
         ("max_halvings", ctypes.c_int32), ("time_budget_s", ctypes.c_double), ("pcg_grid", ctypes.c_int32),
         ("pcg_threads", ctypes.c_int32), ("pcg_lanes", ctypes.c_int32), ("progress", ctypes.c_int32),
         ("newton_start", ctypes.c_int32), ("tangent", ctypes.c_int32), ("smoother_omega", ctypes.c_double),
+        ("prolongation", ctypes.c_int32), ("pad_options", ctypes.c_int32),
     ]
 
 
@@ -125,7 +126,7 @@ def load():
     lib.drape_set_network.argtypes = [P, P]
     lib.drape_network_gradient.argtypes = [P, P, P, P, P, P, P, P]
     lib.drape_network_train.argtypes = [P, P, ctypes.c_int32, P, P, P, ctypes.c_int32, ctypes.c_double, P]
-    lib.drape_multilevel_view.argtypes = [P, ctypes.c_int32, P, P, P]
+    lib.drape_multilevel_view.argtypes = [P, ctypes.c_int32, P, P, P, P]
     lib.drape_energy_change.argtypes = [P, P, P, ctypes.c_double, P, ctypes.c_double, ctypes.c_int32, P]
     lib.drape_max_step.argtypes = [P, P, P, P]
     lib.drape_static_residual.argtypes = [P, P, P]
@@ -358,15 +359,17 @@ class Drape:
         self._check(self.lib.drape_precondition(self.h, _ptr(blk), _ptr(_f64(r)), _ptr(z)))
         return z
 
-    def multilevel_view(self, level, operator=True):
-        """(columns, f64 stencil [225][rows] or None, f32 smoother [9][rows]) of one hierarchy level."""
-        cols = ctypes.c_int32()
-        self._check(self.lib.drape_multilevel_view(self.h, level, ctypes.byref(cols), None, None))
+    def multilevel_view(self, level, operator=True, width=False):
+        """(columns, f64 stencil [w^2 * 9][rows] or None, f32 smoother [9][rows]) of one hierarchy level, w its
+        stencil width (5, or 7 for level 1 under the smoothed prolongation); with width=True also w."""
+        cols, w = ctypes.c_int32(), ctypes.c_int32()
+        self._check(self.lib.drape_multilevel_view(self.h, level, ctypes.byref(cols), ctypes.byref(w), None, None))
         n = cols.value
-        op = np.zeros((225, n * n)) if operator and level > 0 else None
+        op = np.zeros((w.value * w.value * 9, n * n)) if operator and level > 0 else None
         sm = np.zeros((9, n * n), np.float32)
-        self._check(self.lib.drape_multilevel_view(self.h, level, ctypes.byref(cols), _ptr(op), _ptr(sm)))
-        return n, op, sm
+        self._check(self.lib.drape_multilevel_view(self.h, level, ctypes.byref(cols), ctypes.byref(w), _ptr(op),
+                                                   _ptr(sm)))
+        return (n, op, sm, w.value) if width else (n, op, sm)
 
     def energy_change(self, x, d, alpha, x_hat=None, h=0.0, mode=0):
         out = ctypes.c_double()

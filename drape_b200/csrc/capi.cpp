@@ -100,6 +100,7 @@ void drape_default_options(drape_options* o) {
   o->armijo = 1e-4;
   o->max_halvings = 30;
   o->time_budget_s = 0.0;
+  o->prolongation = 1;
 }
 
 drape_status drape_create(const drape_problem_view* v, const drape_options* options, int32_t device, drape_ctx** out) {
@@ -577,10 +578,13 @@ drape_status drape_precondition(drape_ctx* ctx, const float* blocks, const doubl
   });
 }
 
-drape_status drape_multilevel_view(drape_ctx* ctx, int32_t level, int32_t* columns, double* op, float* smoother) {
+drape_status drape_multilevel_view(drape_ctx* ctx, int32_t level, int32_t* columns, int32_t* width, double* op,
+                                   float* smoother) {
   return guarded(ctx, [&](drape::Context& c) {
     if (!columns) return fail(ctx, "columns is null", DRAPE_E_ARG);
-    const int n = c.multilevel_view(level, op, smoother);
+    int w = 0;
+    const int n = c.multilevel_view(level, &w, op, smoother);
+    if (width) *width = w;
     if (n < 0) return fail(ctx, "no such multilevel level", DRAPE_E_ARG);
     *columns = n;
     return DRAPE_OK;

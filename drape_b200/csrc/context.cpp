@@ -915,11 +915,13 @@ void Context::configure_mg() {
   int n[kMgMaxLevels], rows[kMgMaxLevels];
   n[0] = host_.columns;
   rows[0] = R;
-  size_t a_count = 0, s_count = 9 * size_t(R), v_count = 7 * size_t(R);
+  // Level 1 is stored for the 7 x 7 stencil of the smoothed prolongation (the bilinear one uses its first 25
+  // offsets per row); the fine level adds Sp (9R floats) and the vectors t, u, y of the smoothed fine steps.
+  size_t a_count = 0, s_count = 18 * size_t(R), v_count = 10 * size_t(R);
   for (int l = 1; l < L; ++l) {
     n[l] = (n[l - 1] - 1) / 2 + 1;
     rows[l] = n[l] * n[l];
-    a_count += size_t(kMgStencil) * 9 * rows[l];
+    a_count += size_t(l == 1 ? kMgStencilWide : kMgStencil) * 9 * rows[l];
     s_count += 9 * size_t(rows[l]);
     v_count += 3 * size_t(rows[l]);
   }
@@ -950,10 +952,11 @@ void Context::configure_mg() {
     lv.S = sm;
     sm += 9 * size_t(rows[l]);
     if (l > 0) {
+      const int cap = l == 1 ? kMgStencilWide : kMgStencil;
       lv.A64 = a64;
       lv.A = a32;
-      a64 += size_t(kMgStencil) * 9 * rows[l];
-      a32 += size_t(kMgStencil) * 3 * rows[l];
+      a64 += size_t(cap) * 9 * rows[l];
+      a32 += size_t(cap) * 3 * rows[l];
       lv.r = v;
       v += rows[l];
     }
@@ -967,6 +970,10 @@ void Context::configure_mg() {
   d.p[0] = v + 2 * size_t(R);
   d.p[1] = v + 3 * size_t(R);
   d.q = v + 4 * size_t(R);
+  d.t = v + 5 * size_t(R);
+  d.u = v + 6 * size_t(R);
+  d.y = v + 7 * size_t(R);
+  d.Sp = sm;
   d.b = b_.ptr;
   d.x = px_.ptr;
   d.coarse_inv = mg_inv_.ptr;
@@ -976,8 +983,22 @@ void Context::configure_mg() {
   d.state = reinterpret_cast<MgState*>(mg_state_.ptr);
   d.error = mg_error_.ptr;
   mg_ = d;
+  mg_prolongation_ = -1;
+  build_mg_graph();
+}
 
+// The solve graph for the prolongation the options ask for (the kernel sequence differs): level 1's stencil width
+// and the smoothed flag follow it. Rebuilt when the option changes.
+void Context::build_mg_graph() {
+  const int smoothed = opt_.prolongation != 0 ? 1 : 0;
+  if (mg_prolongation_ == smoothed) return;
   sync();
+  if (mg_graph_) {
+    cudaGraphExecDestroy(mg_graph_);
+    mg_graph_ = nullptr;
+  }
+  mg_.smoothed = smoothed;
+  mg_.lv[1].w = smoothed ? 7 : 5;
   // Programmatic dependent launch inside the loop body where the driver accepts it, plain edges otherwise.
   mg_graph_pdl_ = mg_build_solve_graph(mg_, stream_, &mg_graph_, &mg_graph_launches_, true) == cudaSuccess;
   if (!mg_graph_pdl_) {
@@ -985,19 +1006,23 @@ void Context::configure_mg() {
     mg_graph_ = nullptr;
     check(mg_build_solve_graph(mg_, stream_, &mg_graph_, &mg_graph_launches_, false), "multilevel solve graph");
   }
+  mg_prolongation_ = smoothed;
   mg_stale_ = true;
 }
 
 // Set-up for the matrix now in the BSR planes: smoothers, Galerkin products, coarsest inverse.
 void Context::mg_prepare() {
+  build_mg_graph();
   if (!mg_stale_) return;
   check(cudaMemsetAsync(mg_error_.ptr, 0, sizeof(int), stream_), "memset");
   const float omega = opt_.smoother_omega > 0 ? float(opt_.smoother_omega) : 0.0f;  // 0: spectral damping
   const bool reuse = omega == 0.0f && mg_setups_since_power_ < 4;
   mg_setups_since_power_ = reuse ? mg_setups_since_power_ + 1 : 1;
   kcheck(mg_setup(mg_, omega, true, reuse, stream_), "multilevel set-up");
-  // fine smoother, Galerkin products, coarse smoothers, coarsest inverse; the power method and its scaling
-  kernels_ += 2 * (mg_levels_ - 1) + (omega > 0 ? 0 : (reuse ? 0 : kMgPowerSteps + 1) + mg_levels_ - 2);
+  // fine smoother, Galerkin products, coarse smoothers, coarsest inverse; the power method (twice with the
+  // smoothed prolongation: the fine level first) and its scaling; Sp
+  kernels_ += 2 * (mg_levels_ - 1) + (omega > 0 ? 0 : (reuse ? 0 : (kMgPowerSteps + 1) * (mg_.smoothed ? 2 : 1)) +
+                                                       mg_levels_ - 1) + mg_.smoothed;
   if (opt_.preconditioner == 2) {
     if (!net_) throw std::invalid_argument("preconditioner 2 needs a preconditioner network (drape_set_network)");
     ensure_nn_buffers();
@@ -1095,12 +1120,13 @@ void Context::time_multilevel(int iterations, float* out3) {
   out3[2] = mg_graph_pdl_ ? 1.0f : 0.0f;
 }
 
-int Context::multilevel_view(int level, double* op, float* smoother) {
+int Context::multilevel_view(int level, int* width, double* op, float* smoother) {
   if (level < 0 || level >= mg_levels_) return -1;
   mg_prepare();
   const MgLevel& lv = mg_.lv[level];
+  if (width) *width = level > 0 ? lv.w : 0;
   if (op && level > 0)
-    check(cudaMemcpyAsync(op, lv.A64, size_t(kMgStencil) * 9 * lv.rows * sizeof(double), cudaMemcpyDeviceToHost,
+    check(cudaMemcpyAsync(op, lv.A64, size_t(lv.w) * lv.w * 9 * lv.rows * sizeof(double), cudaMemcpyDeviceToHost,
                           stream_), "download");
   if (smoother)
     check(cudaMemcpyAsync(smoother, lv.S, 9 * size_t(lv.rows) * sizeof(float), cudaMemcpyDeviceToHost, stream_),

@@ -128,8 +128,9 @@ class Context {
   int mg_levels() const { return mg_levels_; }
   // One V-cycle z = M r for the given f32 blocks (9B row-major) and right-hand side (the preconditioner check).
   void precondition_host(const float* blocks, const double* r, double* z);
-  // Level `level`'s grid columns, f64 Galerkin stencil [225][rows] (level >= 1) and smoother [9][rows].
-  int multilevel_view(int level, double* op, float* smoother);
+  // Level `level`'s grid columns, stencil width (width, 0 on the fine level), f64 Galerkin stencil
+  // [width^2 * 9][rows] (level >= 1) and smoother [9][rows].
+  int multilevel_view(int level, int* width, double* op, float* smoother);
 
   // ---- preconditioner network
   void attach_network(Network* net) { net_ = net; mg_stale_ = true; }
@@ -166,6 +167,7 @@ class Context {
   PcgResult direction_solve(double rtol, int max_iterations);
   PcgResult mg_pcg(double rtol, int max_iterations, bool* stalled);
   void configure_mg();
+  void build_mg_graph();
   void mg_prepare();
   void upload_blocks(const float* blocks);
   double direction_slope();
@@ -224,6 +226,7 @@ class Context {
   DeviceArray<int> mg_error_;
   MgState* pinned_mg_ = nullptr;
   cudaGraphExec_t mg_graph_ = nullptr;
+  int mg_prolongation_ = -1;  // the prolongation (0 bilinear, 1 smoothed) mg_ and mg_graph_ are built for
   int mg_graph_launches_ = 0;
   bool mg_graph_pdl_ = false;
 

@@ -73,16 +73,18 @@ __device__ __forceinline__ float3 smooth(const float* S, int rows, int i, float3
                      m[2] * r.x + m[5] * r.y + m[8] * r.z);
 }
 
-// Coarse stencil row I times the vector v at the offset's neighbour (0 outside the grid).
-__device__ __forceinline__ bool stencil_neighbour(int n, int X, int Y, int o, int* J) {
-  int dx = o % 5 - 2, dy = o / 5 - 2, x = X + dx, y = Y + dy;
+// Column vertex J of offset o in a stencil of width w around (X, Y) on an n x n grid (false outside the grid).
+__device__ __forceinline__ bool stencil_neighbour(int n, int w, int X, int Y, int o, int* J) {
+  const int h = w >> 1;
+  int dx = o % w - h, dy = o / w - h, x = X + dx, y = Y + dy;
   if (x < 0 || y < 0 || x >= n || y >= n) return false;
   *J = y * n + x;
   return true;
 }
 
-__device__ __forceinline__ float3 stencil_apply(const float4* A, int I, int o, float3 v) {
-  const float4* b = A + (size_t(I) * kMgStencil + o) * 3;
+// Block (I, o) of a coarse level's f32 stencil (w2 = w * w offsets per row) times v.
+__device__ __forceinline__ float3 stencil_apply(const float4* A, int w2, int I, int o, float3 v) {
+  const float4* b = A + (size_t(I) * w2 + o) * 3;
   const float4 u = b[0], w = b[1], t = b[2];
   const float m[9] = {u.x, u.y, u.z, u.w, w.x, w.y, w.z, w.w, t.x};
   return mul(m, v);
@@ -158,18 +160,27 @@ int restrict_grid(int coarse_rows) { return (coarse_rows + kRestrictRows - 1) / 
 // A_{l+1}[I][o] = sum_{i in supp I} sum_{j} w(i, I) A_l(i, j) w(j, J), J = I + offset(o); f64 sums.
 // One warp per coarse row: the warp first stages the nine fine support rows' entries (column, weight, block) in
 // shared memory, then lane o < 25 sums the entries landing on offset o, in entry order (deterministic).
-constexpr int kGalerkinWarps = 2;                 // 2 x 225 x 88 B of staged entries per CTA
-constexpr int kGalerkinEntries = 9 * kMgStencil;  // a row couples within 2 vertices per axis: <= 25 blocks
-
+// kSrcW: 0 for the fine BSR level (<= 25 blocks per row), else the source stencil width (5 or 7). The staged
+// entries of one warp take 9 x 25 x 88 B (2 warps per CTA) or 9 x 49 x 88 B (7 x 7 source: 1 warp per CTA).
 struct GalerkinEntry {
   double m[9];
   double w;
   int jx, jy;  // the fine column's grid coordinates (jx < 0: outside the grid)
 };
 
-template <bool kSrcBsr>
-__global__ void __launch_bounds__(32 * kGalerkinWarps) galerkin_kernel(MgFine fine, MgLevel src, MgLevel dst,
-                                                                         int* error) {
+template <int kSrcW>
+struct GalerkinShape {
+  static constexpr int kEntries = 9 * (kSrcW == 7 ? kMgStencilWide : kMgStencil);
+  static constexpr int kWarps = kSrcW == 7 ? 1 : 2;
+};
+
+template <int kSrcW>
+__global__ void __launch_bounds__(32 * GalerkinShape<kSrcW>::kWarps) galerkin_kernel(MgFine fine, MgLevel src,
+                                                                                       MgLevel dst, int* error) {
+  constexpr bool kSrcBsr = kSrcW == 0;
+  constexpr int kGalerkinWarps = GalerkinShape<kSrcW>::kWarps;
+  constexpr int kGalerkinEntries = GalerkinShape<kSrcW>::kEntries;
+  constexpr int kSrcW2 = kSrcW * kSrcW;
   __shared__ GalerkinEntry list[kGalerkinWarps][kGalerkinEntries];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int I = blockIdx.x * kGalerkinWarps + warp;
@@ -186,7 +197,7 @@ __global__ void __launch_bounds__(32 * kGalerkinWarps) galerkin_kernel(MgFine fi
         first = fine.row_ptr[i];
         len = fine.row_ptr[i + 1] - first;
       } else {
-        len = kMgStencil;
+        len = kSrcW2;
       }
     }
   }
@@ -221,7 +232,7 @@ __global__ void __launch_bounds__(32 * kGalerkinWarps) galerkin_kernel(MgFine fi
         for (int e = 0; e < 9; ++e) E.m[e] = m[e];
       } else {
         int j;
-        const bool in = stencil_neighbour(nf, si % nf, si / nf, t, &j);
+        const bool in = stencil_neighbour(nf, kSrcW, si % nf, si / nf, t, &j);
         E.jx = in ? j % nf : -1;
         E.jy = in ? j / nf : -1;
 #pragma unroll
@@ -235,7 +246,7 @@ __global__ void __launch_bounds__(32 * kGalerkinWarps) galerkin_kernel(MgFine fi
 #pragma unroll
     for (int e = 0; e < 9; ++e) acc[e] = 0.0;
     int J;
-    if (stencil_neighbour(nc, X, Y, lane, &J)) {
+    if (stencil_neighbour(nc, 5, X, Y, lane, &J)) {
       const int JX = J % nc, JY = J / nc;
       for (int t = 0; t < total; ++t) {
         const GalerkinEntry& E = L[t];
@@ -285,13 +296,183 @@ __global__ void jacobi_smoother_kernel(MgFine fine, MgLevel lv, double omega) {
 #pragma unroll
     for (int e = 0; e < 9; ++e) m[e] = f[e];
   } else {
+    const int centre = (lv.w * lv.w - 1) / 2;
 #pragma unroll
-    for (int e = 0; e < 9; ++e) m[e] = lv.A64[(12 * 9 + e) * lv.rows + i];
+    for (int e = 0; e < 9; ++e) m[e] = lv.A64[(centre * 9 + e) * lv.rows + i];
   }
   float s[9];
   inverse3(m, omega, s);
 #pragma unroll
   for (int e = 0; e < 9; ++e) lv.S[e * lv.rows + i] = s[e];
+}
+
+// Sp = omega_P D^{-1} for the smoothed prolongation. S0 holds `scale` D^{-1} when this runs (scale 1 before the
+// power method scales the smoothers; a fixed damping omega otherwise). omega_P = kMgProlongC / lambda with
+// lambda = 2 / (1.1 omega_0 (1 + 1/30)), the power-method estimate of lambda_max(D^{-1} A) behind the level-0
+// damping omega_0 (the fixed omega when `fixed`): Sp = kMgProlongC * 1.1 * (1 + 1/30) / 2 * omega_0 / scale * S0.
+__global__ void sp_kernel(int count, const float* S0, const float* omega, int fixed, float* Sp) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  const float c = kMgProlongC * 1.1f * (1.0f + 1.0f / 30.0f) * 0.5f;
+  Sp[t] = (fixed ? c : c * omega[0]) * S0[t];
+}
+
+// Level 1 under the smoothed prolongation P_0 = (I - Sp A) P (mg.h), for coarse row I at fine vertex c = 2I:
+//   B_i = P_0[i, I] = P(i, I) Id - Sp_i sum_k A_ik P(k, I)     fine rows i within 3 of c (P(k, I) != 0 within 1)
+//   W_j = sum_i A_ji B_i                                      within 5
+//   Z_k = sum_j A_kj Sp_j W_j,  V_k = W_k - Z_k                within 7
+//   A_1[I, J] = sum_k P(k, J) V_k^T                           J within 3 of I (7 x 7)
+// which is P_0^T A P_0 for a symmetric A (A_ij = A_ji^T) and symmetric Sp blocks: sum_i P_0[i,I]^T A_ij = W_j^T and
+// sum_j W_j^T P_0[j, J] = sum_k P(k, J) (W_k - Z_k)^T. The ring J - I = 4, the only part dropped, holds products of
+// the weak axial hinge couplings (~1e-12 of the largest entry). One CTA per coarse row, the three windows in shared
+// memory in f64 (37 KB), 8 lanes per fine row and 4 rows per warp; sums in a fixed order (deterministic).
+constexpr int kGsWarps = 8;
+__device__ __forceinline__ void reduce8(double v[9]) {
+#pragma unroll
+  for (int o = 4; o; o >>= 1)
+#pragma unroll
+    for (int e = 0; e < 9; ++e) v[e] += __shfl_xor_sync(0xffffffffu, v[e], o);
+}
+
+__global__ void __launch_bounds__(32 * kGsWarps, 3) galerkin_smoothed_kernel(MgFine fine, const float* Sp, MgLevel dst) {
+  __shared__ double sB[49][9], sW[121][9], sY[121][9], sV[225][9];
+  const int I = blockIdx.x;
+  const int nc = dst.n, nf = fine.n, R = fine.R;
+  const int X = I % nc, Y = I / nc, cx = 2 * X, cy = 2 * Y;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, sub = lane >> 3, l8 = lane & 7;
+  // fine row of window index w (width ww, radius ww / 2) around c; -1 outside the grid
+  auto window_row = [&](int w, int ww) {
+    const int h = ww >> 1, fx = cx + w % ww - h, fy = cy + w / ww - h;
+    return (fx >= 0 && fy >= 0 && fx < nf && fy < nf) ? fy * nf + fx : -1;
+  };
+  // window index of fine column j in the window of width ww around c; -1 outside it
+  auto window_of = [&](int j, int ww) {
+    const int h = ww >> 1, dx = j % nf - cx + h, dy = j / nf - cy + h;
+    return (dx >= 0 && dy >= 0 && dx < ww && dy < ww) ? dy * ww + dx : -1;
+  };
+  auto sp_block = [&](int i, double m[9]) {
+#pragma unroll
+    for (int e = 0; e < 9; ++e) m[e] = Sp[e * R + i];
+  };
+  // Stage 1: B over the 7 x 7 window.
+  for (int base = warp * 4; base < 49; base += kGsWarps * 4) {
+    const int w = base + sub;
+    const int i = w < 49 ? window_row(w, 7) : -1;
+    double acc[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) acc[e] = 0.0;
+    if (i >= 0) {
+      for (int k = fine.row_ptr[i] + l8; k < fine.row_ptr[i + 1]; k += 8) {
+        const int j = fine.col_idx[k];
+        const double p = w1d(j % nf, X) * w1d(j / nf, Y);
+        if (p == 0.0) continue;
+        float m[9];
+        load_block(fine.A, k, m);
+#pragma unroll
+        for (int e = 0; e < 9; ++e) acc[e] += p * m[e];
+      }
+    }
+    reduce8(acc);
+    if (w < 49 && l8 == 0) {
+      if (i < 0) {
+#pragma unroll
+        for (int e = 0; e < 9; ++e) sB[w][e] = 0.0;
+      } else {
+        double sp[9];
+        sp_block(i, sp);
+        const double p = w1d(i % nf, X) * w1d(i / nf, Y);
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+          for (int b = 0; b < 3; ++b)
+            sB[w][3 * a + b] = (a == b ? p : 0.0) -
+                               (sp[3 * a] * acc[b] + sp[3 * a + 1] * acc[3 + b] + sp[3 * a + 2] * acc[6 + b]);
+      }
+    }
+  }
+  __syncthreads();
+  // Stage 2: W = A B over the 11 x 11 window, Y = Sp W.
+  for (int base = warp * 4; base < 121; base += kGsWarps * 4) {
+    const int w = base + sub;
+    const int j = w < 121 ? window_row(w, 11) : -1;
+    double acc[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) acc[e] = 0.0;
+    if (j >= 0) {
+      for (int k = fine.row_ptr[j] + l8; k < fine.row_ptr[j + 1]; k += 8) {
+        const int wb = window_of(fine.col_idx[k], 7);
+        if (wb < 0) continue;
+        float m[9];
+        load_block(fine.A, k, m);
+        const double* b = sB[wb];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+            acc[3 * a + c] += m[3 * a] * b[c] + m[3 * a + 1] * b[3 + c] + m[3 * a + 2] * b[6 + c];
+      }
+    }
+    reduce8(acc);
+    if (w < 121 && l8 == 0) {
+      double sp[9];
+      if (j >= 0) sp_block(j, sp);
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          sW[w][3 * a + c] = j >= 0 ? acc[3 * a + c] : 0.0;
+          sY[w][3 * a + c] = j >= 0 ? sp[3 * a] * acc[c] + sp[3 * a + 1] * acc[3 + c] + sp[3 * a + 2] * acc[6 + c] : 0.0;
+        }
+    }
+  }
+  __syncthreads();
+  // Stage 3: V = W - A Y over the 15 x 15 window.
+  for (int base = warp * 4; base < 225; base += kGsWarps * 4) {
+    const int w = base + sub;
+    const int r = w < 225 ? window_row(w, 15) : -1;
+    double acc[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) acc[e] = 0.0;
+    if (r >= 0) {
+      for (int k = fine.row_ptr[r] + l8; k < fine.row_ptr[r + 1]; k += 8) {
+        const int wy = window_of(fine.col_idx[k], 11);
+        if (wy < 0) continue;
+        float m[9];
+        load_block(fine.A, k, m);
+        const double* b = sY[wy];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+            acc[3 * a + c] += m[3 * a] * b[c] + m[3 * a + 1] * b[3 + c] + m[3 * a + 2] * b[6 + c];
+      }
+    }
+    reduce8(acc);
+    if (w < 225 && l8 == 0) {
+      const int ww = r >= 0 ? window_of(r, 11) : -1;
+#pragma unroll
+      for (int e = 0; e < 9; ++e) sV[w][e] = r < 0 ? 0.0 : (ww >= 0 ? sW[ww][e] : 0.0) - acc[e];
+    }
+  }
+  __syncthreads();
+  // A_1[I, J] = sum_k P(k, J) V_k^T, k the 3 x 3 fine vertices around 2J (all inside the 15 x 15 window).
+  for (int t = threadIdx.x; t < kMgStencilWide * 9; t += blockDim.x) {
+    const int o = t / 9, e = t % 9, a = e / 3, b = e % 3;
+    const int JX = X + o % 7 - 3, JY = Y + o / 7 - 3;
+    double v = 0.0;
+    if (JX >= 0 && JY >= 0 && JX < nc && JY < nc) {
+      for (int q = 0; q < 9; ++q) {
+        const int kx = 2 * JX + q % 3 - 1, ky = 2 * JY + q / 3 - 1;
+        if (kx < 0 || ky < 0 || kx >= nf || ky >= nf) continue;
+        const double p = (q % 3 != 1 ? 0.5 : 1.0) * (q / 3 != 1 ? 0.5 : 1.0);
+        v += p * sV[(ky - cy + 7) * 15 + (kx - cx + 7)][3 * b + a];
+      }
+    }
+    dst.A64[(o * 9 + e) * dst.rows + I] = v;
+    float* b32 = reinterpret_cast<float*>(dst.A + (size_t(I) * kMgStencilWide + o) * 3);
+    b32[e] = float(v);
+    if (e < 3) b32[9 + e] = 0.0f;
+  }
 }
 
 // Dense inverse of the coarsest operator by Gauss-Jordan elimination with partial pivoting (implicit row
@@ -309,10 +490,11 @@ __global__ void __launch_bounds__(1024) coarse_inverse_kernel(MgLevel lv, float*
   for (int t = threadIdx.x; t < m * w; t += blockDim.x) M[t] = 0.0;
   for (int t = threadIdx.x; t < m; t += blockDim.x) s_used[t] = 0;
   __syncthreads();
-  for (int t = threadIdx.x; t < lv.rows * kMgStencil; t += blockDim.x) {
-    const int I = t / kMgStencil, o = t % kMgStencil;
+  const int w2 = lv.w * lv.w;
+  for (int t = threadIdx.x; t < lv.rows * w2; t += blockDim.x) {
+    const int I = t / w2, o = t % w2;
     int J;
-    if (!stencil_neighbour(n, I % n, I / n, o, &J)) continue;
+    if (!stencil_neighbour(n, lv.w, I % n, I / n, o, &J)) continue;
     for (int e = 0; e < 9; ++e) M[(3 * I + e / 3) * w + 3 * J + e % 3] = lv.A64[(o * 9 + e) * lv.rows + I];
   }
   for (int t = threadIdx.x; t < m; t += blockDim.x) M[t * w + m + t] = 1.0;
@@ -384,35 +566,48 @@ __device__ __forceinline__ float3 warp_sum3(float3 v) {
   return v;
 }
 
+// The flexible PCG's stopping test at the start of an iteration (the first kernel of its V-cycle): the residual
+// norm from the update kernel's per-CTA partials against the tolerance, non-finite values, the iteration limit
+// and, at the end of each stall window, a residual that fell by less than 10 %. Every CTA computes the same sums
+// and takes the same decision; CTA 0 records it. Returns true when the solve has ended.
+__device__ bool pcg_stop(MgState* st, const float* rr_partial, int rr_count) {
+  if (st->done) return true;
+  const float rr = sum_partials(rr_partial, rr_count);
+  const int it = st->iterations;
+  const float rr0 = it == 0 ? rr : st->rr0;
+  const bool window_end = it > 0 && st->stall_window > 0 && it % st->stall_window == 0;
+  const int window = st->stall_window > 0 ? it / st->stall_window : 0;
+  int status = kStatusRunning;
+  if (rr <= rr0 * st->tol2) status = kStatusConverged;
+  else if (!isfinite(rr)) status = kStatusBreakdown;
+  else if (it >= st->max_iterations) status = kStatusLimit;
+  else if (window_end && !(rr <= 0.81f * st->stall_rr[(window - 1) & 1])) status = kStatusStalled;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->rr = rr;
+    if (it == 0) st->rr0 = rr;
+    if (it == 0 || window_end) st->stall_rr[window & 1] = rr;
+    if (status != kStatusRunning) {
+      st->status = status;
+      st->done = 1;
+    }
+  }
+  return status != kStatusRunning;
+}
+
 // r_{l+1} = P^T (r_l - A_l z_l), z_{l+1} = S_{l+1} r_{l+1}: one warp per coarse row; lanes 3s .. 3s + 2 take
-// the 9 fine support rows s (their blocks or stencil offsets interleaved), lanes 27..31 idle.
-// The level-0 restriction of a flexible PCG iteration first tests convergence, the limit and a stall.
-template <bool kSrcBsr, bool kCheck>
+// the 9 fine support rows s (their blocks or stencil offsets interleaved), lanes 27..31 idle. kSrcW: 0 for the fine
+// level (BSR), else the source level's stencil width. Under the smoothed prolongation the fine restriction runs
+// with src.r = t and src.z = Sp t (P_0^T t = P^T (t - A Sp t)).
+// The level-0 restriction of a flexible PCG iteration first tests convergence, the limit and a stall (kCheck).
+template <int kSrcW, bool kCheck>
 __global__ void __launch_bounds__(kRestrictThreads) restrict_kernel(RestrictArgs a) {
+  constexpr bool kSrcBsr = kSrcW == 0;
+  constexpr int kSrcW2 = kSrcW * kSrcW;
   pdl_enter();
   if (kCheck) {
-    MgState* st = a.state;
-    if (st->done) return;
-    const float rr = sum_partials(a.rr_partial, a.rr_count);
-    const int it = st->iterations;
-    const float rr0 = it == 0 ? rr : st->rr0;
-    const bool window_end = it > 0 && st->stall_window > 0 && it % st->stall_window == 0;
-    const int window = st->stall_window > 0 ? it / st->stall_window : 0;
-    int status = kStatusRunning;
-    if (rr <= rr0 * st->tol2) status = kStatusConverged;
-    else if (!isfinite(rr)) status = kStatusBreakdown;
-    else if (it >= st->max_iterations) status = kStatusLimit;
-    else if (window_end && !(rr <= 0.81f * st->stall_rr[(window - 1) & 1])) status = kStatusStalled;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-      st->rr = rr;
-      if (it == 0) st->rr0 = rr;
-      if (it == 0 || window_end) st->stall_rr[window & 1] = rr;
-      if (status != kStatusRunning) {
-        st->status = status;
-        st->done = 1;
-      }
-    }
-    if (status != kStatusRunning) return;
+    if (pcg_stop(a.state, a.rr_partial, a.rr_count)) return;
+  } else if (a.state && a.state->done) {
+    return;
   }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int I = blockIdx.x * kRestrictRows + warp;
@@ -439,11 +634,11 @@ __global__ void __launch_bounds__(kRestrictThreads) restrict_kernel(RestrictArgs
         }
       } else {
 #pragma unroll
-        for (int t = 0; t < 9; ++t) {
+        for (int t = 0; t < (kSrcW2 + 2) / 3; ++t) {
           const int o = k3 + 3 * t;
           int j;
-          if (o < kMgStencil && stencil_neighbour(nf, fx, fy, o, &j))
-            acc = add3(acc, stencil_apply(a.src.A, i, o, f3(a.src.z[j])));
+          if (o < kSrcW2 && stencil_neighbour(nf, kSrcW, fx, fy, o, &j))
+            acc = add3(acc, stencil_apply(a.src.A, kSrcW2, i, o, f3(a.src.z[j])));
         }
       }
       const float w = (ax ? 0.5f : 1.0f) * (by ? 0.5f : 1.0f);
@@ -454,6 +649,86 @@ __global__ void __launch_bounds__(kRestrictThreads) restrict_kernel(RestrictArgs
   if (lane == 0 && I < a.dst.rows) {
     a.dst.r[I] = pack(t);
     if (!a.coarsest) a.dst.z[I] = pack(smooth(a.dst.S, a.dst.rows, I, t, false));
+  }
+}
+
+struct SmoothedArgs {
+  MgFine fine;
+  const float4* r;      // residual: fine right-hand side
+  const float4* z;      // pre-smoothed z_0
+  const float* Sp;      // omega_P D^{-1}
+  float4* t;            // out: r - A z_0
+  float4* u;            // out: Sp t
+  const float4* e1;     // level-1 correction (interp_smoothed_kernel)
+  int nc;               // level-1 columns
+  float4* y;            // out: z_0 + P_0 e_1
+  MgState* state;       // flexible PCG state (null: stand-alone V-cycle)
+  const float* rr_partial;
+  int rr_count;
+};
+
+// Fine step before the smoothed restriction: t = r - A z_0, u = Sp t; inside flexible PCG it first takes the
+// iteration's stopping test (kCheck), which restrict_kernel takes without the smoothed prolongation.
+template <bool kCheck>
+__global__ void __launch_bounds__(kRowThreads) residual_smoothed_kernel(SmoothedArgs a) {
+  pdl_enter();
+  if (kCheck) {
+    if (pcg_stop(a.state, a.rr_partial, a.rr_count)) return;
+  } else if (a.state && a.state->done) {
+    return;
+  }
+  const int lane = threadIdx.x % kLanes;
+  const int i = blockIdx.x * (kRowThreads / kLanes) + threadIdx.x / kLanes;
+  const bool active = i < a.fine.R;
+  float3 acc = make_float3(0.f, 0.f, 0.f);
+  if (active) {  // <= 25 blocks per row: <= 4 per lane, column indices fetched first
+    const int k0 = a.fine.row_ptr[i] + lane, k1 = a.fine.row_ptr[i + 1];
+    int jj[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) jj[t] = k0 + kLanes * t < k1 ? a.fine.col_idx[k0 + kLanes * t] : -1;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      if (jj[t] < 0) continue;
+      float m[9];
+      load_block(a.fine.A, k0 + kLanes * t, m);
+      acc = add3(acc, mul(m, f3(a.z[jj[t]])));
+    }
+  }
+  acc = group_sum(acc);
+  if (active && lane == 0) {
+    const float3 t = sub3(f3(a.r[i]), acc);
+    a.t[i] = pack(t);
+    a.u[i] = pack(smooth(a.Sp, a.fine.R, i, t, false));
+  }
+}
+
+// Smoothed prolongation of the level-1 correction: v = P e_1 (bilinear), y = z_0 + v - Sp A v.
+__global__ void __launch_bounds__(kRowThreads) interp_smoothed_kernel(SmoothedArgs a) {
+  pdl_enter();
+  if (a.state && a.state->done) return;
+  const int lane = threadIdx.x % kLanes;
+  const int i = blockIdx.x * (kRowThreads / kLanes) + threadIdx.x / kLanes;
+  const int n = a.fine.n;
+  const bool active = i < a.fine.R;
+  float3 acc = make_float3(0.f, 0.f, 0.f);
+  if (active) {
+    const int k0 = a.fine.row_ptr[i] + lane, k1 = a.fine.row_ptr[i + 1];
+    int jj[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) jj[t] = k0 + kLanes * t < k1 ? a.fine.col_idx[k0 + kLanes * t] : -1;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      if (jj[t] < 0) continue;
+      const int j = jj[t];
+      float m[9];
+      load_block(a.fine.A, k0 + kLanes * t, m);
+      acc = add3(acc, mul(m, interpolate(a.e1, a.nc, j % n, j / n)));
+    }
+  }
+  acc = group_sum(acc);
+  if (active && lane == 0) {
+    const float3 v = interpolate(a.e1, a.nc, i % n, i / n);
+    a.y[i] = pack(sub3(add3(f3(a.z[i]), v), smooth(a.Sp, a.fine.R, i, acc, false)));
   }
 }
 
@@ -489,10 +764,12 @@ __global__ void __launch_bounds__(1024) tail_kernel(MgLevel T, MgLevel C, const 
   __shared__ float rc_s[3 * kMgCoarsestRowsMax], ec_s[3 * kMgCoarsestRowsMax];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, warps = blockDim.x >> 5;
   const int n = T.n, nc = C.n, m = 3 * C.rows;
+  const int w2 = T.w * T.w;
   for (int i = warp; i < T.rows; i += warps) {
     float3 acc = make_float3(0.f, 0.f, 0.f);
     int j;
-    if (lane < kMgStencil && stencil_neighbour(n, i % n, i / n, lane, &j)) acc = stencil_apply(T.A, i, lane, f3(T.z[j]));
+    for (int o = lane; o < w2; o += 32)
+      if (stencil_neighbour(n, T.w, i % n, i / n, o, &j)) acc = add3(acc, stencil_apply(T.A, w2, i, o, f3(T.z[j])));
     acc = warp_sum3(acc);
     if (lane == 0) t_s[i] = sub3(f3(T.r[i]), acc);
   }
@@ -534,7 +811,8 @@ __global__ void __launch_bounds__(1024) tail_kernel(MgLevel T, MgLevel C, const 
   for (int i = warp; i < T.rows; i += warps) {
     float3 acc = make_float3(0.f, 0.f, 0.f);
     int j;
-    if (lane < kMgStencil && stencil_neighbour(n, i % n, i / n, lane, &j)) acc = stencil_apply(T.A, i, lane, y_s[j]);
+    for (int o = lane; o < w2; o += 32)
+      if (stencil_neighbour(n, T.w, i % n, i / n, o, &j)) acc = add3(acc, stencil_apply(T.A, w2, i, o, y_s[j]));
     acc = warp_sum3(acc);
     if (lane == 0) T.e[i] = pack(add3(y_s[i], smooth(T.S, T.rows, i, sub3(f3(T.r[i]), acc), true)));
   }
@@ -544,6 +822,7 @@ struct ProlongArgs {
   MgFine fine;       // level-0 operator (kFine)
   MgLevel lv;        // level l: r, z (pre-smoothed), S, A; writes e
   MgLevel coarse;    // level l + 1: e
+  const float4* y;   // kY: z_0 + P_0 e_1 at every fine row
   const MgState* state;
   // level 0 only: partial dots of the new z with the current and previous residuals
   const float4* r_prev;
@@ -551,15 +830,23 @@ struct ProlongArgs {
   float* zrp_partial;
 };
 
-// y = z_l + P e_{l+1};  e_l = y + S^T (r_l - A_l y), y at the neighbours interpolated on the fly.
-template <bool kFine>
+// y = z_l + P e_{l+1};  e_l = y + S^T (r_l - A_l y), y at the neighbours interpolated on the fly. kW: 0 for the
+// fine level (BSR), else the level's stencil width. kY (fine level under the smoothed prolongation): y was formed
+// by interp_smoothed_kernel and is read from a.y.
+template <int kW, bool kY>
 __global__ void __launch_bounds__(kRowThreads) prolong_kernel(ProlongArgs a) {
+  constexpr bool kFine = kW == 0;
+  constexpr int kW2 = kW * kW;
   pdl_enter();
   if (a.state && a.state->done) return;
   const int lane = threadIdx.x % kLanes;
   const int i = blockIdx.x * (kRowThreads / kLanes) + threadIdx.x / kLanes;
   const int n = a.lv.n, nc = a.coarse.n;
   const bool active = i < a.lv.rows;
+  auto y_at = [&](int j) -> float3 {
+    if (kY) return f3(a.y[j]);
+    return add3(f3(a.lv.z[j]), interpolate(a.coarse.e, nc, j % n, j / n));
+  };
   float3 acc = make_float3(0.f, 0.f, 0.f);
   if (active) {
     if (kFine) {  // <= 25 blocks per row: <= 4 per lane, column indices fetched first
@@ -570,8 +857,7 @@ __global__ void __launch_bounds__(kRowThreads) prolong_kernel(ProlongArgs a) {
 #pragma unroll
       for (int t = 0; t < 4; ++t) {
         if (jj[t] < 0) continue;
-        const int j = jj[t];
-        const float3 y = add3(f3(a.lv.z[j]), interpolate(a.coarse.e, nc, j % n, j / n));
+        const float3 y = y_at(jj[t]);
         float m[9];
         load_block(a.fine.A, k0 + kLanes * t, m);
         acc = add3(acc, mul(m, y));
@@ -579,12 +865,11 @@ __global__ void __launch_bounds__(kRowThreads) prolong_kernel(ProlongArgs a) {
     } else {
       const int X = i % n, Y = i / n;
 #pragma unroll
-      for (int t = 0; t < 4; ++t) {
+      for (int t = 0; t < (kW2 + kLanes - 1) / kLanes; ++t) {
         const int o = lane + kLanes * t;
         int j;
-        if (o >= kMgStencil || !stencil_neighbour(n, X, Y, o, &j)) continue;
-        const float3 y = add3(f3(a.lv.z[j]), interpolate(a.coarse.e, nc, j % n, j / n));
-        acc = add3(acc, stencil_apply(a.lv.A, i, o, y));
+        if (o >= kW2 || !stencil_neighbour(n, kW, X, Y, o, &j)) continue;
+        acc = add3(acc, stencil_apply(a.lv.A, kW2, i, o, y_at(j)));
       }
     }
   }
@@ -592,7 +877,7 @@ __global__ void __launch_bounds__(kRowThreads) prolong_kernel(ProlongArgs a) {
   float zr = 0.0f, zrp = 0.0f;
   if (active && lane == 0) {
     const float3 r = f3(a.lv.r[i]);
-    const float3 y = add3(f3(a.lv.z[i]), interpolate(a.coarse.e, nc, i % n, i / n));
+    const float3 y = y_at(i);
     const float3 e = add3(y, smooth(a.lv.S, a.lv.rows, i, sub3(r, acc), true));
     a.lv.e[i] = pack(e);
     if (kFine && a.zr_partial) {  // inside flexible PCG only (a stand-alone cycle has no r_prev)
@@ -782,6 +1067,27 @@ MgLevel level0(const MgDevice& d, int parity) {
 cudaError_t launch_cycle(const MgDevice& d, int parity, bool in_pcg, bool pdl, cudaStream_t s, int* launches) {
   const int L = d.levels;
   MgState* st = in_pcg ? d.state : nullptr;
+  const bool smoothed = d.smoothed != 0;
+  SmoothedArgs sa{};
+  sa.fine = d.fine;
+  sa.r = d.r[parity];
+  sa.z = d.lv[0].z;
+  sa.Sp = d.Sp;
+  sa.t = d.t;
+  sa.u = d.u;
+  sa.e1 = d.lv[1].e;
+  sa.nc = d.lv[1].n;
+  sa.y = d.y;
+  sa.state = st;
+  sa.rr_partial = d.partial + kPartRr * kMgPartials;
+  sa.rr_count = update_grid(d.fine.R);
+  cudaError_t e;
+  if (smoothed) {  // t = r - A z_0, u = Sp t (and the stopping test inside flexible PCG)
+    e = in_pcg ? launch(residual_smoothed_kernel<true>, row_grid(d.fine.R), kRowThreads, s, pdl, sa)
+               : launch(residual_smoothed_kernel<false>, row_grid(d.fine.R), kRowThreads, s, pdl, sa);
+    if (e != cudaSuccess) return e;
+    ++*launches;
+  }
   // with three or more levels, the last two run in one CTA (tail_kernel: level L - 2 is a stencil level, n <= 9)
   const bool tail = L >= 3;
   const int last_restricted = tail ? L - 2 : L - 1;
@@ -789,23 +1095,27 @@ cudaError_t launch_cycle(const MgDevice& d, int parity, bool in_pcg, bool pdl, c
     RestrictArgs a{};
     a.fine = d.fine;
     a.src = l == 0 ? level0(d, parity) : d.lv[l];
+    if (l == 0 && smoothed) {
+      a.src.r = d.t;
+      a.src.z = d.u;
+    }
     a.dst = d.lv[l + 1];
     a.coarsest = l + 2 == L;
-    a.state = d.state;
+    a.state = st;
     a.rr_partial = d.partial + kPartRr * kMgPartials;
     a.rr_count = update_grid(d.fine.R);
     const int grid = restrict_grid(a.dst.rows);
-    cudaError_t e;
-    if (l == 0 && in_pcg) e = launch(restrict_kernel<true, true>, grid, kRestrictThreads, s, pdl, a);
-    else if (l == 0) e = launch(restrict_kernel<true, false>, grid, kRestrictThreads, s, pdl, a);
-    else e = launch(restrict_kernel<false, false>, grid, kRestrictThreads, s, pdl, a);
+    if (l == 0 && in_pcg && !smoothed) e = launch(restrict_kernel<0, true>, grid, kRestrictThreads, s, pdl, a);
+    else if (l == 0) e = launch(restrict_kernel<0, false>, grid, kRestrictThreads, s, pdl, a);
+    else if (a.src.w == 7) e = launch(restrict_kernel<7, false>, grid, kRestrictThreads, s, pdl, a);
+    else e = launch(restrict_kernel<5, false>, grid, kRestrictThreads, s, pdl, a);
     if (e != cudaSuccess) return e;
     ++*launches;
   }
-  cudaError_t e = tail ? launch(tail_kernel, 1, 1024, s, pdl, d.lv[L - 2], d.lv[L - 1], (const float*)d.coarse_inv,
-                                (const MgState*)st)
-                       : launch(coarse_solve_kernel, 1, 1024, s, pdl, d.lv[L - 1], (const float*)d.coarse_inv,
-                                (const MgState*)st);
+  e = tail ? launch(tail_kernel, 1, 1024, s, pdl, d.lv[L - 2], d.lv[L - 1], (const float*)d.coarse_inv,
+                    (const MgState*)st)
+           : launch(coarse_solve_kernel, 1, 1024, s, pdl, d.lv[L - 1], (const float*)d.coarse_inv,
+                    (const MgState*)st);
   if (e != cudaSuccess) return e;
   ++*launches;
   for (int l = last_restricted - 1; l >= 0; --l) {
@@ -813,6 +1123,7 @@ cudaError_t launch_cycle(const MgDevice& d, int parity, bool in_pcg, bool pdl, c
     a.fine = d.fine;
     a.lv = l == 0 ? level0(d, parity) : d.lv[l];
     a.coarse = d.lv[l + 1];
+    a.y = d.y;
     a.state = st;
     if (l == 0 && in_pcg) {
       a.r_prev = d.r[1 - parity];
@@ -820,8 +1131,17 @@ cudaError_t launch_cycle(const MgDevice& d, int parity, bool in_pcg, bool pdl, c
       a.zrp_partial = d.partial + kPartZrPrev * kMgPartials;
     }
     const int grid = row_grid(a.lv.rows);
-    e = l == 0 ? launch(prolong_kernel<true>, grid, kRowThreads, s, pdl, a)
-               : launch(prolong_kernel<false>, grid, kRowThreads, s, pdl, a);
+    if (l == 0 && smoothed) {  // y = z_0 + P_0 e_1, then the post-smoothing on y
+      if ((e = launch(interp_smoothed_kernel, grid, kRowThreads, s, pdl, sa)) != cudaSuccess) return e;
+      ++*launches;
+      e = launch(prolong_kernel<0, true>, grid, kRowThreads, s, pdl, a);
+    } else if (l == 0) {
+      e = launch(prolong_kernel<0, false>, grid, kRowThreads, s, pdl, a);
+    } else if (a.lv.w == 7) {
+      e = launch(prolong_kernel<7, false>, grid, kRowThreads, s, pdl, a);
+    } else {
+      e = launch(prolong_kernel<5, false>, grid, kRowThreads, s, pdl, a);
+    }
     if (e != cudaSuccess) return e;
     ++*launches;
   }
@@ -894,10 +1214,10 @@ __global__ void __launch_bounds__(kRowThreads) power_kernel(PowerArgs a) {
         acc = add3(acc, mul(m, value(a.fine.col_idx[k])));
       }
     } else {
-      const int n = lv.n, X = i % n, Y = i / n;
-      for (int o = lane; o < kMgStencil; o += kLanes) {
+      const int n = lv.n, X = i % n, Y = i / n, w2 = lv.w * lv.w;
+      for (int o = lane; o < w2; o += kLanes) {
         int j;
-        if (stencil_neighbour(n, X, Y, o, &j)) acc = add3(acc, stencil_apply(lv.A, i, o, value(j)));
+        if (stencil_neighbour(n, lv.w, X, Y, o, &j)) acc = add3(acc, stencil_apply(lv.A, w2, i, o, value(j)));
       }
     }
   }
@@ -935,41 +1255,70 @@ __global__ void scale_smoother_kernel(float* S, int count, const float* omega) {
 
 }  // namespace
 
+namespace {
+
+// The power method on levels [first, end) (S holds D^{-1} there), its omega_l into d.omega.
+cudaError_t power_method(const MgDevice& d, int first, int end, cudaStream_t s) {
+  PowerArgs pa{};
+  pa.fine = d.fine;
+  for (int l = 0; l < d.levels; ++l) pa.lv[l] = d.lv[l];
+  pa.first = first;
+  pa.end = end;
+  pa.cta_start[first] = 0;
+  for (int l = first; l < end; ++l) pa.cta_start[l + 1] = pa.cta_start[l] + row_grid(d.lv[l].rows);
+  pa.partial = d.partial;
+  const int grid = pa.cta_start[end];
+  if (grid > kMgPartials) return cudaErrorInvalidValue;
+  for (int k = 0; k < kMgPowerSteps; ++k) {
+    pa.parity = k & 1;
+    pa.start = k == 0;
+    power_kernel<<<grid, kRowThreads, 0, s>>>(pa);
+  }
+  pa.parity = (kMgPowerSteps - 1) & 1;
+  power_finish_kernel<<<1, 32, 0, s>>>(pa, d.omega);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
 cudaError_t mg_setup(const MgDevice& d, float omega, bool fine_smoother, bool reuse_omega, cudaStream_t s) {
   if (d.levels < 2) return cudaErrorInvalidValue;
   cudaError_t e;
   const int first = fine_smoother ? 0 : 1, end = d.levels - 1;  // smoothed levels
   const double fixed = omega > 0.0f ? omega : 1.0;              // D^{-1} alone before the power method
+  const bool spectral = omega <= 0.0f && first < end;
   if (fine_smoother) jacobi_smoother_kernel<true><<<(d.fine.R + 255) / 256, 256, 0, s>>>(d.fine, d.lv[0], fixed);
-  for (int l = 0; l + 1 < d.levels; ++l) {
-    const int grid = (d.lv[l + 1].rows + kGalerkinWarps - 1) / kGalerkinWarps;
-    if (l == 0) galerkin_kernel<true><<<grid, 32 * kGalerkinWarps, 0, s>>>(d.fine, d.lv[0], d.lv[1], d.error);
-    else galerkin_kernel<false><<<grid, 32 * kGalerkinWarps, 0, s>>>(d.fine, d.lv[l], d.lv[l + 1], d.error);
+  int l0 = 0;  // first level whose Galerkin product the bilinear loop below forms
+  if (d.smoothed) {
+    // The smoothed prolongation needs the level-0 spectral estimate before level 1 exists: power method on the
+    // fine level first, Sp from it, then the 7 x 7 level-1 product.
+    if (spectral && !reuse_omega && first == 0 && (e = power_method(d, 0, 1, s)) != cudaSuccess) return e;
+    const int count = 9 * d.fine.R;
+    sp_kernel<<<(count + 255) / 256, 256, 0, s>>>(count, d.lv[0].S, d.omega, omega > 0.0f ? 1 : 0, d.Sp);
+    galerkin_smoothed_kernel<<<d.lv[1].rows, 32 * kGsWarps, 0, s>>>(d.fine, d.Sp, d.lv[1]);
+    if (2 < d.levels) jacobi_smoother_kernel<false><<<(d.lv[1].rows + 255) / 256, 256, 0, s>>>(d.fine, d.lv[1], fixed);
+    l0 = 1;
+  }
+  for (int l = l0; l + 1 < d.levels; ++l) {
+    if (l == 0) {
+      const int grid = (d.lv[1].rows + GalerkinShape<0>::kWarps - 1) / GalerkinShape<0>::kWarps;
+      galerkin_kernel<0><<<grid, 32 * GalerkinShape<0>::kWarps, 0, s>>>(d.fine, d.lv[0], d.lv[1], d.error);
+    } else if (d.lv[l].w == 7) {
+      const int grid = (d.lv[l + 1].rows + GalerkinShape<7>::kWarps - 1) / GalerkinShape<7>::kWarps;
+      galerkin_kernel<7><<<grid, 32 * GalerkinShape<7>::kWarps, 0, s>>>(d.fine, d.lv[l], d.lv[l + 1], d.error);
+    } else {
+      const int grid = (d.lv[l + 1].rows + GalerkinShape<5>::kWarps - 1) / GalerkinShape<5>::kWarps;
+      galerkin_kernel<5><<<grid, 32 * GalerkinShape<5>::kWarps, 0, s>>>(d.fine, d.lv[l], d.lv[l + 1], d.error);
+    }
     if (l + 2 < d.levels) {
       const MgLevel& c = d.lv[l + 1];
       jacobi_smoother_kernel<false><<<(c.rows + 255) / 256, 256, 0, s>>>(d.fine, c, fixed);
     }
   }
-  if (omega <= 0.0f && first < end) {
-    PowerArgs pa{};
-    pa.fine = d.fine;
-    for (int l = 0; l < d.levels; ++l) pa.lv[l] = d.lv[l];
-    pa.first = first;
-    pa.end = end;
-    pa.cta_start[first] = 0;
-    for (int l = first; l < end; ++l) pa.cta_start[l + 1] = pa.cta_start[l] + row_grid(d.lv[l].rows);
-    pa.partial = d.partial;
-    const int grid = pa.cta_start[end];
-    if (grid > kMgPartials) return cudaErrorInvalidValue;
-    if (!reuse_omega) {
-      for (int k = 0; k < kMgPowerSteps; ++k) {
-        pa.parity = k & 1;
-        pa.start = k == 0;
-        power_kernel<<<grid, kRowThreads, 0, s>>>(pa);
-      }
-      pa.parity = (kMgPowerSteps - 1) & 1;
-      power_finish_kernel<<<1, 32, 0, s>>>(pa, d.omega);
-    }
+  if (spectral) {
+    // without the smoothed prolongation every smoothed level in one power method; with it, the rest
+    const int from = d.smoothed && first == 0 ? 1 : first;
+    if (!reuse_omega && from < end && (e = power_method(d, from, end, s)) != cudaSuccess) return e;
     for (int l = first; l < end; ++l) {
       const int count = 9 * d.lv[l].rows;
       scale_smoother_kernel<<<(count + 255) / 256, 256, 0, s>>>(d.lv[l].S, count, d.omega + l);

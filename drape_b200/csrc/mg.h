@@ -9,17 +9,25 @@
 // 5 x 5 stencil of 3x3 blocks (a fine coupling reaches 2 vertices away, a hinge's opposite vertices); the
 // coarsest level (n <= 5) is solved exactly through its dense inverse.
 //
-// Coarse stencil layouts, o = (dy + 2) * 5 + (dx + 2) the offset of column vertex J = I + (dx, dy), e = 3 * row +
-// col within the block, entries outside the grid zero:
+// Coarse stencil layouts, w the level's stencil width (5, or 7 for level 1 under the smoothed prolongation),
+// h = w / 2, o = (dy + h) * w + (dx + h) the offset of column vertex J = I + (dx, dy), e = 3 * row + col within the
+// block, entries outside the grid zero:
 //   A64[(o * 9 + e) * rows + I]        f64 master (the next Galerkin product, the coarsest inverse)
-//   A[(I * 25 + o) * 3 + q], q < 3     f32 copy read by the cycle: one 48-byte block per (row, offset) as three
+//   A[(I * w^2 + o) * 3 + q], q < 3    f32 copy read by the cycle: one 48-byte block per (row, offset) as three
 //                                      float4 (m00 m01 m02 m10 | m11 m12 m20 m21 | m22 0 0 0)
 // Smoother blocks (one 3x3 per row, any level): S[e * rows + I].
 //
 // One V-cycle z = M r (pre-smoothing S, post-smoothing S^T, so M is symmetric when S is symmetric or the post
 // step uses the transpose of the pre step):
-//   level l:  z_l = S_l r_l;  r_{l+1} = P^T (r_l - A_l z_l);  ...;  e_L = A_L^{-1} r_L;
-//             y_l = z_l + P e_{l+1};  e_l = y_l + S_l^T (r_l - A_l y_l).
+//   level l:  z_l = S_l r_l;  r_{l+1} = P_l^T (r_l - A_l z_l);  ...;  e_L = A_L^{-1} r_L;
+//             y_l = z_l + P_l e_{l+1};  e_l = y_l + S_l^T (r_l - A_l y_l).
+//
+// Smoothed prolongation (MgDevice::smoothed): from the fine level to level 1 the bilinear P is smoothed once,
+// P_0 = (I - omega_P D^{-1} A) P with omega_P = (4/3) / lambda, lambda the power-method estimate of
+// lambda_max(D^{-1} A) (the prolongation smoothing of smoothed aggregation: Vanek, Mandel and Brezina, Computing 56
+// (1996) 179-196). Level 1 = P_0^T A P_0 reaches four coarse steps; the ring at four is at rounding level (~1e-12 of
+// the largest entry) and level 1 keeps the 7 x 7 stencil. The cycle's fine steps become
+//   r_1 = P^T (t - A Sp t), t = r - A z_0, Sp = omega_P D^{-1};    y_0 = z_0 + v - Sp A v, v = P e_1.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -28,15 +36,18 @@
 namespace drape {
 
 constexpr int kMgMaxLevels = 10;
-constexpr int kMgStencil = 25;
+constexpr int kMgStencil = 25;         // 5 x 5 coarse stencil
+constexpr int kMgStencilWide = 49;     // 7 x 7: level 1 under the smoothed prolongation
+constexpr float kMgProlongC = 4.0f / 3.0f;  // omega_P = kMgProlongC / lambda
 constexpr int kMgCoarsestMax = 5;      // coarsen while n > 5 and n - 1 is even
 constexpr int kMgCoarsestRowsMax = 25; // dense coarse inverse of at most 75 x 75 (n <= 5)
 
 struct MgLevel {
   int n = 0, rows = 0;
+  int w = 5;              // stencil width of a coarse level (5 or 7)
   // coarse levels (l >= 1)
-  double* A64 = nullptr;  // [225][rows]
-  float4* A = nullptr;    // [rows][25][3] f32 blocks, 48 B each (see the layout above)
+  double* A64 = nullptr;  // [w^2 * 9][rows]
+  float4* A = nullptr;    // [rows][w^2][3] f32 blocks, 48 B each (see the layout above)
   // every level
   float* S = nullptr;     // smoother [9][rows]
   float4* r = nullptr;    // level right-hand side (level 0: the PCG residual, owned by the solver)
@@ -79,6 +90,12 @@ struct MgDevice {
   float* partial = nullptr;  // [4][kMgPartials]: zr, z.r_prev, pq, rr per CTA
   MgState* state = nullptr;
   int* error = nullptr;      // coarse factorisation found a zero pivot
+  // smoothed prolongation from the fine level (see above); null pointers: the bilinear P everywhere
+  int smoothed = 0;
+  float* Sp = nullptr;       // omega_P D^{-1}, [9][R]
+  float4* t = nullptr;       // fine residual after pre-smoothing, r - A z_0
+  float4* u = nullptr;       // Sp t
+  float4* y = nullptr;       // z_0 + P_0 e_1
 };
 
 constexpr int kMgRowsPerCta = 32;  // level-0 row kernels: 8 lanes per row, 256 threads

@@ -87,6 +87,10 @@ typedef struct {
                                   1: projected (clamped membrane stress, Gauss-Newton hinge): SPD up to the barrier */
   double smoother_omega;       /* multilevel: damping of the Jacobi smoothers; 0 (default): per level
                                   2 / (1.1 lambda (1 + 1/30)) from the power method on D^{-1} A (stable) */
+  int32_t prolongation;        /* multilevel fine-to-coarse prolongation: 0 bilinear; 1 (default) bilinear smoothed
+                                  once, (I - (4/3) lambda^{-1} D^{-1} A) P (smoothed aggregation's prolongation
+                                  smoothing; level 1 becomes a 7 x 7 stencil) */
+  int32_t pad_options;
 } drape_options;
 
 /* Outcome of drape_solve_equilibrium (gpu-result.json fields, run-e7.ts:100-106). */
@@ -255,10 +259,13 @@ drape_status drape_row_terms(drape_ctx* ctx, const double* x, const double* x_ha
 /* The multilevel preconditioner (no counterpart in the reference): z = M r, one V-cycle for the given f32 blocks
  * (NULL: the last assembled matrix) and rhs r (3R f64, rounded to f32); z is 3R f64. */
 drape_status drape_precondition(drape_ctx* ctx, const float* blocks, const double* r, double* z);
-/* Level `level` of the hierarchy for the current matrix: *columns = its grid columns, op (level >= 1, may be NULL)
- * the f64 Galerkin stencil [225][rows] (offset o = (dy + 2) * 5 + dx + 2, entry e = 3 * row + col), smoother
- * (may be NULL) the f32 blocks [9][rows]. DRAPE_E_ARG when the problem has no hierarchy or level is out of range. */
-drape_status drape_multilevel_view(drape_ctx* ctx, int32_t level, int32_t* columns, double* op, float* smoother);
+/* Level `level` of the hierarchy for the current matrix: *columns = its grid columns, *width (may be NULL) its
+ * stencil width w (5, or 7 for level 1 under the smoothed prolongation; 0 for the fine level), op (level >= 1, may
+ * be NULL) the f64 Galerkin stencil [w^2 * 9][rows] (offset o = (dy + w/2) * w + dx + w/2, entry e = 3 * row + col),
+ * smoother (may be NULL) the f32 blocks [9][rows]. DRAPE_E_ARG when the problem has no hierarchy or level is out of
+ * range. */
+drape_status drape_multilevel_view(drape_ctx* ctx, int32_t level, int32_t* columns, int32_t* width, double* op,
+                                   float* smoother);
 
 /* Timed stand-alone launches for the roofline: average device ms per launch of the BSR SpMV on the last
  * assembled matrix (lanes per row 4/8/16/32) and of the row assembly at the current state. */

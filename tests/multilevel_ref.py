@@ -145,23 +145,40 @@ def chebyshev_apply(A, Dinv, r, lo, hi, degree):
     return z
 
 
+def truncate_stencil(A, n, radius):
+    """A coarse operator on an n x n grid with every block coupling vertices more than `radius` grid steps apart
+    (in either axis) dropped."""
+    C = A.tocoo()
+    i, j = C.row // 3, C.col // 3
+    keep = (np.abs(i % n - j % n) <= radius) & (np.abs(i // n - j // n) <= radius)
+    return sp.csr_matrix((C.data[keep], (C.row[keep], C.col[keep])), shape=A.shape)
+
+
 class Hierarchy:
     """omega > 0: fixed damping on every level; omega = None: spectral_omega per level (the device default)."""
 
-    def __init__(self, A, n, omega=None, fine_smoother=None, smooth_prolongation=()):
-        """smooth_prolongation: levels whose prolongation is smoothed once (smoothed_prolongation; a candidate
-        coarse space, not the device's), () for the device's bilinear one everywhere."""
+    def __init__(self, A, n, omega=None, fine_smoother=None, smooth_prolongation=(), truncate=None):
+        """smooth_prolongation: levels whose prolongation is smoothed once (smoothed_prolongation), () for the
+        bilinear one everywhere. truncate: the coarse operator below a smoothed prolongation keeps only the
+        couplings within this many coarse steps (the device: smooth_prolongation=(0,), truncate=3, level 1 a 7 x 7
+        stencil); None keeps the whole product."""
         self.cols = level_columns(n)
         if len(self.cols) < 2:
             raise ValueError("grid cannot be coarsened")
         self.A = [A.tocsr()]
         self.P = []
+        self.width = [0]
         for l in range(len(self.cols) - 1):
             P = prolongation(self.cols[l])
-            if l in smooth_prolongation:
+            wide = l in smooth_prolongation
+            if wide:
                 P = smoothed_prolongation(self.A[-1], P, l)
             self.P.append(P)
-            self.A.append((P.T @ self.A[-1] @ P).tocsr())
+            C = (P.T @ self.A[-1] @ P).tocsr()
+            if wide and truncate is not None:
+                C = truncate_stencil(C, self.cols[l + 1], truncate)
+            self.A.append(C)
+            self.width.append(2 * truncate + 1 if wide and truncate is not None else 5)
         self.omega = [omega if omega else spectral_omega(Al, l) for l, Al in enumerate(self.A[:-1])]
         self.S = [jacobi_smoother(Al, w) for Al, w in zip(self.A[:-1], self.omega)]
         if fine_smoother is not None:
@@ -177,13 +194,16 @@ class Hierarchy:
         return y + block_apply(S, r - A @ y, transpose=True)
 
     def stencil(self, level):
-        """Level operator as the GPU's [225][rows] stencil array."""
+        """Level operator as the GPU's [w^2 * 9][rows] stencil array (w = self.width[level])."""
         n = self.cols[level]
         A = self.A[level]
         rows = n * n
-        out = np.zeros((25 * 9, rows))
+        w = self.width[level]
+        h = w // 2
+        offsets = [(dx, dy) for dy in range(-h, h + 1) for dx in range(-h, h + 1)]
+        out = np.zeros((w * w * 9, rows))
         Ad = A.tocsr()
-        for o, (dx, dy) in enumerate(STENCIL):
+        for o, (dx, dy) in enumerate(offsets):
             X, Y = np.meshgrid(np.arange(n), np.arange(n), indexing="xy")
             X, Y = X.ravel(), Y.ravel()
             ok = (X + dx >= 0) & (X + dx < n) & (Y + dy >= 0) & (Y + dy < n)
