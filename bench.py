@@ -156,7 +156,8 @@ def run_gpu(args):
 
     def options_for(name):
         return api.default_options(pcg_max_iterations=args.pcg_max, max_steps=args.max_steps,
-                                   equilibrium_absolute=args.absolute,
+                                   equilibrium_absolute=args.absolute, prolongation=args.prolongation,
+                                   forcing=args.forcing,
                                    preconditioner={"jacobi": 0, "multilevel": 1, "learned": 2}[name])
 
     net = api.Network.trained(device=local) if args.preconditioner == "learned" or args.compare == "all" else None
@@ -274,7 +275,8 @@ def run_gpu(args):
         "config": {"workload": f"sheet n{args.n} over sphere r=0.25 + ground plane y=-0.25, {PRECOND[args.preconditioner]}, "
                                f"PTC dt0=1e-3 s to |grad E_s|<={args.absolute:g} N", "columns": args.n, "rows": R,
                    "blocks": B, "seed": args.seed, "preconditioner": args.preconditioner,
-                   "tolerance_N": args.absolute, "parallelism": f"replicas{world}",
+                   "tolerance_N": args.absolute, "prolongation": ["bilinear", "smoothed"][args.prolongation],
+                   "parallelism": f"replicas{world}",
                    "l2": "flushed (512 MiB write) before every timed solve"},
         "solve": {"converged": last["reason"] == "tolerance", "reason": last["reason"],
                   "final_residual_N": last["final_residual"], "ptc_steps": last["ptc_steps"],
@@ -486,14 +488,15 @@ def probe(args):
     if args.probe == "solve":
         d = api.Drape.sheet(args.n, seed=args.seed, plane=bool(args.plane),
                             options=api.default_options(preconditioner=pre, equilibrium_absolute=args.absolute,
-                                                        time_budget_s=args.budget))
+                                                        time_budget_s=args.budget, prolongation=args.prolongation,
+                                                        forcing=args.forcing))
         if pre == 2:
             d.set_network(api.Network.trained())
         log = d.solve_equilibrium(check=False)
         if args.out:
             np.save(args.out, d.state)
-        keys = ("reason", "ptc_steps", "newton_iterations", "pcg_iterations", "fallbacks", "ms_pcg", "final_residual",
-                "device_seconds", "static_energy")
+        keys = ("reason", "ptc_steps", "newton_iterations", "pcg_iterations", "fallbacks", "ms_pcg", "ms_assembly",
+                "ms_other", "final_residual", "device_seconds", "static_energy", "kernel_launches")
         return {k: log[k] for k in keys}
     if args.probe == "spmv":
         parts, offset = [], 0
@@ -537,7 +540,7 @@ def probe(args):
     lib = api.load()
     out = {"probe": args.probe, "columns": args.n, "ptc_steps": args.probe_steps}
     if args.probe == "cycle":
-        d.set_options(api.default_options(preconditioner=1))
+        d.set_options(api.default_options(preconditioner=1, prolongation=args.prolongation))
         _, info = d.pcg(b, 1e-6, 2000, blocks=blocks)
         out["pcg"] = info
         lib.drape_time_multilevel.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]
@@ -579,6 +582,11 @@ def main():
                     help="--impl reference --full-solve: print the FULL_SOLVE entry (per-step times) of the solve")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--preconditioner", default="learned", choices=["jacobi", "multilevel", "learned"])
+    ap.add_argument("--forcing", type=int, default=0, choices=[0, 1],
+                    help="Newton direction tolerance: 0 fixed PCG rtol 1e-6, 1 Eisenstat-Walker (the reference GPU "
+                         "stage's forcingFor, e4_rules.rs:15-22)")
+    ap.add_argument("--prolongation", type=int, default=1, choices=[0, 1],
+                    help="multilevel fine-to-coarse prolongation: 0 bilinear, 1 smoothed once (default)")
     ap.add_argument("--compare", default="jacobi", choices=["none", "jacobi", "all"],
                     help="after the timed steps, one device-timed solve of the same workload with each other solver")
     ap.add_argument("--probe", default=None, choices=["cycle", "network", "spmv", "solve"],

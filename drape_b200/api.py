@@ -73,6 +73,15 @@ class ProblemView(ctypes.Structure):
     ]
 
 
+class TimeStepLog(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int32), ("status", ctypes.c_int32), ("pcg_iterations", ctypes.c_int32),
+                ("mu_retries", ctypes.c_int32), ("scale", ctypes.c_double), ("final_relative_residual", ctypes.c_double),
+                ("max_mu", ctypes.c_double), ("seconds", ctypes.c_double)]
+
+
+STEP_STATUS = {1: "converged", 2: "iteration_limit", 3: "line_search_failed", 5: "regularization_cap", 6: "non_finite"}
+
+
 class StepRecord(ctypes.Structure):
     _fields_ = [("step", ctypes.c_int32), ("inner", ctypes.c_int32), ("rejected", ctypes.c_int32),
                 ("pcg_iterations", ctypes.c_int32), ("h", ctypes.c_double), ("residual", ctypes.c_double),
@@ -127,6 +136,7 @@ def load():
     lib.drape_network_gradient.argtypes = [P, P, P, P, P, P, P, P]
     lib.drape_network_train.argtypes = [P, P, ctypes.c_int32, P, P, P, ctypes.c_int32, ctypes.c_double, P]
     lib.drape_multilevel_view.argtypes = [P, ctypes.c_int32, P, P, P, P]
+    lib.drape_time_step.argtypes = [P, ctypes.c_double, P, ctypes.c_double, ctypes.c_int32, P, P]
     lib.drape_energy_change.argtypes = [P, P, P, ctypes.c_double, P, ctypes.c_double, ctypes.c_int32, P]
     lib.drape_max_step.argtypes = [P, P, P, P]
     lib.drape_static_residual.argtypes = [P, P, P]
@@ -273,6 +283,18 @@ class Drape:
         out = log.as_dict()
         out["status"] = st
         return out
+
+    def time_step(self, h, velocity=None, tolerance=1e-8, max_iterations=30):
+        """One backward-Euler step (drape_time_step) from the current state with `velocity` (3V, None: at rest):
+        returns (new velocity, log dict); the context's state advances."""
+        v_out = np.zeros(3 * self.V)
+        log = TimeStepLog()
+        v = _f64(velocity)
+        self._check(self.lib.drape_time_step(self.h, ctypes.c_double(h), _ptr(v), ctypes.c_double(tolerance),
+                                             max_iterations, _ptr(v_out), ctypes.byref(log)))
+        d = {k: getattr(log, k) for k, _ in TimeStepLog._fields_}
+        d["status_name"] = STEP_STATUS.get(d["status"], "unknown")
+        return v_out, d
 
     def step_records(self):
         n = ctypes.c_int32()

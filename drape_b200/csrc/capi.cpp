@@ -263,6 +263,17 @@ drape_status drape_solve_equilibrium(drape_ctx* ctx, const double* start, double
   });
 }
 
+drape_status drape_time_step(drape_ctx* ctx, double h, const double* v, double tolerance, int32_t max_iterations,
+                             double* v_out, drape_time_step_log* log) {
+  return guarded(ctx, [&](drape::Context& c) {
+    if (!(h > 0) || !(tolerance > 0) || max_iterations < 1)
+      return fail(ctx, "drape_time_step: h and tolerance must be positive and max_iterations at least 1",
+                  DRAPE_E_ARG);
+    c.time_step(h, v, tolerance, max_iterations, v_out, log);
+    return DRAPE_OK;
+  });
+}
+
 drape_status drape_solve_batch(drape_ctx* const* ctxs, int32_t count, int32_t workers, drape_run_log* logs,
                                drape_status* statuses, double* solve_seconds, double* total_seconds) {
   if (!ctxs || count < 1 || workers < 1)

@@ -399,8 +399,17 @@ double Context::static_energy() {
   return reduce_partials(kReduceGrid, 0, kEnergy);
 }
 
-// One attempt at step size h from xn_ (into x_): feasible start, then the regularised inexact Newton.
+// One attempt at step size h from xn_ (into x_): the PTC prediction x_n + h^2 g, the feasible start, then the
+// regularised inexact Newton to the inner tolerance.
 AttemptResult Context::attempt(double h, double scale) {
+  kcheck(launch_predict(dp_, xn_.ptr, nullptr, h, xhat_.ptr, stream_), "predict");
+  return newton(h, scale, opt_.inner_tolerance, opt_.inner_max, opt_.newton_start == 1);
+}
+
+// The regularised inexact Newton on Phi(x) = 1/(2h^2)(x - x_hat)^T M (x - x_hat) + E_s(x) with x_hat in xhat_,
+// from xn_ (feasible_start: from x_n + alpha_max (x_hat - x_n), the CCD-cut prediction) into x_, until
+// |grad Phi| / scale <= tolerance or `max_updates` updates.
+AttemptResult Context::newton(double h, double scale, double tolerance, int max_updates, bool feasible_start) {
   AttemptResult res;
   const double inv_h2 = 1.0 / (h * h);
   const size_t nv = 3 * size_t(host_.V);
@@ -410,9 +419,8 @@ AttemptResult Context::attempt(double h, double scale) {
     phase_ms_[phase] += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return out;
   };
-  kcheck(launch_predict(dp_, xn_.ptr, h * h, xhat_.ptr, stream_), "predict");
   mg_setups_since_power_ = 1 << 20;  // a new step size: fresh spectral estimates at the first set-up
-  if (opt_.newton_start == 1) {
+  if (feasible_start) {
     // The reference's start: x_n + alpha_max (x_hat - x_n).
     kcheck(launch_sub(int(nv), xhat_.ptr, xn_.ptr, towards_.ptr, stream_), "towards");
     double a0 = t_phase(kCcd, [&] { return max_step(xn_.ptr, towards_.ptr); });
@@ -446,12 +454,12 @@ AttemptResult Context::attempt(double h, double scale) {
       res.non_finite = true;
       return res;
     }
-    if (rel <= opt_.inner_tolerance) {
+    if (rel <= tolerance) {
       finish(1);
       res.status = 0;
       return res;
     }
-    if (it == opt_.inner_max) {
+    if (it == max_updates) {
       finish(2);
       res.status = 1;
       return res;
@@ -734,6 +742,41 @@ int Context::solve_equilibrium(const double* start, double h0, drape_run_log* lo
                  mg_outcome_[5], mg_outcome_[6], mg_outcome_[7]);
   if (log) *log = out;
   return reason;
+}
+
+// One backward-Euler step of size h from the current state x_n with velocity v (drape.rs:410-417,
+// drape-e4.ts:45-52): x_hat = x_n + h v + h^2 g, the scale |grad Phi(x_n)|, the regularised Newton from the
+// CCD-cut prediction x_n + alpha_max (x_hat - x_n) to |grad Phi| / scale <= tolerance, then v = (x - x_n) / h.
+int Context::time_step(double h, const double* v_in, double tolerance, int max_iterations, double* v_out,
+                       drape_time_step_log* log) {
+  const size_t nv = 3 * size_t(host_.V);
+  if (!(h > 0) || !(tolerance > 0) || max_iterations < 1) throw std::invalid_argument("invalid time step arguments");
+  std::memset(phase_ms_, 0, sizeof phase_ms_);
+  records_.clear();
+  attempts_.clear();
+  record_step_ = 1;
+  auto t0 = std::chrono::steady_clock::now();
+  if (vel_.n != nv) vel_.alloc(nv);
+  if (v_in) vel_.upload(v_in, nv, stream_);
+  else check(cudaMemsetAsync(vel_.ptr, 0, nv * sizeof(double), stream_), "memset");
+  check(cudaMemcpyAsync(xn_.ptr, x_.ptr, nv * sizeof(double), cudaMemcpyDeviceToDevice, stream_), "save");
+  kcheck(launch_predict(dp_, xn_.ptr, vel_.ptr, h, xhat_.ptr, stream_), "predict");
+  const double scale = assemble(xn_.ptr, 1.0 / (h * h), 0.0, 0, false);
+  AttemptResult res = newton(h, scale, tolerance, max_iterations, true);
+  kcheck(launch_velocity(int(nv), x_.ptr, xn_.ptr, h, vel_.ptr, stream_), "velocity");
+  if (v_out) vel_.download(v_out, nv, stream_);
+  sync();
+  drape_time_step_log out{};
+  out.iterations = res.updates;
+  out.status = res.non_finite ? 6 : res.status == 0 ? 1 : res.status == 1 ? 2 : res.status == 2 ? 3 : 5;
+  out.pcg_iterations = res.pcg_iterations;
+  out.mu_retries = res.mu_retries;
+  out.scale = scale;
+  out.final_relative_residual = records_.empty() ? 0.0 : records_.back().relative_residual;
+  out.max_mu = res.max_mu;
+  out.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  if (log) *log = out;
+  return out.status;
 }
 
 // ---------------------------------------------------------------- host-buffer entry points

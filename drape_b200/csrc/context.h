@@ -100,6 +100,10 @@ class Context {
   double static_residual();                        // |grad E_s(x)| at the current state
   double static_energy();                          // E_s(x) at the current state
   int solve_equilibrium(const double* start, double h0, drape_run_log* log);
+  // One backward-Euler step of size h from the current state and velocity v_in (3V, host; null: at rest); the
+  // state advances, v_out (3V, host, may be null) receives the new velocity. Returns the log's status.
+  int time_step(double h, const double* v_in, double tolerance, int max_iterations, double* v_out,
+                drape_time_step_log* log);
   const std::vector<drape_step_record>& steps() const { return steps_; }
   const std::vector<drape_newton_record>& newton_records() const { return records_; }
   const std::vector<drape_attempt_record>& attempt_records() const { return attempts_; }
@@ -174,6 +178,7 @@ class Context {
   double max_step(const double* x, const double* d);
   double energy_change(const double* x, const double* d, double alpha, double inv_h2, int mode);
   AttemptResult attempt(double h, double scale);
+  AttemptResult newton(double h, double scale, double tolerance, int max_updates, bool feasible_start);
   void record_phase(int phase, cudaEvent_t a, cudaEvent_t b);
 
   HostProblem host_;
@@ -248,6 +253,7 @@ class Context {
   DeviceArray<int> rt_ptr_, rt_ent_, rt_pos_, rh_ptr_, rh_ent_, rh_pos_;
   // state and work (vertex layout f64)
   DeviceArray<double> x_, xn_, xhat_, xt_, d_, towards_;
+  DeviceArray<double> vel_;  // backward-Euler velocity (time_step)
   DeviceArray<double> g_, partial_, scalars_;
   // BSR f32 planes and PCG vectors (float4 rows)
   DeviceArray<float4> a0_, a1_;

@@ -262,11 +262,14 @@ __global__ void __launch_bounds__(256) reduce_partials(const double* partial, in
 }
 
 // x_hat = x + h^2 g on the rows' vertices (x_hat starts as a copy of x).
-__global__ void predict_rows_kernel(DevProblem p, const double* x, double h2, double* x_hat) {
+// x_hat = x + h v + h^2 g on the free vertices (rows); v null: x + h^2 g (the PTC prediction, e7_ptc.rs:54-58);
+// with v: the backward-Euler prediction (drape.rs:177-185, drape-step.ts:26-38).
+__global__ void predict_rows_kernel(DevProblem p, const double* x, const double* vel, double h, double* x_hat) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= p.R) return;
   const int v = p.row_vertex[r];
-  for (int k = 0; k < 3; ++k) x_hat[3 * v + k] = x[3 * v + k] + h2 * p.gravity[k];
+  for (int k = 0; k < 3; ++k)
+    x_hat[3 * v + k] = x[3 * v + k] + (vel ? h * vel[3 * v + k] : 0.0) + h * h * p.gravity[k];
 }
 
 __global__ void axpy_kernel(int n, const double* x, double alpha, const double* d, double* out) {
@@ -383,10 +386,22 @@ cudaError_t launch_reduce(const double* partial, int n, int op, double* out, int
   return cudaGetLastError();
 }
 
-cudaError_t launch_predict(const DevProblem& p, const double* x, double h2, double* x_hat, cudaStream_t s) {
+cudaError_t launch_predict(const DevProblem& p, const double* x, const double* vel, double h, double* x_hat,
+                           cudaStream_t s) {
   cudaError_t e = cudaMemcpyAsync(x_hat, x, 3 * sizeof(double) * (size_t)p.V, cudaMemcpyDeviceToDevice, s);
   if (e != cudaSuccess) return e;
-  predict_rows_kernel<<<blocks_for(p.R, 256), 256, 0, s>>>(p, x, h2, x_hat);
+  predict_rows_kernel<<<blocks_for(p.R, 256), 256, 0, s>>>(p, x, vel, h, x_hat);
+  return cudaGetLastError();
+}
+
+// v = (x - x_prev) / h on every vertex (fixed vertices: zero).
+__global__ void velocity_kernel(int n, const double* x, const double* x_prev, double inv_h, double* v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) v[i] = (x[i] - x_prev[i]) * inv_h;
+}
+
+cudaError_t launch_velocity(int n, const double* x, const double* x_prev, double h, double* v, cudaStream_t s) {
+  velocity_kernel<<<blocks_for(n, 256), 256, 0, s>>>(n, x, x_prev, 1.0 / h, v);
   return cudaGetLastError();
 }
 

@@ -45,7 +45,11 @@ cudaError_t launch_slope(const DevProblem& p, const double* g, const double* d, 
 cudaError_t launch_inf_norm(const DevProblem& p, const double* d, double* partial, int grid, cudaStream_t s);
 // out[slot] = sum (op 0) or min (op 1) of n partials.
 cudaError_t launch_reduce(const double* partial, int n, int op, double* out, int slot, cudaStream_t s);
-cudaError_t launch_predict(const DevProblem& p, const double* x, double h2, double* x_hat, cudaStream_t s);
+// x_hat = x + h v + h^2 g on the free vertices (v null: x + h^2 g), x elsewhere.
+cudaError_t launch_predict(const DevProblem& p, const double* x, const double* vel, double h, double* x_hat,
+                           cudaStream_t s);
+// v = (x - x_prev) / h over n values.
+cudaError_t launch_velocity(int n, const double* x, const double* x_prev, double h, double* v, cudaStream_t s);
 cudaError_t launch_axpy(int n, const double* x, double alpha, const double* d, double* out, cudaStream_t s);
 cudaError_t launch_sub(int n, const double* a, const double* b, double* out, cudaStream_t s);
 cudaError_t launch_scatter_direction(const DevProblem& p, const float4* sol, double* d, cudaStream_t s);

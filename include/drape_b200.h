@@ -108,6 +108,16 @@ typedef struct {
   int32_t pad;
 } drape_run_log;
 
+/* Outcome of drape_time_step (the reference's TimeStep, drape.rs:403-408, and the step's StepSolution status,
+ * newton.ts:8): status 1 converged, 2 iteration limit, 3 line search failed, 5 regularisation (mu) cap, 6 non-finite
+ * residual. */
+typedef struct {
+  int32_t iterations, status, pcg_iterations, mu_retries;
+  double scale;                  /* |grad Phi(x_n)|, the residual's scale */
+  double final_relative_residual; /* |grad Phi(x)| / scale at the end */
+  double max_mu, seconds;
+} drape_time_step_log;
+
 /* One accepted PTC step (gpu-ptc.bin columns, run-e7.ts:96). residual is |grad E_s| at the step's start;
  * seconds is the solve's host time at the step's end (the solve synchronizes its stream there), so a solve run to
  * a tight tolerance also tells when it passed a looser one: the first step whose starting residual is below that
@@ -183,6 +193,15 @@ drape_status drape_get_state(const drape_ctx* ctx, double* xyz, double* final_h)
 /* PTC to equilibrium from `start_xyz` (NULL: the current state) with first step `h0` (<= 0: options.h0)
  * (replaces solveEquilibrium, drape-e7.ts:156-180; oracle ptc_solve, e7_ptc.rs:170-189). */
 drape_status drape_solve_equilibrium(drape_ctx* ctx, const double* start_xyz, double h0, drape_run_log* log);
+/* One dynamic (backward-Euler) step of size h s from the context's state x_n with velocity v (3V m/s, NULL: at
+ * rest), the reference's time_step (drape.rs:410-417; GPU: drape-e4.ts:45-52 timeStep): prediction
+ * x_hat = x_n + h v + h^2 g on the free vertices, Newton on Phi(x) = (x - x_hat)^T M (x - x_hat) / (2 h^2) + E(x)
+ * from the CCD-cut prediction x_n + alpha_max (x_hat - x_n), regularised like the PTC's inner Newton, until
+ * |grad Phi| / |grad Phi(x_n)| <= tolerance or max_iterations updates. The context's state becomes the step's
+ * result; v_out (3V, may be NULL) receives (x - x_n) / h. The Newton records of the step are then in
+ * drape_newton_records (step 1). Returns DRAPE_OK whatever the Newton's status (see log). */
+drape_status drape_time_step(drape_ctx* ctx, double h, const double* v, double tolerance, int32_t max_iterations,
+                             double* v_out, drape_time_step_log* log);
 /* Many independent drapes at once: each of `count` distinct contexts runs drape_solve_equilibrium(ctx, NULL, 0, ...)
  * from its current state, on `workers` host threads that take the next unsolved drape in turn. Every context keeps
  * its own stream, so the kernels of up to `workers` drapes share the GPU; the threads block on events rather than

@@ -194,6 +194,33 @@ int oracle_ptc(void* p, const double* start, double h0, int controller, double e
   }
 }
 
+// One backward-Euler step (drape.rs:410-417) of size h from (x, v): Newton (regularised) to |grad Phi| / scale <=
+// tolerance or max_iterations updates, direction 0 band Cholesky / 1 f64 block-Jacobi PCG (rtol, maxit). Writes
+// the new positions and velocity; stats: [updates, status (1 converged, 2 limit, 3 line search, 5 mu cap), final
+// relative residual, scale, max mu].
+int oracle_time_step(void* p, const double* x, const double* v, double h, double tolerance, int max_iterations,
+                     int direction, double rtol, int maxit, double* x_out, double* v_out, double* stats) {
+  try {
+    auto& d = *static_cast<Handle*>(p)->drape;
+    size_t V = d.mesh.rest.size();
+    NewtonSettings set{tolerance, max_iterations, 1e-4, 30};
+    DirectionSolver dir{direction != 0, rtol, maxit};
+    TimeStepResult r = time_step(d, to_vec3(x, V), v ? to_vec3(v, V) : std::vector<Vec3>(V, Vec3{0, 0, 0}), h, set, dir);
+    from_vec3(r.solution.positions, x_out);
+    from_vec3(r.velocity, v_out);
+    const StepStatus st = r.solution.status;
+    int code = st == StepStatus::Converged ? 1 : st == StepStatus::IterationLimit ? 2
+             : st == StepStatus::LineSearchFailed ? 3 : st == StepStatus::RegularizationCap ? 5 : 1;
+    double out[5] = {double(r.solution.halvings.size()), double(code), r.solution.residuals.back(), r.scale,
+                     r.solution.regularization.max_mu};
+    std::memcpy(stats, out, sizeof out);
+    return 0;
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return 1;
+  }
+}
+
 // Block-Jacobi PCG on a BSR system (f64, or f32 emulating the GPU's operation order when single != 0).
 // info: [iterations, converged, breakdown, recursive relative residual].
 void oracle_pcg(int rows, const int32_t* row_ptr, const int32_t* col_idx, const double* vals, const double* rhs,

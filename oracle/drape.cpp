@@ -361,6 +361,29 @@ StepSolution solve_step_regularized(const DrapeStep& s, std::vector<Vec3> start,
   }
 }
 
+// drape.rs:177-185 (x_hat = x + h v + h^2 g on free vertices, pinned ones stay), with this scene's gravity vector.
+std::vector<Vec3> dynamic_prediction(const Drape& d, const std::vector<Vec3>& x, const std::vector<Vec3>& v, double h) {
+  std::vector<Vec3> p = x;
+  for (int i : d.free_)
+    for (int k = 0; k < 3; ++k) p[i][k] = x[i][k] + h * v[i][k] + h * h * d.gravity[k];
+  return p;
+}
+
+// drape.rs:410-417 with the regularised solver (the E4 scheme's; e3_generate.rs:46).
+TimeStepResult time_step(const Drape& d, const std::vector<Vec3>& x, const std::vector<Vec3>& v, double h,
+                         const NewtonSettings& set, const DirectionSolver& dir) {
+  d.time_step = h;
+  DrapeStep step{&d, dynamic_prediction(d, x, v, h)};
+  TimeStepResult out;
+  out.scale = vector_norm(step.residual(x));
+  auto start = d.has_contact() ? feasible_start(step, x) : step.x_hat;
+  out.solution = solve_step_regularized(step, start, out.scale, set, dir);
+  out.velocity.resize(x.size());
+  for (size_t i = 0; i < x.size(); ++i)
+    for (int k = 0; k < 3; ++k) out.velocity[i][k] = (out.solution.positions[i][k] - x[i][k]) / h;
+  return out;
+}
+
 // e4_rules.rs:15-44
 double next_forcing(double previous, double ratio) {
   double eta = 0.9 * ratio * ratio, safeguard = 0.9 * previous * previous;

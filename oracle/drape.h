@@ -135,6 +135,18 @@ int line_search(const DrapeStep& s, const std::vector<Vec3>& x, const std::vecto
 StepSolution solve_step_regularized(const DrapeStep& s, std::vector<Vec3> start, double scale,
                                     const NewtonSettings& set, const DirectionSolver& dir);
 
+// One backward-Euler step from (x, v) (drape.rs:403-417): x_hat = x + h v + h^2 g on the free vertices, Newton on
+// Phi from x_hat, or with colliders from its feasible cut x + alpha_max (x_hat - x) (drape.rs:397-401), the residual
+// scaled by |grad Phi(x)|; velocity (x_new - x) / h.
+struct TimeStepResult {
+  StepSolution solution;
+  double scale = 0;
+  std::vector<Vec3> velocity;
+};
+std::vector<Vec3> dynamic_prediction(const Drape& d, const std::vector<Vec3>& x, const std::vector<Vec3>& v, double h);
+TimeStepResult time_step(const Drape& d, const std::vector<Vec3>& x, const std::vector<Vec3>& v, double h,
+                         const NewtonSettings& set, const DirectionSolver& dir);
+
 // e4_rules.rs:15-44
 double next_forcing(double previous, double ratio);
 double f32_spacing(double max_abs);

@@ -47,6 +47,8 @@ def load():
         lib.oracle_ptc.argtypes = [P, P, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                    ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                    ctypes.c_int, ctypes.c_int, ctypes.c_double, P, P]
+        lib.oracle_time_step.argtypes = [P, P, P, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_double, ctypes.c_int, P, P, P]
         lib.oracle_pcg.argtypes = [ctypes.c_int, P, P, P, P, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                    ctypes.c_double, ctypes.c_int, ctypes.c_int, P, P]
         _lib = lib
@@ -126,6 +128,17 @@ class Scene:
 
     def static_energy(self, x):
         return self.lib.oracle_static_energy(P(self.h), ptr(x))
+
+    def time_step(self, x, v, h, tolerance=1e-10, max_iterations=30, pcg=False, rtol=1e-6, maxit=2000):
+        """One backward-Euler step (drape.rs:410-417) from (x, v): (x_new, v_new, stats dict)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        v = None if v is None else np.ascontiguousarray(v, dtype=np.float64)
+        x_out, v_out, st = np.zeros(3 * self.V), np.zeros(3 * self.V), np.zeros(5)
+        if self.lib.oracle_time_step(P(self.h), ptr(x), None if v is None else ptr(v), h, tolerance, max_iterations,
+                                     int(pcg), rtol, maxit, ptr(x_out), ptr(v_out), ptr(st)):
+            raise RuntimeError(self.lib.oracle_last_error().decode())
+        return x_out, v_out, dict(zip(["iterations", "status", "final_relative_residual", "scale", "max_mu"],
+                                      st.tolist()))
 
     def ptc(self, start=None, h0=1e-3, doubling=True, equilibrium=0.0, absolute=1e-6, floor=False,
             max_steps=1000, pcg=True, rtol=1e-6, maxit=2000, progress=False, predicted_start=False, budget_s=0.0):

@@ -127,3 +127,19 @@ def test_sheet_scene_counts_and_material():
     assert s.dhat == 2e-3 and s.kappa == 1e3
     m = s.mass()
     assert abs(m.sum() - 0.15) <= 1e-12
+
+
+def test_backward_euler_free_fall_and_velocity():
+    """The oracle's dynamic step (drape.rs:410-417) from rest with no contact yet: the sheet falls as one body,
+    v = g h after the first step (the membrane and hinges are unloaded), and the returned velocity is
+    (x_new - x) / h."""
+    sc = oracle_py.Scene("sheet", 9, seed=0, plane=True)
+    x0 = sc.start()
+    h = 1.0 / 240.0
+    x1, v1, st = sc.time_step(x0, None, h, tolerance=1e-10)
+    assert st["status"] == 1 and st["iterations"] >= 1
+    assert np.allclose(v1, (x1 - x0) / h, rtol=0, atol=1e-12)
+    vy = v1.reshape(-1, 3)[:, 1]
+    assert np.allclose(vy, -9.81 * h, rtol=1e-3), (vy.min(), vy.max())  # the 1e-5 m start jitter strains it
+    x2, v2, _ = sc.time_step(x1, v1, h, tolerance=1e-10)
+    assert np.allclose(v2.reshape(-1, 3)[:, 1], -2 * 9.81 * h, rtol=1e-3)

@@ -42,15 +42,17 @@ def _solve_noalloc(torch, rp, ci, vals, rhs, rtol, maxit, measure_memory=False):
     x4 = torch.full((R, 4), float("nan"), dtype=torch.float32, device=dev)  # the solve must overwrite it
     row_ptr = torch.tensor(np.asarray(rp, np.int32), device=dev)
     col_idx = torch.tensor(np.asarray(ci, np.int32), device=dev)
-    torch.cuda.synchronize()
     info = np.zeros(3, np.int32)
     rel = ctypes.c_double()
+    torch.cuda.synchronize()
+    # the caller's buffers are all in place: the device's free memory just before and just after the call
+    free_before = torch.cuda.mem_get_info(0)[0] if measure_memory else None
     st = fn(R, P(row_ptr.data_ptr()), P(col_idx.data_ptr()), P(a0.data_ptr()), P(a1.data_ptr()), P(a2.data_ptr()),
             P(b4.data_ptr()), P(x4.data_ptr()), rtol, maxit, None, info.ctypes.data_as(P), ctypes.byref(rel))
     assert st == 0, lib.drape_last_error(None).decode()
     free_after = torch.cuda.mem_get_info(0)[0] if measure_memory else None
     x = x4[:, :3].reshape(-1).double().cpu().numpy()
-    return ((x, free_after) if measure_memory else x), int(info[0]), int(info[1])
+    return ((x, free_before, free_after) if measure_memory else x), int(info[0]), int(info[1])
 
 
 def _check_against_both(torch, rp, ci, vals, rhs, label, measure_memory=False):
@@ -63,12 +65,9 @@ def _check_against_both(torch, rp, ci, vals, rhs, label, measure_memory=False):
     ref_ctx.close()
     x64, info64 = oracle_py.pcg(rp, ci, vals, rhs, 1e-10, 20000)
     assert info64["converged"], label
-    torch.cuda.synchronize()
-    free_before = torch.cuda.mem_get_info(0)[0] if measure_memory else None
     x_new, iters, status = _solve_noalloc(torch, rp, ci, vals, rhs, 1e-7, 20000, measure_memory=measure_memory)
     if measure_memory:
-        free_after = x_new[1]
-        x_new = x_new[0]
+        x_new, free_before, free_after = x_new
         # The driver hands out device memory in 2 MiB pages; any allocation by the call shows up as a whole page.
         assert abs(free_before - free_after) < (2 << 20), (label, free_before, free_after)
     assert status == 1 and info_ref["status"] == "converged", label
