@@ -544,10 +544,11 @@ def probe(args):
         _, info = d.pcg(b, 1e-6, 2000, blocks=blocks)
         out["pcg"] = info
         lib.drape_time_multilevel.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]
-        tm = (ctypes.c_float * 3)()
+        tm = (ctypes.c_float * 4)()
         for its in (20, 200):
             assert lib.drape_time_multilevel(d.h, its, tm) == 0, lib.drape_last_error(d.h)
-            out[f"iterations_{its}"] = {"vcycle_ms": tm[0], "pcg_iteration_ms": tm[1], "pdl": tm[2]}
+            out[f"iterations_{its}"] = {"vcycle_ms": tm[0], "pcg_iteration_ms": tm[1], "pdl": tm[2],
+                                        "pcg_iteration_stream_ms": tm[3]}
         out["spmv_ms"] = d.time_spmv(200, 8, 256)
     else:
         net = api.Network.trained()

@@ -274,6 +274,27 @@ drape_status drape_time_step(drape_ctx* ctx, double h, const double* v, double t
   });
 }
 
+drape_status drape_prolong_state(const drape_ctx* cctx, const double* coarse, int32_t coarse_columns, double* fine_out,
+                                 int32_t* moved, int32_t* infeasible) {
+  drape_ctx* ctx = const_cast<drape_ctx*>(cctx);
+  return guarded(ctx, [&](drape::Context& c) {
+    if (!coarse || !fine_out || coarse_columns < 2) return fail(ctx, "drape_prolong_state: invalid arguments", DRAPE_E_ARG);
+    const drape::HostProblem& p = c.problem();
+    std::vector<double> in(coarse, coarse + 3 * size_t(coarse_columns) * coarse_columns), out;
+    std::vector<int> bad;
+    int m = 0;
+    try {
+      m = drape::prolong_state(p, in, coarse_columns, &out, &bad);
+    } catch (const std::invalid_argument& e) {
+      return fail(ctx, e.what(), DRAPE_E_ARG);
+    }
+    std::copy(out.begin(), out.end(), fine_out);
+    if (moved) *moved = m;
+    if (infeasible) *infeasible = int32_t(bad.size());
+    return DRAPE_OK;
+  });
+}
+
 drape_status drape_solve_batch(drape_ctx* const* ctxs, int32_t count, int32_t workers, drape_run_log* logs,
                                drape_status* statuses, double* solve_seconds, double* total_seconds) {
   if (!ctxs || count < 1 || workers < 1)
@@ -669,11 +690,11 @@ drape_status drape_time_assembly(drape_ctx* ctx, int32_t launches, float* ms) {
   });
 }
 
-drape_status drape_time_multilevel(drape_ctx* ctx, int32_t iterations, float* out3) {
+drape_status drape_time_multilevel(drape_ctx* ctx, int32_t iterations, float* out4) {
   return guarded(ctx, [&](drape::Context& c) {
-    if (iterations < 2 || !out3) return fail(ctx, "invalid arguments", DRAPE_E_ARG);
+    if (iterations < 2 || !out4) return fail(ctx, "invalid arguments", DRAPE_E_ARG);
     if (c.mg_levels() == 0) return fail(ctx, "no multilevel hierarchy for this problem", DRAPE_E_ARG);
-    c.time_multilevel(iterations, out3);
+    c.time_multilevel(iterations, out4, out4 + 3);
     return DRAPE_OK;
   });
 }

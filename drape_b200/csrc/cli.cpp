@@ -3,6 +3,7 @@
 //
 //   drape --case <dir> [--mode cold|warm|prolong] [--start <state prefix>]
 //         [--preconditioner jacobi|multilevel|learned] [--network <weights file>] [--device <n>] [--checks]
+//   drape prolong --coarse <state prefix> --coarse-n <n> --fine-dir <case dir> --out <state prefix>
 //   environment: E7_BUDGET_S (time budget of the solve, s), E7_PROGRESS (one stderr line per accepted step)
 //
 // Reads <dir>/problem.json + problem.bin (`oracle e7-generate`), solves to equilibrium with the rules of the
@@ -260,7 +261,59 @@ bool write_checks(drape_ctx* ctx, const std::string& dir, const std::string& tex
 
 }  // namespace
 
+// `drape prolong --coarse <state prefix> --coarse-n <n> --fine-dir <case dir> --out <state prefix>`: the start state
+// of the prolong mode from a coarse equilibrium, in place of `oracle e7-prolong` (e7_prolong.rs:52-64): host
+// arithmetic only (drape::prolong_state), written in the coarse state's dtype with its final_h.
+int prolong_main(int argc, char** argv) {
+  std::string coarse, fine_dir, out, n_text;
+  for (int i = 1; i < argc; ++i) {
+    const std::string k = argv[i];
+    std::string* dst = k == "--coarse" ? &coarse : k == "--coarse-n" ? &n_text : k == "--fine-dir" ? &fine_dir
+                     : k == "--out" ? &out : nullptr;
+    if (!dst || i + 1 >= argc) {
+      std::fprintf(stderr, "drape prolong: unknown or incomplete option %s\n", k.c_str());
+      return 2;
+    }
+    *dst = argv[++i];
+  }
+  if (coarse.empty() || fine_dir.empty() || out.empty() || n_text.empty()) {
+    std::fprintf(stderr, "usage: drape prolong --coarse <state prefix> --coarse-n <n> --fine-dir <case dir> --out <state prefix>\n");
+    return 2;
+  }
+  try {
+    const drape::HostProblem fine = drape::read_problem_files(fine_dir);
+    std::vector<double> xc;
+    double h = 0.0;
+    std::string err;
+    if (!read_state(coarse, &xc, &h, &err)) throw std::runtime_error(err);
+    const bool single = drape::read_text_file(coarse + ".json").find("\"f32\"") != std::string::npos;
+    std::vector<double> xf;
+    std::vector<int> bad;
+    const int moved = drape::prolong_state(fine, xc, std::atoi(n_text.c_str()), &xf, &bad);
+    std::printf("prolongation: %d vertices projected to d = d_hat, %zu infeasible\n", moved, bad.size());
+    if (!bad.empty()) throw std::runtime_error("infeasible start after projection");
+    bool ok;
+    if (single) {
+      std::vector<float> f(xf.begin(), xf.end());
+      ok = write_bytes(out + ".bin", f.data(), f.size() * sizeof(float));
+    } else {
+      ok = write_bytes(out + ".bin", xf.data(), xf.size() * sizeof(double));
+    }
+    std::ofstream j(out + ".json");
+    char buf[256];
+    std::snprintf(buf, sizeof buf, "{\"vertices\":%d,\"final_h\":%.17g,\"dtype\":\"%s\"}\n", fine.V, h,
+                  single ? "f32" : "f64");
+    j << buf;
+    if (!ok || !j) throw std::runtime_error("cannot write " + out);
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "drape prolong: %s\n", e.what());
+    return 1;
+  }
+  return 0;
+}
+
 int main(int argc, char** argv) {
+  if (argc > 1 && std::string(argv[1]) == "prolong") return prolong_main(argc - 1, argv + 1);
   Args a;
   std::string err;
   if (!parse(argc, argv, &a, &err)) {

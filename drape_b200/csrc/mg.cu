@@ -22,12 +22,32 @@ constexpr int kUpdateThreads = 256;     // one thread per row
 
 enum { kPartZr = 0, kPartZrPrev = 1, kPartPq = 2, kPartRr = 3 };
 
-// Programmatic dependent launch: a kernel of the cycle lets the next one launch at once (its CTAs then wait in
-// griddepcontrol.wait until this grid has completed and its writes are visible). Both are no-ops for a kernel
-// launched without the attribute.
-__device__ __forceinline__ void pdl_enter() {
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+// Programmatic dependent launch. Each kernel of the cycle first waits for the previous grid (griddepcontrol.wait
+// returns once it has completed and its writes are visible) and only then lets the next kernel launch. So when a
+// kernel starts, the kernel before its predecessor has completed: the code before its own wait may read anything
+// written two or more kernels back (the static matrix, the row structure, vectors of earlier phases) and so
+// overlaps those loads with the predecessor's tail; what the predecessor writes is read only after the wait. Both
+// instructions are no-ops for a kernel launched without the attribute (then every earlier kernel has completed).
+__device__ __forceinline__ void pdl_wait() {
   asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// Pulls the cache line of p into L1 ahead of its use.
+__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
+// A 36-byte f32 block of the fine BSR planes (a0, a1 16 bytes, a2 4 bytes) into L1.
+__device__ __forceinline__ void prefetch_block(const DevBsr& A, int k) {
+  prefetch_l1(A.a0 + k);
+  prefetch_l1(A.a1 + k);
+  prefetch_l1(A.a2 + k);
+}
+
+// A 48-byte coarse stencil block into L1 (it may straddle two 128-byte lines).
+__device__ __forceinline__ void prefetch_stencil(const float4* A, int w2, int I, int o) {
+  const float4* b = A + (size_t(I) * w2 + o) * 3;
+  prefetch_l1(b);
+  prefetch_l1(b + 2);
 }
 
 template <typename... Params, typename... Args>
@@ -603,52 +623,70 @@ template <int kSrcW, bool kCheck>
 __global__ void __launch_bounds__(kRestrictThreads) restrict_kernel(RestrictArgs a) {
   constexpr bool kSrcBsr = kSrcW == 0;
   constexpr int kSrcW2 = kSrcW * kSrcW;
-  pdl_enter();
+  constexpr int kPer = kSrcBsr ? 9 : (kSrcW2 + 2) / 3;  // entries per lane (<= 25 blocks per fine row)
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int I = blockIdx.x * kRestrictRows + warp;
+  const int s = lane / 3, k3 = lane % 3;
+  const int nc = a.dst.n, nf = a.src.n;
+  const int X = I % nc, Y = I / nc, ax = s % 3 - 1, by = s / 3 - 1;
+  const int fx = 2 * X + ax, fy = 2 * Y + by;
+  const bool has_row = I < a.dst.rows && lane < 27 && fx >= 0 && fy >= 0 && fx < nf && fy < nf;
+  const int i = has_row ? fy * nf + fx : 0;
+  // Before the wait (mg.h's ordering): the row structure, the operator's blocks and the coarse smoother, which no
+  // kernel of the solve writes; src.r and src.z come from the previous kernel and are read after it.
+  int jj[kPer];
+  int k0 = 0;
+  if (kSrcBsr) {
+    int k1 = 0;
+    if (has_row) {
+      k0 = a.fine.row_ptr[i] + k3;
+      k1 = a.fine.row_ptr[i + 1];
+    }
+#pragma unroll
+    for (int t = 0; t < kPer; ++t) {
+      jj[t] = has_row && k0 + 3 * t < k1 ? a.fine.col_idx[k0 + 3 * t] : -1;
+      if (jj[t] >= 0) prefetch_block(a.fine.A, k0 + 3 * t);
+    }
+  } else {
+#pragma unroll
+    for (int t = 0; t < kPer; ++t) {
+      const int o = k3 + 3 * t;
+      int j = -1;
+      jj[t] = has_row && o < kSrcW2 && stencil_neighbour(nf, kSrcW, fx, fy, o, &j) ? j : -1;
+      if (jj[t] >= 0) prefetch_stencil(a.src.A, kSrcW2, i, o);
+    }
+  }
+  float sm[9];
+  const bool writer = lane == 0 && I < a.dst.rows && !a.coarsest;
+#pragma unroll
+  for (int e = 0; e < 9; ++e) sm[e] = writer ? a.dst.S[e * a.dst.rows + I] : 0.0f;
+  pdl_wait();
   if (kCheck) {
     if (pcg_stop(a.state, a.rr_partial, a.rr_count)) return;
   } else if (a.state && a.state->done) {
     return;
   }
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int I = blockIdx.x * kRestrictRows + warp;
-  const int s = lane / 3, k3 = lane % 3;
   float3 t = make_float3(0.f, 0.f, 0.f);
-  if (I < a.dst.rows && lane < 27) {
-    const int nc = a.dst.n, nf = a.src.n;
-    const int X = I % nc, Y = I / nc, ax = s % 3 - 1, by = s / 3 - 1;
-    const int fx = 2 * X + ax, fy = 2 * Y + by;
-    if (fx >= 0 && fy >= 0 && fx < nf && fy < nf) {
-      const int i = fy * nf + fx;
-      float3 acc = make_float3(0.f, 0.f, 0.f);
-      if (kSrcBsr) {  // <= 25 blocks per row: <= 9 per lane, column indices fetched first
-        const int k0 = a.fine.row_ptr[i] + k3, k1 = a.fine.row_ptr[i + 1];
-        int jj[9];
+  if (has_row) {
+    float3 acc = make_float3(0.f, 0.f, 0.f);
 #pragma unroll
-        for (int t = 0; t < 9; ++t) jj[t] = k0 + 3 * t < k1 ? a.fine.col_idx[k0 + 3 * t] : -1;
-#pragma unroll
-        for (int t = 0; t < 9; ++t) {
-          if (jj[t] < 0) continue;
-          float m[9];
-          load_block(a.fine.A, k0 + 3 * t, m);
-          acc = add3(acc, mul(m, f3(a.src.z[jj[t]])));
-        }
+    for (int q = 0; q < kPer; ++q) {
+      if (jj[q] < 0) continue;
+      if (kSrcBsr) {
+        float m[9];
+        load_block(a.fine.A, k0 + 3 * q, m);
+        acc = add3(acc, mul(m, f3(a.src.z[jj[q]])));
       } else {
-#pragma unroll
-        for (int t = 0; t < (kSrcW2 + 2) / 3; ++t) {
-          const int o = k3 + 3 * t;
-          int j;
-          if (o < kSrcW2 && stencil_neighbour(nf, kSrcW, fx, fy, o, &j))
-            acc = add3(acc, stencil_apply(a.src.A, kSrcW2, i, o, f3(a.src.z[j])));
-        }
+        acc = add3(acc, stencil_apply(a.src.A, kSrcW2, i, k3 + 3 * q, f3(a.src.z[jj[q]])));
       }
-      const float w = (ax ? 0.5f : 1.0f) * (by ? 0.5f : 1.0f);
-      t = scale3(w, k3 == 0 ? sub3(f3(a.src.r[i]), acc) : scale3(-1.0f, acc));
     }
+    const float w = (ax ? 0.5f : 1.0f) * (by ? 0.5f : 1.0f);
+    t = scale3(w, k3 == 0 ? sub3(f3(a.src.r[i]), acc) : scale3(-1.0f, acc));
   }
   t = warp_sum3(t);
   if (lane == 0 && I < a.dst.rows) {
     a.dst.r[I] = pack(t);
-    if (!a.coarsest) a.dst.z[I] = pack(smooth(a.dst.S, a.dst.rows, I, t, false));
+    if (!a.coarsest) a.dst.z[I] = pack(mul(sm, t));
   }
 }
 
@@ -669,72 +707,93 @@ struct SmoothedArgs {
 
 // Fine step before the smoothed restriction: t = r - A z_0, u = Sp t; inside flexible PCG it first takes the
 // iteration's stopping test (kCheck), which restrict_kernel takes without the smoothed prolongation.
+// The row structure of fine row i for 8 lanes: each lane's <= 4 column indices (-1 past the row's end) and its
+// first block index; the blocks are prefetched into L1.
+__device__ __forceinline__ int fine_row(const MgFine& f, int i, bool active, int lane, int jj[4]) {
+  int k0 = 0, k1 = 0;
+  if (active) {
+    k0 = f.row_ptr[i] + lane;
+    k1 = f.row_ptr[i + 1];
+  }
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    jj[t] = active && k0 + kLanes * t < k1 ? f.col_idx[k0 + kLanes * t] : -1;
+    if (jj[t] >= 0) prefetch_block(f.A, k0 + kLanes * t);
+  }
+  return k0;
+}
+
 template <bool kCheck>
 __global__ void __launch_bounds__(kRowThreads) residual_smoothed_kernel(SmoothedArgs a) {
-  pdl_enter();
+  const int lane = threadIdx.x % kLanes;
+  const int i = blockIdx.x * (kRowThreads / kLanes) + threadIdx.x / kLanes;
+  const bool active = i < a.fine.R;
+  // Before the wait: the row structure and blocks, Sp; r and z_0 are the previous kernel's (the update).
+  int jj[4];
+  const int k0 = fine_row(a.fine, i, active, lane, jj);
+  float sp[9];
+#pragma unroll
+  for (int e = 0; e < 9; ++e) sp[e] = active && lane == 0 ? a.Sp[e * a.fine.R + i] : 0.0f;
+  pdl_wait();
   if (kCheck) {
     if (pcg_stop(a.state, a.rr_partial, a.rr_count)) return;
   } else if (a.state && a.state->done) {
     return;
   }
-  const int lane = threadIdx.x % kLanes;
-  const int i = blockIdx.x * (kRowThreads / kLanes) + threadIdx.x / kLanes;
-  const bool active = i < a.fine.R;
   float3 acc = make_float3(0.f, 0.f, 0.f);
-  if (active) {  // <= 25 blocks per row: <= 4 per lane, column indices fetched first
-    const int k0 = a.fine.row_ptr[i] + lane, k1 = a.fine.row_ptr[i + 1];
-    int jj[4];
 #pragma unroll
-    for (int t = 0; t < 4; ++t) jj[t] = k0 + kLanes * t < k1 ? a.fine.col_idx[k0 + kLanes * t] : -1;
-#pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      if (jj[t] < 0) continue;
-      float m[9];
-      load_block(a.fine.A, k0 + kLanes * t, m);
-      acc = add3(acc, mul(m, f3(a.z[jj[t]])));
-    }
+  for (int t = 0; t < 4; ++t) {
+    if (jj[t] < 0) continue;
+    float m[9];
+    load_block(a.fine.A, k0 + kLanes * t, m);
+    acc = add3(acc, mul(m, f3(a.z[jj[t]])));
   }
   acc = group_sum(acc);
   if (active && lane == 0) {
     const float3 t = sub3(f3(a.r[i]), acc);
     a.t[i] = pack(t);
-    a.u[i] = pack(smooth(a.Sp, a.fine.R, i, t, false));
+    a.u[i] = pack(mul(sp, t));
   }
 }
 
 // Smoothed prolongation of the level-1 correction: v = P e_1 (bilinear), y = z_0 + v - Sp A v.
 __global__ void __launch_bounds__(kRowThreads) interp_smoothed_kernel(SmoothedArgs a) {
-  pdl_enter();
-  if (a.state && a.state->done) return;
   const int lane = threadIdx.x % kLanes;
   const int i = blockIdx.x * (kRowThreads / kLanes) + threadIdx.x / kLanes;
   const int n = a.fine.n;
   const bool active = i < a.fine.R;
+  // Before the wait: the row structure and blocks, Sp and z_0 (the update's, many kernels back); e_1 is the
+  // previous kernel's.
+  int jj[4];
+  const int k0 = fine_row(a.fine, i, active, lane, jj);
+  const bool writer = active && lane == 0;
+  float sp[9];
+#pragma unroll
+  for (int e = 0; e < 9; ++e) sp[e] = writer ? a.Sp[e * a.fine.R + i] : 0.0f;
+  const float3 zi = writer ? f3(a.z[i]) : make_float3(0.f, 0.f, 0.f);
+  pdl_wait();
+  if (a.state && a.state->done) return;
   float3 acc = make_float3(0.f, 0.f, 0.f);
-  if (active) {
-    const int k0 = a.fine.row_ptr[i] + lane, k1 = a.fine.row_ptr[i + 1];
-    int jj[4];
 #pragma unroll
-    for (int t = 0; t < 4; ++t) jj[t] = k0 + kLanes * t < k1 ? a.fine.col_idx[k0 + kLanes * t] : -1;
-#pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      if (jj[t] < 0) continue;
-      const int j = jj[t];
-      float m[9];
-      load_block(a.fine.A, k0 + kLanes * t, m);
-      acc = add3(acc, mul(m, interpolate(a.e1, a.nc, j % n, j / n)));
-    }
+  for (int t = 0; t < 4; ++t) {
+    if (jj[t] < 0) continue;
+    const int j = jj[t];
+    float m[9];
+    load_block(a.fine.A, k0 + kLanes * t, m);
+    acc = add3(acc, mul(m, interpolate(a.e1, a.nc, j % n, j / n)));
   }
   acc = group_sum(acc);
-  if (active && lane == 0) {
+  if (writer) {
     const float3 v = interpolate(a.e1, a.nc, i % n, i / n);
-    a.y[i] = pack(sub3(add3(f3(a.z[i]), v), smooth(a.Sp, a.fine.R, i, acc, false)));
+    a.y[i] = pack(sub3(add3(zi, v), mul(sp, acc)));
   }
 }
 
 // e_L = A_L^{-1} r_L (dense f32 inverse), one CTA: r staged in shared memory, one warp per output entry.
 __global__ void __launch_bounds__(1024) coarse_solve_kernel(MgLevel lv, const float* inv, const MgState* state) {
-  pdl_enter();
+  const int m3 = 3 * lv.rows;
+  for (int l = threadIdx.x; l * 32 < m3 * m3; l += blockDim.x) prefetch_l1(inv + 32 * l);  // static inverse
+  pdl_wait();
   if (state && state->done) return;
   __shared__ float rs[3 * kMgCoarsestRowsMax];
   const int m = 3 * lv.rows;
@@ -758,7 +817,13 @@ __global__ void __launch_bounds__(1024) coarse_solve_kernel(MgLevel lv, const fl
 // and a prolongation (three launches) with one; the vectors stay in shared memory, one warp per row product.
 constexpr int kTailRows = 81;  // n_T <= 9
 __global__ void __launch_bounds__(1024) tail_kernel(MgLevel T, MgLevel C, const float* inv, const MgState* state) {
-  pdl_enter();
+  {  // before the wait: the level's stencil, smoother and the coarsest inverse into L1 (static within a solve)
+    const int mc = 3 * C.rows, a_lines = (T.rows * T.w * T.w * 48 + 127) / 128, s_lines = (9 * T.rows + 31) / 32;
+    for (int l = threadIdx.x; l < a_lines; l += blockDim.x) prefetch_l1(reinterpret_cast<const char*>(T.A) + 128 * l);
+    for (int l = threadIdx.x; l < s_lines; l += blockDim.x) prefetch_l1(T.S + 32 * l);
+    for (int l = threadIdx.x; l * 32 < mc * mc; l += blockDim.x) prefetch_l1(inv + 32 * l);
+  }
+  pdl_wait();
   if (state && state->done) return;
   __shared__ float3 t_s[kTailRows], y_s[kTailRows];
   __shared__ float rc_s[3 * kMgCoarsestRowsMax], ec_s[3 * kMgCoarsestRowsMax];
@@ -837,55 +902,79 @@ template <int kW, bool kY>
 __global__ void __launch_bounds__(kRowThreads) prolong_kernel(ProlongArgs a) {
   constexpr bool kFine = kW == 0;
   constexpr int kW2 = kW * kW;
-  pdl_enter();
-  if (a.state && a.state->done) return;
+  constexpr int kPer = kFine ? 4 : (kW2 + kLanes - 1) / kLanes;  // <= 25 blocks per fine row: <= 4 per lane
   const int lane = threadIdx.x % kLanes;
   const int i = blockIdx.x * (kRowThreads / kLanes) + threadIdx.x / kLanes;
   const int n = a.lv.n, nc = a.coarse.n;
   const bool active = i < a.lv.rows;
-  auto y_at = [&](int j) -> float3 {
-    if (kY) return f3(a.y[j]);
-    return add3(f3(a.lv.z[j]), interpolate(a.coarse.e, nc, j % n, j / n));
-  };
+  // Before the wait: the row structure and blocks, and this level's r and z (written by its restriction, or on the
+  // fine level by the update, two or more kernels back), S and r_prev. The coarse correction e (the previous
+  // kernel's) and y (kY: the previous kernel's) are read after it.
+  int jj[kPer];
+  int k0 = 0;
+  if (kFine) {
+    int k1 = 0;
+    if (active) {
+      k0 = a.fine.row_ptr[i] + lane;
+      k1 = a.fine.row_ptr[i + 1];
+    }
+#pragma unroll
+    for (int t = 0; t < kPer; ++t) {
+      jj[t] = active && k0 + kLanes * t < k1 ? a.fine.col_idx[k0 + kLanes * t] : -1;
+      if (jj[t] >= 0) prefetch_block(a.fine.A, k0 + kLanes * t);
+    }
+  } else {
+    const int X = i % n, Y = i / n;
+#pragma unroll
+    for (int t = 0; t < kPer; ++t) {
+      const int o = lane + kLanes * t;
+      int j = -1;
+      jj[t] = active && o < kW2 && stencil_neighbour(n, kW, X, Y, o, &j) ? j : -1;
+      if (jj[t] >= 0) prefetch_stencil(a.lv.A, kW2, i, o);
+    }
+  }
+  float3 zj[kPer];
+#pragma unroll
+  for (int t = 0; t < kPer; ++t) zj[t] = !kY && jj[t] >= 0 ? f3(a.lv.z[jj[t]]) : make_float3(0.f, 0.f, 0.f);
+  const bool writer = active && lane == 0;
+  const bool dots = kFine && a.zr_partial;  // inside flexible PCG only (a stand-alone cycle has no r_prev)
+  float sm[9];
+#pragma unroll
+  for (int e = 0; e < 9; ++e) sm[e] = writer ? a.lv.S[e * a.lv.rows + i] : 0.0f;
+  const float3 r = writer ? f3(a.lv.r[i]) : make_float3(0.f, 0.f, 0.f);
+  const float3 zi = writer && !kY ? f3(a.lv.z[i]) : make_float3(0.f, 0.f, 0.f);
+  const float3 rp = writer && dots ? f3(a.r_prev[i]) : make_float3(0.f, 0.f, 0.f);
+  pdl_wait();
+  if (a.state && a.state->done) return;
   float3 acc = make_float3(0.f, 0.f, 0.f);
-  if (active) {
-    if (kFine) {  // <= 25 blocks per row: <= 4 per lane, column indices fetched first
-      const int k0 = a.fine.row_ptr[i] + lane, k1 = a.fine.row_ptr[i + 1];
-      int jj[4];
 #pragma unroll
-      for (int t = 0; t < 4; ++t) jj[t] = k0 + kLanes * t < k1 ? a.fine.col_idx[k0 + kLanes * t] : -1;
-#pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        if (jj[t] < 0) continue;
-        const float3 y = y_at(jj[t]);
-        float m[9];
-        load_block(a.fine.A, k0 + kLanes * t, m);
-        acc = add3(acc, mul(m, y));
-      }
+  for (int t = 0; t < kPer; ++t) {
+    const int j = jj[t];
+    if (j < 0) continue;
+    const float3 y = kY ? f3(a.y[j]) : add3(zj[t], interpolate(a.coarse.e, nc, j % n, j / n));
+    if (kFine) {
+      float m[9];
+      load_block(a.fine.A, k0 + kLanes * t, m);
+      acc = add3(acc, mul(m, y));
     } else {
-      const int X = i % n, Y = i / n;
-#pragma unroll
-      for (int t = 0; t < (kW2 + kLanes - 1) / kLanes; ++t) {
-        const int o = lane + kLanes * t;
-        int j;
-        if (o >= kW2 || !stencil_neighbour(n, kW, X, Y, o, &j)) continue;
-        acc = add3(acc, stencil_apply(a.lv.A, kW2, i, o, y_at(j)));
-      }
+      acc = add3(acc, stencil_apply(a.lv.A, kW2, i, lane + kLanes * t, y));
     }
   }
   acc = group_sum(acc);
   float zr = 0.0f, zrp = 0.0f;
-  if (active && lane == 0) {
-    const float3 r = f3(a.lv.r[i]);
-    const float3 y = y_at(i);
-    const float3 e = add3(y, smooth(a.lv.S, a.lv.rows, i, sub3(r, acc), true));
+  if (writer) {
+    const float3 y = kY ? f3(a.y[i]) : add3(zi, interpolate(a.coarse.e, nc, i % n, i / n));
+    const float3 d = sub3(r, acc);
+    // e = y + S^T (r - A y)
+    const float3 e = add3(y, make_float3(sm[0] * d.x + sm[3] * d.y + sm[6] * d.z, sm[1] * d.x + sm[4] * d.y + sm[7] * d.z,
+                                         sm[2] * d.x + sm[5] * d.y + sm[8] * d.z));
     a.lv.e[i] = pack(e);
-    if (kFine && a.zr_partial) {  // inside flexible PCG only (a stand-alone cycle has no r_prev)
+    if (dots) {
       zr = dot3(e, r);
-      zrp = dot3(e, f3(a.r_prev[i]));
+      zrp = dot3(e, rp);
     }
   }
-  if (kFine && a.zr_partial) {
+  if (dots) {
     zr = cta_sum(zr);
     zrp = cta_sum(zrp);
     if (threadIdx.x == 0) {
@@ -910,36 +999,49 @@ struct DirectionArgs {
 
 // beta (Polak-Ribiere form of flexible CG) = z.(r - r_prev) / rz_old;  p = z + beta p_old;  q = A p.
 __global__ void __launch_bounds__(kRowThreads) direction_kernel(DirectionArgs a) {
-  pdl_enter();
   MgState* st = a.state;
-  if (st->done) return;
-  const float zr = sum_partials(a.zr_partial, a.zr_count);
-  const float zrp = sum_partials(a.zrp_partial, a.zr_count);
-  const bool first = st->iterations == 0;
-  const float beta = first ? 0.0f : (zr - zrp) / st->rz_old;
   const int lane = threadIdx.x % kLanes;
   const int i = blockIdx.x * (kRowThreads / kLanes) + threadIdx.x / kLanes;
   const bool active = i < a.fine.R;
+  // Before the wait: the row structure and blocks, the previous direction p_old (this kernel's own output one
+  // iteration back) and the update's scalars; z and the partial dot products are the previous kernel's.
+  int jj[4];
+  int k0 = 0, k1 = 0;
+  if (active) {
+    k0 = a.fine.row_ptr[i] + lane;
+    k1 = a.fine.row_ptr[i + 1];
+  }
+  float3 po[4];
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    jj[t] = active && k0 + kLanes * t < k1 ? a.fine.col_idx[k0 + kLanes * t] : -1;
+    if (jj[t] >= 0) prefetch_block(a.fine.A, k0 + kLanes * t);
+    po[t] = jj[t] >= 0 ? f3(a.p_old[jj[t]]) : make_float3(0.f, 0.f, 0.f);
+  }
+  const float3 po_i = active && lane == 0 ? f3(a.p_old[i]) : make_float3(0.f, 0.f, 0.f);
+  const int iterations = st->iterations;
+  const float rz_old = st->rz_old;
+  pdl_wait();
+  if (st->done) return;
+  const float zr = sum_partials(a.zr_partial, a.zr_count);
+  const float zrp = sum_partials(a.zrp_partial, a.zr_count);
+  const bool first = iterations == 0;
+  const float beta = first ? 0.0f : (zr - zrp) / rz_old;
   float3 acc = make_float3(0.f, 0.f, 0.f);
-  if (active) {  // <= 25 blocks per row: <= 4 per lane, column indices fetched first
-    const int k0 = a.fine.row_ptr[i] + lane, k1 = a.fine.row_ptr[i + 1];
-    int jj[4];
 #pragma unroll
-    for (int t = 0; t < 4; ++t) jj[t] = k0 + kLanes * t < k1 ? a.fine.col_idx[k0 + kLanes * t] : -1;
-#pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      if (jj[t] < 0) continue;
-      const int j = jj[t];
-      const float3 p = first ? f3(a.z[j]) : add3(f3(a.z[j]), scale3(beta, f3(a.p_old[j])));
-      float m[9];
-      load_block(a.fine.A, k0 + kLanes * t, m);
-      acc = add3(acc, mul(m, p));
-    }
+  for (int t = 0; t < 4; ++t) {
+    if (jj[t] < 0) continue;
+    const float3 z = f3(a.z[jj[t]]);
+    const float3 p = first ? z : add3(z, scale3(beta, po[t]));
+    float m[9];
+    load_block(a.fine.A, k0 + kLanes * t, m);
+    acc = add3(acc, mul(m, p));
   }
   acc = group_sum(acc);
   float pq = 0.0f;
   if (active && lane == 0) {
-    const float3 p = first ? f3(a.z[i]) : add3(f3(a.z[i]), scale3(beta, f3(a.p_old[i])));
+    const float3 z = f3(a.z[i]);
+    const float3 p = first ? z : add3(z, scale3(beta, po_i));
     a.p_new[i] = pack(p);
     a.q[i] = pack(acc);
     pq = dot3(p, acc);
@@ -971,8 +1073,17 @@ struct UpdateArgs {
 
 // alpha = z.r / p.q;  x += alpha p;  r_next = r - alpha q;  z_pre = S0 r_next.
 __global__ void __launch_bounds__(kUpdateThreads) update_kernel(UpdateArgs a) {
-  pdl_enter();
   MgState* st = a.state;
+  const int i = blockIdx.x * kUpdateThreads + threadIdx.x;
+  const bool active = i < a.R;
+  // Before the wait: x, the current residual (the previous iteration's update wrote them) and the fine smoother;
+  // p, q, z.r and the partial p.q are the previous kernel's.
+  const float3 x = active ? f3(a.x[i]) : make_float3(0.f, 0.f, 0.f);
+  const float3 rc = active ? f3(a.r_cur[i]) : make_float3(0.f, 0.f, 0.f);
+  float sm[9];
+#pragma unroll
+  for (int e = 0; e < 9; ++e) sm[e] = active ? a.S0[e * a.R + i] : 0.0f;
+  pdl_wait();
   if (st->done) {
     if (a.set_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(a.cond, 0);
     return;
@@ -989,14 +1100,13 @@ __global__ void __launch_bounds__(kUpdateThreads) update_kernel(UpdateArgs a) {
     }
     return;
   }
-  const int i = blockIdx.x * kUpdateThreads + threadIdx.x;
   float rr = 0.0f;
-  if (i < a.R) {
+  if (active) {
     const float3 p = f3(a.p[i]);
-    a.x[i] = pack(add3(f3(a.x[i]), scale3(alpha, p)));
-    const float3 r = sub3(f3(a.r_cur[i]), scale3(alpha, f3(a.q[i])));
+    a.x[i] = pack(add3(x, scale3(alpha, p)));
+    const float3 r = sub3(rc, scale3(alpha, f3(a.q[i])));
     a.r_next[i] = pack(r);
-    a.z_pre[i] = pack(smooth(a.S0, a.R, i, r, false));
+    a.z_pre[i] = pack(mul(sm, r));
     rr = dot3(r, r);
   }
   rr = cta_sum(rr);
@@ -1360,7 +1470,8 @@ cudaError_t mg_pcg_init(const MgDevice& d, float tol2, int max_iterations, int s
 namespace {
 
 // Iterations of parity 0 and 1 (one graph body); the second update kernel owns the WHILE condition.
-cudaError_t launch_body(const MgDevice& d, cudaGraphConditionalHandle cond, bool pdl, cudaStream_t s, int* launches) {
+cudaError_t launch_body(const MgDevice& d, cudaGraphConditionalHandle cond, bool graph, bool pdl, cudaStream_t s,
+                        int* launches) {
   const int R = d.fine.R;
   for (int par = 0; par < 2; ++par) {
     cudaError_t e = launch_cycle(d, par, true, pdl, s, launches);
@@ -1391,7 +1502,7 @@ cudaError_t launch_body(const MgDevice& d, cudaGraphConditionalHandle cond, bool
     ua.pq_count = row_grid(R);
     ua.rr_partial = d.partial + kPartRr * kMgPartials;
     ua.cond = cond;
-    ua.set_cond = par == 1;
+    ua.set_cond = graph && par == 1;
     if ((e = launch(update_kernel, update_grid(R), kUpdateThreads, s, pdl, ua)) != cudaSuccess) return e;
     *launches += 2;
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -1421,7 +1532,7 @@ cudaError_t mg_build_solve_graph(const MgDevice& d, cudaStream_t s, cudaGraphExe
         cudaSuccess)
       goto done;
     *launches_per_body = 0;
-    cudaError_t le = launch_body(d, cond, pdl, s, launches_per_body);
+    cudaError_t le = launch_body(d, cond, true, pdl, s, launches_per_body);
     e = cudaStreamEndCapture(s, &body);
     if (le != cudaSuccess) e = le;
     if (e != cudaSuccess) goto done;
@@ -1430,6 +1541,15 @@ cudaError_t mg_build_solve_graph(const MgDevice& d, cudaStream_t s, cudaGraphExe
 done:
   cudaGraphDestroy(graph);
   return e;
+}
+
+cudaError_t mg_launch_iterations(const MgDevice& d, int pairs, cudaStream_t s) {
+  int launches = 0;
+  for (int k = 0; k < pairs; ++k) {
+    cudaError_t e = launch_body(d, cudaGraphConditionalHandle{}, false, true, s, &launches);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 cudaError_t mg_apply(const MgDevice& d, cudaStream_t s) {

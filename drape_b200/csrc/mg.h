@@ -124,6 +124,9 @@ cudaError_t mg_pcg_init(const MgDevice& d, float tol2, int max_iterations, int s
 // programmatic dependencies (each launches while its predecessor finishes).
 cudaError_t mg_build_solve_graph(const MgDevice& d, cudaStream_t s, cudaGraphExec_t* exec, int* launches_per_body,
                                  bool pdl);
+// `pairs` x 2 flexible PCG iterations launched one kernel at a time on the stream (programmatic dependent launch,
+// no graph): the kernels a profiler sees individually; the state must come from mg_pcg_init.
+cudaError_t mg_launch_iterations(const MgDevice& d, int pairs, cudaStream_t s);
 // One V-cycle z = M r on level 0 alone (r in d.r[0], z in d.lv[0].e): the preconditioner check.
 cudaError_t mg_apply(const MgDevice& d, cudaStream_t s);
 

@@ -443,4 +443,65 @@ double json_number(const std::string& text, const std::string& anchor, const std
   return number(text, anchor, key);
 }
 
+namespace {
+
+// Distance to collider `c` (8 doubles: kind 1 plane n.x = w, 2 sphere |x - c| = w) and its gradient.
+double collider_distance(const double* c, const double x[3], double n[3]) {
+  if (c[0] == 1.0) {
+    for (int k = 0; k < 3; ++k) n[k] = c[1 + k];
+    return c[1] * x[0] + c[2] * x[1] + c[3] * x[2] - c[4];
+  }
+  double q[3] = {x[0] - c[1], x[1] - c[2], x[2] - c[3]};
+  const double len = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
+  for (int k = 0; k < 3; ++k) n[k] = q[k] / len;
+  return len - c[4];
+}
+
+}  // namespace
+
+int prolong_state(const HostProblem& fine, const std::vector<double>& coarse, int coarse_columns,
+                  std::vector<double>* out, std::vector<int>* infeasible) {
+  const int nc = coarse_columns, nf = 2 * (coarse_columns - 1) + 1;
+  if (nc < 2 || coarse.size() != size_t(3) * nc * nc)
+    throw std::invalid_argument("prolong: the coarse state does not hold " + std::to_string(nc) + "^2 vertices");
+  if (size_t(nf) * nf != size_t(fine.V))
+    throw std::invalid_argument("prolong: prolonged " + std::to_string(nf * nf) + " vertices, the fine mesh has " +
+                                std::to_string(fine.V));
+  out->assign(3 * size_t(fine.V), 0.0);
+  for (int v = 0; v < fine.V; ++v) {
+    const int i = v % nf, j = v / nf;
+    const int i0 = i / 2, i1 = (i + 1) / 2, j0 = j / 2, j1 = (j + 1) / 2;
+    const int corners[4] = {j0 * nc + i0, j0 * nc + i1, j1 * nc + i0, j1 * nc + i1};
+    for (int k = 0; k < 3; ++k) {
+      double sum = 0.0;
+      for (int c : corners) sum += coarse[3 * size_t(c) + k];
+      (*out)[3 * size_t(v) + k] = sum / 4.0;
+    }
+  }
+  int moved = 0;
+  for (int v = 0; v < fine.V; ++v) {
+    double* x = out->data() + 3 * size_t(v);
+    const double before[3] = {x[0], x[1], x[2]};
+    for (int c = 0; c < fine.collider_count(); ++c) {
+      double n[3];
+      const double d = collider_distance(fine.colliders.data() + 8 * size_t(c), x, n);
+      if (d < fine.dhat)
+        for (int k = 0; k < 3; ++k) x[k] += (fine.dhat - d) * n[k];
+    }
+    moved += (x[0] != before[0] || x[1] != before[1] || x[2] != before[2]) ? 1 : 0;
+  }
+  if (infeasible) {
+    infeasible->clear();
+    for (int v = 0; v < fine.V; ++v) {
+      double dmin = INFINITY;
+      for (int c = 0; c < fine.collider_count(); ++c) {
+        double n[3];
+        dmin = std::min(dmin, collider_distance(fine.colliders.data() + 8 * size_t(c), out->data() + 3 * size_t(v), n));
+      }
+      if (dmin <= 0.0) infeasible->push_back(v);
+    }
+  }
+  return moved;
+}
+
 }  // namespace drape

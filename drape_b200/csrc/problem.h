@@ -64,6 +64,14 @@ double json_number(const std::string& text, const std::string& anchor, const std
 // Writes the same pair (the subset this GPU stage reads, plus f64 geometry).
 void write_problem_files(const HostProblem& p, const std::string& dir);
 
+// Coarse-to-fine start state for the prolong mode (the reference's e7_prolong.rs:7-64): the (2n - 1)^2 grid from the
+// n^2 one, every fine vertex the average of its four (possibly repeated) coarse corners; then every vertex closer
+// than d_hat to a collider moves along that collider's normal to d = d_hat, one pass over the colliders in order.
+// Returns the number of vertices moved; `infeasible` (may be null) receives the vertices at or inside a collider
+// afterwards. Throws std::invalid_argument when the prolonged grid is not `fine`'s.
+int prolong_state(const HostProblem& fine, const std::vector<double>& coarse, int coarse_columns,
+                  std::vector<double>* out, std::vector<int>* infeasible);
+
 // Checks sizes and index ranges of every array; returns an empty string when consistent.
 std::string validate(const HostProblem& p);
 

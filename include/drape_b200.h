@@ -202,6 +202,15 @@ drape_status drape_solve_equilibrium(drape_ctx* ctx, const double* start_xyz, do
  * drape_newton_records (step 1). Returns DRAPE_OK whatever the Newton's status (see log). */
 drape_status drape_time_step(drape_ctx* ctx, double h, const double* v, double tolerance, int32_t max_iterations,
                              double* v_out, drape_time_step_log* log);
+
+/* Coarse-to-fine start state for the prolong mode, in place of `oracle e7-prolong` (e7_prolong.rs:7-64): the
+ * (2n - 1)^2 vertices of `ctx`'s mesh from the n^2 coarse positions `coarse` (3 n^2, n = coarse_columns), each the
+ * average of its four (possibly repeated) coarse corners, then every vertex closer than d_hat to one of ctx's
+ * colliders moved along that collider's normal to d = d_hat (one pass, colliders in order). fine_out: 3V;
+ * *moved (may be NULL): vertices moved; *infeasible (may be NULL): vertices still at or inside a collider (the
+ * reference refuses such a start). DRAPE_E_ARG when the grids do not match. */
+drape_status drape_prolong_state(const drape_ctx* ctx, const double* coarse, int32_t coarse_columns, double* fine_out,
+                                 int32_t* moved, int32_t* infeasible);
 /* Many independent drapes at once: each of `count` distinct contexts runs drape_solve_equilibrium(ctx, NULL, 0, ...)
  * from its current state, on `workers` host threads that take the next unsolved drape in turn. Every context keeps
  * its own stream, so the kernels of up to `workers` drapes share the GPU; the threads block on events rather than
@@ -298,10 +307,11 @@ drape_status drape_time_assembly(drape_ctx* ctx, int32_t launches, float* ms);
 drape_status drape_spmv_benchmark(int32_t device, int32_t rows, int64_t blocks, const int32_t* row_ptr,
                                   const int32_t* col_idx, const float* values, const float* x, int32_t launches,
                                   int32_t lanes_per_row, int32_t threads, float* y, float* ms);
-/* Multilevel timings on the last assembled matrix and right-hand side: out3 = [ms per stand-alone V-cycle,
+/* Multilevel timings on the last assembled matrix and right-hand side: out4 = [ms per stand-alone V-cycle,
  * ms per flexible PCG iteration inside the solve graph (exactly `iterations` iterations), 1 if the graph's kernels
- * are linked by programmatic dependent launch]. */
-drape_status drape_time_multilevel(drape_ctx* ctx, int32_t iterations, float* out3);
+ * are linked by programmatic dependent launch, ms per iteration of the same iterations launched kernel by kernel
+ * on the stream (the launches a profiler sees one by one)]. */
+drape_status drape_time_multilevel(drape_ctx* ctx, int32_t iterations, float* out4);
 /* SM-clock cycles CTA 0 of the PCG kernel spent per phase since the last clear: [phase A (p, q = A p),
  * its CTA sum, its grid reduction, phase B (x, r, z), its CTA sum, its grid reduction, iterations]; clear != 0
  * zeroes the counters. */

@@ -11,7 +11,7 @@ import pytest
 
 from drape_b200 import api
 from drape_b200.build import CLI
-from tests import e7_replays
+from tests import e7_replays, oracle_py
 
 pytestmark = pytest.mark.gpu
 
@@ -82,3 +82,37 @@ def test_learned_preconditioner_from_the_command():
         _run("--case", t, "--mode", "cold", "--preconditioner", "learned")
         res = json.load(open(os.path.join(t, "gpu-cold", "gpu-result.json")))
         assert res["preconditioner"] == "learned" and res["stop"] == "tolerance", res
+
+
+def test_prolong_workflow():
+    """The prolong path of the pipeline (run-e7.ts:59-63 after e7_prolong.rs:52-64), on cases written by the oracle's
+    own e7-generate: the GPU's n17 equilibrium of the reference's base case is prolonged to the n33 case by
+    `drape prolong`, which writes the state `oracle e7-prolong` writes (its f64 values rounded to the coarse state's
+    f32); `drape --mode prolong` from it stops on the case's tolerance at an f64 equilibrium of the n33 case (the
+    oracle's polish lands within 1e-4 m, relative static energy 1e-9), in fewer steps than the cold solve."""
+    from tests.polish_state import polished_error
+
+    oracle_py.build()
+    with tempfile.TemporaryDirectory() as t:
+        c17, c33 = os.path.join(t, "drape-n17"), os.path.join(t, "drape-n33")
+        for n, c in ((17, c17), (33, c33)):
+            subprocess.run([oracle_py.CLI, "e7-generate", "--n", str(n), "--edit", "base", "--out", c], check=True,
+                           capture_output=True)
+        _run("--case", c17, "--mode", "cold")
+        eq = os.path.join(c17, "gpu-cold", "gpu-equilibrium")
+        start, ostart = os.path.join(t, "start33"), os.path.join(t, "oracle_start33")
+        _run("prolong", "--coarse", eq, "--coarse-n", "17", "--fine-dir", c33, "--out", start)
+        subprocess.run([oracle_py.CLI, "e7-prolong", "--coarse", eq, "--coarse-n", "17", "--fine-dir", c33, "--out",
+                        ostart], check=True, capture_output=True)
+        mine = np.fromfile(start + ".bin", np.float32)
+        ref = np.fromfile(ostart + ".bin", np.float64).astype(np.float32)
+        assert mine.size == 3 * 33 * 33 and np.array_equal(mine, ref)
+        _run("--case", c33, "--mode", "prolong", "--start", start)
+        res = json.load(open(os.path.join(c33, "gpu-prolong", "gpu-result.json")))
+        assert res["stop"] == "tolerance" and res["mode"] == "prolong", res
+        _run("--case", c33, "--mode", "cold")
+        cold = json.load(open(os.path.join(c33, "gpu-cold", "gpu-result.json")))
+        assert res["accepted_steps"] < cold["accepted_steps"], (res["accepted_steps"], cold["accepted_steps"])
+        x = np.fromfile(os.path.join(c33, "gpu-prolong", "gpu-equilibrium.bin"), np.float32).astype(np.float64)
+        err, e_rel, _, _, _ = polished_error(oracle_py.Scene("reference", 33, edit="base"), x)
+        assert err <= 1e-4 and e_rel <= 1e-9, (err, e_rel)
