@@ -116,3 +116,41 @@ def test_prolong_workflow():
         x = np.fromfile(os.path.join(c33, "gpu-prolong", "gpu-equilibrium.bin"), np.float32).astype(np.float64)
         err, e_rel, _, _, _ = polished_error(oracle_py.Scene("reference", 33, edit="base"), x)
         assert err <= 1e-4 and e_rel <= 1e-9, (err, e_rel)
+
+
+def test_comparer_verdict_on_cold_and_prolong_runs():
+    """The comparer's gates (e7_compare.rs:276-363, restated in tests/e7_compare.py) on the command's own outputs
+    for the reference's n17 base case written by the oracle's e7-generate, with the oracle's cold reference
+    solve beside it: every gate holds for the cold run, and for a prolong run of the n33 case from the prolonged
+    n17 equilibrium; a state pushed into the sphere trips intersection_free."""
+    from tests import e7_compare
+
+    oracle_py.build()
+    with tempfile.TemporaryDirectory() as t:
+        c17, c33 = os.path.join(t, "drape-n17"), os.path.join(t, "drape-n33")
+        for n, c in ((17, c17), (33, c33)):
+            subprocess.run([oracle_py.CLI, "e7-generate", "--n", str(n), "--edit", "base", "--out", c], check=True,
+                           capture_output=True)
+        subprocess.run([oracle_py.CLI, "e7-solve", "--dir", c17, "--mode", "cold"], check=True, capture_output=True)
+        _run("--case", c17, "--mode", "cold")
+        o17 = oracle_py.Scene("reference", 17, edit="base")
+        verdict, details = e7_compare.compare(c17, "cold", o17)
+        assert set(verdict) >= {"intersection_free", "rules_replayed_ok", "static_energy_ok", "final_state_residual_ok",
+                                "oracle_converged"}
+        assert all(verdict.values()), (verdict, details)
+        assert abs(details["energy_gap_over_cold"]) <= 1e-6 and details["max_vertex_gap_over_side"] <= 1e-3, details
+        start = os.path.join(t, "start33")
+        _run("prolong", "--coarse", os.path.join(c17, "gpu-cold", "gpu-equilibrium"), "--coarse-n", "17",
+             "--fine-dir", c33, "--out", start)
+        _run("--case", c33, "--mode", "prolong", "--start", start)
+        verdict, details = e7_compare.compare(c33, "prolong", oracle_py.Scene("reference", 33, edit="base"), start)
+        assert verdict["start_feasible"] and all(verdict.values()), (verdict, details)
+        # a planted intersection: the last kept state of the n17 run with a vertex inside the sphere
+        path = os.path.join(c17, "gpu-cold", "gpu-states.bin")
+        s = np.fromfile(path, np.float32)
+        V = 17 * 17
+        centre = 3 * ((V // 2) + (s.size // (3 * V) - 1) * V)
+        s[centre + 2] -= 0.05  # 5 cm down into the sphere (z up)
+        s.tofile(path)
+        verdict, _ = e7_compare.compare(c17, "cold", o17)
+        assert not verdict["intersection_free"]
