@@ -703,6 +703,7 @@ struct SmoothedArgs {
   MgState* state;       // flexible PCG state (null: stand-alone V-cycle)
   const float* rr_partial;
   int rr_count;
+  float* rr_init;       // residual_smoothed_kernel at the start of flexible PCG: per-CTA |r|^2 (else null)
 };
 
 // Fine step before the smoothed restriction: t = r - A z_0, u = Sp t; inside flexible PCG it first takes the
@@ -749,10 +750,17 @@ __global__ void __launch_bounds__(kRowThreads) residual_smoothed_kernel(Smoothed
     acc = add3(acc, mul(m, f3(a.z[jj[t]])));
   }
   acc = group_sum(acc);
+  float rr = 0.0f;
   if (active && lane == 0) {
-    const float3 t = sub3(f3(a.r[i]), acc);
+    const float3 r = f3(a.r[i]);
+    const float3 t = sub3(r, acc);
     a.t[i] = pack(t);
     a.u[i] = pack(mul(sp, t));
+    rr = dot3(r, r);
+  }
+  if (a.rr_init) {  // the first stopping test reads these slots (update_residual_kernel's layout)
+    rr = cta_sum(rr);
+    if (threadIdx.x == 0) a.rr_init[blockIdx.x] = rr;
   }
 }
 
@@ -1119,6 +1127,85 @@ __global__ void __launch_bounds__(kUpdateThreads) update_kernel(UpdateArgs a) {
   }
 }
 
+// The update fused with the smoothed path's fine residual (one kernel instead of two): alpha = z.r / p.q;
+// x += alpha p; r' = r - alpha q; z_0 = S0 r'; t = r' - A z_0; u = Sp t. r' and z_0 at the row's neighbours are
+// recomputed from r, q and S0 (local once alpha is known), so no CTA waits for another's update; the partial
+// |r'|^2 goes to the rows' CTA slot (row_grid(R) slots) for the next iteration's stopping test (restrict_kernel
+// <0, true> on t and u).
+__global__ void __launch_bounds__(kRowThreads) update_residual_kernel(UpdateArgs a, SmoothedArgs s) {
+  MgState* st = a.state;
+  const int lane = threadIdx.x % kLanes;
+  const int i = blockIdx.x * (kRowThreads / kLanes) + threadIdx.x / kLanes;
+  const bool active = i < a.R;
+  // Before the wait: the row structure and blocks, r and S0 at the neighbours and the row, x and Sp at the row
+  // (all written one iteration back or static); p, q and the partial p.q are the previous kernel's.
+  int jj[4];
+  const int k0 = fine_row(s.fine, i, active, lane, jj);
+  float3 rj[4];
+  float sj[4][9];
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    rj[t] = jj[t] >= 0 ? f3(a.r_cur[jj[t]]) : make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+    for (int e = 0; e < 9; ++e) sj[t][e] = jj[t] >= 0 ? a.S0[e * a.R + jj[t]] : 0.0f;
+  }
+  const bool writer = active && lane == 0;
+  float si[9], spi[9];
+#pragma unroll
+  for (int e = 0; e < 9; ++e) {
+    si[e] = writer ? a.S0[e * a.R + i] : 0.0f;
+    spi[e] = writer ? s.Sp[e * a.R + i] : 0.0f;
+  }
+  const float3 xi = writer ? f3(a.x[i]) : make_float3(0.f, 0.f, 0.f);
+  const float3 ri = writer ? f3(a.r_cur[i]) : make_float3(0.f, 0.f, 0.f);
+  pdl_wait();
+  if (st->done) {
+    if (a.set_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(a.cond, 0);
+    return;
+  }
+  const float pq = sum_partials(a.pq_partial, a.pq_count);
+  const float zr = st->zr;
+  const float alpha = zr / pq;
+  if (!(pq > 0.0f) || !isfinite(alpha)) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      st->pq = pq;
+      st->status = kStatusBreakdown;
+      st->done = 1;
+      if (a.set_cond) cudaGraphSetConditional(a.cond, 0);
+    }
+    return;
+  }
+  float3 acc = make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    if (jj[t] < 0) continue;
+    const float3 rn = sub3(rj[t], scale3(alpha, f3(a.q[jj[t]])));
+    float m[9];
+    load_block(s.fine.A, k0 + kLanes * t, m);
+    acc = add3(acc, mul(m, mul(sj[t], rn)));
+  }
+  acc = group_sum(acc);
+  float rr = 0.0f;
+  if (writer) {
+    a.x[i] = pack(add3(xi, scale3(alpha, f3(a.p[i]))));
+    const float3 rn = sub3(ri, scale3(alpha, f3(a.q[i])));
+    a.r_next[i] = pack(rn);
+    a.z_pre[i] = pack(mul(si, rn));
+    const float3 t = sub3(rn, acc);
+    s.t[i] = pack(t);
+    s.u[i] = pack(mul(spi, t));
+    rr = dot3(rn, rn);
+  }
+  rr = cta_sum(rr);
+  if (threadIdx.x == 0) a.rr_partial[blockIdx.x] = rr;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->pq = pq;
+    st->alpha = alpha;
+    st->rz_old = zr;
+    st->iterations = st->iterations + 1;
+  }
+}
+
 struct InitArgs {
   int R;
   const float4* b;
@@ -1192,10 +1279,11 @@ cudaError_t launch_cycle(const MgDevice& d, int parity, bool in_pcg, bool pdl, c
   sa.rr_partial = d.partial + kPartRr * kMgPartials;
   sa.rr_count = update_grid(d.fine.R);
   cudaError_t e;
-  if (smoothed) {  // t = r - A z_0, u = Sp t (and the stopping test inside flexible PCG)
-    e = in_pcg ? launch(residual_smoothed_kernel<true>, row_grid(d.fine.R), kRowThreads, s, pdl, sa)
-               : launch(residual_smoothed_kernel<false>, row_grid(d.fine.R), kRowThreads, s, pdl, sa);
-    if (e != cudaSuccess) return e;
+  // t = r - A z_0, u = Sp t: inside flexible PCG the previous iteration's update_residual_kernel (or the start,
+  // mg_pcg_init) formed them; a stand-alone V-cycle forms them here.
+  if (smoothed && !in_pcg) {
+    if ((e = launch(residual_smoothed_kernel<false>, row_grid(d.fine.R), kRowThreads, s, pdl, sa)) != cudaSuccess)
+      return e;
     ++*launches;
   }
   // with three or more levels, the last two run in one CTA (tail_kernel: level L - 2 is a stencil level, n <= 9)
@@ -1213,9 +1301,9 @@ cudaError_t launch_cycle(const MgDevice& d, int parity, bool in_pcg, bool pdl, c
     a.coarsest = l + 2 == L;
     a.state = st;
     a.rr_partial = d.partial + kPartRr * kMgPartials;
-    a.rr_count = update_grid(d.fine.R);
+    a.rr_count = smoothed ? row_grid(d.fine.R) : update_grid(d.fine.R);  // the update's CTA count
     const int grid = restrict_grid(a.dst.rows);
-    if (l == 0 && in_pcg && !smoothed) e = launch(restrict_kernel<0, true>, grid, kRestrictThreads, s, pdl, a);
+    if (l == 0 && in_pcg) e = launch(restrict_kernel<0, true>, grid, kRestrictThreads, s, pdl, a);
     else if (l == 0) e = launch(restrict_kernel<0, false>, grid, kRestrictThreads, s, pdl, a);
     else if (a.src.w == 7) e = launch(restrict_kernel<7, false>, grid, kRestrictThreads, s, pdl, a);
     else e = launch(restrict_kernel<5, false>, grid, kRestrictThreads, s, pdl, a);
@@ -1464,6 +1552,17 @@ cudaError_t mg_pcg_init(const MgDevice& d, float tol2, int max_iterations, int s
   a.max_iterations = max_iterations;
   a.stall_window = stall_window;
   init_kernel<<<update_grid(a.R), kUpdateThreads, 0, s>>>(a);
+  if (d.smoothed) {  // the first iteration's t, u and |r0|^2 slots, as update_residual_kernel leaves them
+    SmoothedArgs sa{};
+    sa.fine = d.fine;
+    sa.r = d.r[0];
+    sa.z = d.lv[0].z;
+    sa.Sp = d.Sp;
+    sa.t = d.t;
+    sa.u = d.u;
+    sa.rr_init = d.partial + kPartRr * kMgPartials;
+    residual_smoothed_kernel<false><<<row_grid(a.R), kRowThreads, 0, s>>>(sa);
+  }
   return cudaGetLastError();
 }
 
@@ -1503,7 +1602,16 @@ cudaError_t launch_body(const MgDevice& d, cudaGraphConditionalHandle cond, bool
     ua.rr_partial = d.partial + kPartRr * kMgPartials;
     ua.cond = cond;
     ua.set_cond = graph && par == 1;
-    if ((e = launch(update_kernel, update_grid(R), kUpdateThreads, s, pdl, ua)) != cudaSuccess) return e;
+    if (d.smoothed) {
+      SmoothedArgs sa{};
+      sa.fine = d.fine;
+      sa.Sp = d.Sp;
+      sa.t = d.t;
+      sa.u = d.u;
+      if ((e = launch(update_residual_kernel, row_grid(R), kRowThreads, s, pdl, ua, sa)) != cudaSuccess) return e;
+    } else if ((e = launch(update_kernel, update_grid(R), kUpdateThreads, s, pdl, ua)) != cudaSuccess) {
+      return e;
+    }
     *launches += 2;
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
