@@ -2,8 +2,9 @@
 
 Workload: the 1.0 m sheet of n x n vertices (default n = 129: 16641 vertices, 32768 triangles, 48896 hinges,
 180993 BSR blocks) over a sphere of radius 0.25 m and a ground plane at y = -0.25 m, isotropic StVK E = 5e5 Pa,
-nu = 0.3, t = 5e-4 m, k_b = 1e-5 N m, IPC d_hat = 2e-3 m, kappa = 1e3; PTC from dt0 = 1e-3 s, PCG rtol 1e-6,
-<= 2000 iterations. One step = one full cold solve to the converged state: |grad E_s| <= 1e-7 N (--absolute), the
+nu = 0.3, t = 5e-4 m, k_b = 1e-5 N m, IPC d_hat = 2e-3 m, kappa = 1e3; PTC from dt0 = 1e-3 s; Newton directions
+to the Eisenstat-Walker forcing tolerance in [1e-7, 1e-2], the reference GPU stage's own setting (run-e7.ts:22,
+e4_rules.rs:15-22; --forcing 0: a fixed PCG rtol 1e-6), <= 2000 PCG iterations. One step = one full cold solve to the converged state: |grad E_s| <= 1e-7 N (--absolute), the
 residual at which the converged state lies within 1e-4 m of the f64 equilibrium; the solve's time to the scene's
 1e-6 N Newton tolerance is reported beside it ("secondary": the same run, read from its step records).
 Direction solver (--preconditioner): learned (default: the multilevel V-cycle flexible PCG with the shipped
@@ -273,9 +274,12 @@ def run_gpu(args):
         "ms_per_step": t * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": f"sheet n{args.n} over sphere r=0.25 + ground plane y=-0.25, {PRECOND[args.preconditioner]}, "
-                               f"PTC dt0=1e-3 s to |grad E_s|<={args.absolute:g} N", "columns": args.n, "rows": R,
+                               f"PTC dt0=1e-3 s to |grad E_s|<={args.absolute:g} N, "
+                               f"{'Eisenstat-Walker forcing' if args.forcing else 'PCG rtol 1e-6'}",
+                   "columns": args.n, "rows": R,
                    "blocks": B, "seed": args.seed, "preconditioner": args.preconditioner,
                    "tolerance_N": args.absolute, "prolongation": ["bilinear", "smoothed"][args.prolongation],
+                   "forcing": ["fixed rtol 1e-6", "eisenstat-walker"][args.forcing],
                    "parallelism": f"replicas{world}",
                    "l2": "flushed (512 MiB write) before every timed solve"},
         "solve": {"converged": last["reason"] == "tolerance", "reason": last["reason"],
@@ -544,11 +548,12 @@ def probe(args):
         _, info = d.pcg(b, 1e-6, 2000, blocks=blocks)
         out["pcg"] = info
         lib.drape_time_multilevel.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]
-        tm = (ctypes.c_float * 4)()
+        tm = (ctypes.c_float * 6)()
         for its in (20, 200):
             assert lib.drape_time_multilevel(d.h, its, tm) == 0, lib.drape_last_error(d.h)
             out[f"iterations_{its}"] = {"vcycle_ms": tm[0], "pcg_iteration_ms": tm[1], "pdl": tm[2],
-                                        "pcg_iteration_stream_ms": tm[3]}
+                                        "pcg_iteration_stream_ms": tm[3], "setup_fresh_ms": tm[4],
+                                        "setup_reuse_ms": tm[5]}
         out["spmv_ms"] = d.time_spmv(200, 8, 256)
     else:
         net = api.Network.trained()
@@ -583,11 +588,11 @@ def main():
                     help="--impl reference --full-solve: print the FULL_SOLVE entry (per-step times) of the solve")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--preconditioner", default="learned", choices=["jacobi", "multilevel", "learned"])
-    ap.add_argument("--forcing", type=int, default=0, choices=[0, 1],
-                    help="Newton direction tolerance: 0 fixed PCG rtol 1e-6, 1 Eisenstat-Walker (the reference GPU "
-                         "stage's forcingFor, e4_rules.rs:15-22)")
-    ap.add_argument("--prolongation", type=int, default=1, choices=[0, 1],
-                    help="multilevel fine-to-coarse prolongation: 0 bilinear, 1 smoothed once (default)")
+    ap.add_argument("--forcing", type=int, default=1, choices=[0, 1],
+                    help="Newton direction tolerance: 1 (default) Eisenstat-Walker, the reference GPU stage's setting "
+                         "(run-e7.ts:22 forcing: true; e4_rules.rs:15-22); 0 a fixed PCG rtol 1e-6")
+    ap.add_argument("--prolongation", type=int, default=0, choices=[0, 1],
+                    help="multilevel fine-to-coarse prolongation: 0 bilinear (default), 1 smoothed once")
     ap.add_argument("--compare", default="jacobi", choices=["none", "jacobi", "all"],
                     help="after the timed steps, one device-timed solve of the same workload with each other solver")
     ap.add_argument("--probe", default=None, choices=["cycle", "network", "spmv", "solve"],

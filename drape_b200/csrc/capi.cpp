@@ -100,7 +100,7 @@ void drape_default_options(drape_options* o) {
   o->armijo = 1e-4;
   o->max_halvings = 30;
   o->time_budget_s = 0.0;
-  o->prolongation = 1;
+  o->prolongation = 0;
 }
 
 drape_status drape_create(const drape_problem_view* v, const drape_options* options, int32_t device, drape_ctx** out) {
@@ -690,11 +690,11 @@ drape_status drape_time_assembly(drape_ctx* ctx, int32_t launches, float* ms) {
   });
 }
 
-drape_status drape_time_multilevel(drape_ctx* ctx, int32_t iterations, float* out4) {
+drape_status drape_time_multilevel(drape_ctx* ctx, int32_t iterations, float* out6) {
   return guarded(ctx, [&](drape::Context& c) {
-    if (iterations < 2 || !out4) return fail(ctx, "invalid arguments", DRAPE_E_ARG);
+    if (iterations < 2 || !out6) return fail(ctx, "invalid arguments", DRAPE_E_ARG);
     if (c.mg_levels() == 0) return fail(ctx, "no multilevel hierarchy for this problem", DRAPE_E_ARG);
-    c.time_multilevel(iterations, out4, out4 + 3);
+    c.time_multilevel(iterations, out6, out6 + 3, out6 + 4);
     return DRAPE_OK;
   });
 }

@@ -1138,8 +1138,20 @@ void Context::precondition_host(const float* blocks, const double* rhs, double* 
   }
 }
 
-void Context::time_multilevel(int iterations, float* out3, float* out3_stream) {
+void Context::time_multilevel(int iterations, float* out3, float* out3_stream, float* out_setup) {
   if (mg_levels_ == 0) throw std::invalid_argument("no multilevel hierarchy for this problem");
+  if (out_setup) {  // one set-up with fresh spectral estimates (power method), one that reuses them
+    for (int k = 0; k < 2; ++k) {
+      mg_prepare();
+      mg_stale_ = true;
+      mg_setups_since_power_ = k == 0 ? (1 << 20) : 1;
+      check(cudaEventRecord(ev_[2], stream_), "event");
+      mg_prepare();
+      check(cudaEventRecord(ev_[3], stream_), "event");
+      sync();
+      cudaEventElapsedTime(&out_setup[k], ev_[2], ev_[3]);
+    }
+  }
   mg_prepare();
   check(cudaMemcpyAsync(mg_.r[0], b_.ptr, host_.R * sizeof(float4), cudaMemcpyDeviceToDevice, stream_), "copy");
   for (int k = 0; k < 3; ++k) kcheck(mg_apply(mg_, stream_), "V-cycle");

@@ -124,8 +124,9 @@ class Context {
   float time_assembly(int launches);
   // Multilevel timings on the last assembled matrix: [ms per stand-alone V-cycle (plain launches), ms per flexible
   // PCG iteration inside the solve graph (a fixed number of iterations), 1 if the graph links its kernels by
-  // programmatic dependent launch]; out3_stream (may be null): ms per iteration launched kernel by kernel.
-  void time_multilevel(int iterations, float* out3, float* out3_stream);
+  // programmatic dependent launch]; out3_stream (may be null): ms per iteration launched kernel by kernel;
+  // out_setup (may be null): ms of one hierarchy set-up with fresh spectral estimates and of one reusing them.
+  void time_multilevel(int iterations, float* out3, float* out3_stream, float* out_setup);
 
   // ---- multilevel preconditioner
   // Levels of the hierarchy the grid allows (0: not a structured grid of free vertices; only block Jacobi).

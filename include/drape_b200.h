@@ -87,7 +87,7 @@ typedef struct {
                                   1: projected (clamped membrane stress, Gauss-Newton hinge): SPD up to the barrier */
   double smoother_omega;       /* multilevel: damping of the Jacobi smoothers; 0 (default): per level
                                   2 / (1.1 lambda (1 + 1/30)) from the power method on D^{-1} A (stable) */
-  int32_t prolongation;        /* multilevel fine-to-coarse prolongation: 0 bilinear; 1 (default) bilinear smoothed
+  int32_t prolongation;        /* multilevel fine-to-coarse prolongation: 0 (default) bilinear; 1 bilinear smoothed
                                   once, (I - (4/3) lambda^{-1} D^{-1} A) P (smoothed aggregation's prolongation
                                   smoothing; level 1 becomes a 7 x 7 stencil) */
   int32_t pad_options;
@@ -307,11 +307,12 @@ drape_status drape_time_assembly(drape_ctx* ctx, int32_t launches, float* ms);
 drape_status drape_spmv_benchmark(int32_t device, int32_t rows, int64_t blocks, const int32_t* row_ptr,
                                   const int32_t* col_idx, const float* values, const float* x, int32_t launches,
                                   int32_t lanes_per_row, int32_t threads, float* y, float* ms);
-/* Multilevel timings on the last assembled matrix and right-hand side: out4 = [ms per stand-alone V-cycle,
+/* Multilevel timings on the last assembled matrix and right-hand side: out6 = [ms per stand-alone V-cycle,
  * ms per flexible PCG iteration inside the solve graph (exactly `iterations` iterations), 1 if the graph's kernels
  * are linked by programmatic dependent launch, ms per iteration of the same iterations launched kernel by kernel
- * on the stream (the launches a profiler sees one by one)]. */
-drape_status drape_time_multilevel(drape_ctx* ctx, int32_t iterations, float* out4);
+ * on the stream (the launches a profiler sees one by one), ms of one hierarchy set-up with fresh spectral
+ * estimates, ms of one reusing them]. */
+drape_status drape_time_multilevel(drape_ctx* ctx, int32_t iterations, float* out6);
 /* SM-clock cycles CTA 0 of the PCG kernel spent per phase since the last clear: [phase A (p, q = A p),
  * its CTA sum, its grid reduction, phase B (x, r, z), its CTA sum, its grid reduction, iterations]; clear != 0
  * zeroes the counters. */

@@ -6,7 +6,8 @@ checker over the `drape` command's gpu-<mode>/ files and the f64 oracle:
   rules_replayed_ok        Eisenstat-Walker forcing (<= 1e-5), the PTC controller, the rejections, and on probe
                            files alpha_max, resolution and line-search acceptance (e7_compare.rs:240-261)
   static_energy_ok         E_s rises by at most 1e-6 of max |E_s| between kept states (e7_compare.rs:100-104)
-  final_state_residual_ok  the final f32 state's f64 r/L <= max(1e-3, 2 x the oracle's floor) (e7_compare.rs:276-290)
+  final_state_residual_ok  the final f32 state's f64 r/L <= max(1e-3, 2 x the representation floor: r/L of the
+                           oracle's cold equilibrium rounded to f32) (e7_compare.rs:276-290)
   oracle_converged         the oracle's own run of the mode converged (its reference-<mode>.json), when present
   start_feasible           a warm or prolong run's start state lies outside the colliders (e7_compare.rs:145-156)
 and the diagnostics: energy gap and largest vertex gap against the oracle's cold equilibrium (e7_compare.rs:293-299),
@@ -104,6 +105,13 @@ def compare(case_dir, mode, oracle, start=None):
         verdict["oracle_converged"] = bool(ref["converged"]) and ref.get("mu_cap_steps", 0) == 0
         details["oracle"] = {k: ref.get(k) for k in ("converged", "ptc_steps", "newton_iterations", "rejected_attempts")}
         floor = ref.get("representation_floor", 0.0) or 0.0
+    cold_eq = os.path.join(case_dir, "equilibrium-cold")
+    if not floor and os.path.exists(cold_eq + ".json"):
+        # the representation floor: r/L of the oracle's own equilibrium rounded to f32 (the f32 state files hold no
+        # better), as the reference records it beside its cold solve
+        xr = _state(cold_eq).astype(np.float32).astype(np.float64)
+        floor = float(np.linalg.norm(oracle.static_gradient(xr)) / oracle.gravity_load)
+    details["representation_floor"] = floor
     verdict["final_state_residual_ok"] = r_over_l <= max(RESIDUAL_FLOOR_ALLOWANCE, FLOOR_FACTOR * floor)
     if start is not None:
         x0 = _state(start)
@@ -111,7 +119,6 @@ def compare(case_dir, mode, oracle, start=None):
         details["start_residual_over_load"] = float(np.linalg.norm(oracle.static_gradient(x0)) / oracle.gravity_load)
         details["start_min_distance_over_dhat"] = d0
         verdict["start_feasible"] = d0 > 0
-    cold_eq = os.path.join(case_dir, "equilibrium-cold")
     if os.path.exists(cold_eq + ".json"):
         xc = _state(cold_eq)
         e_c = oracle.static_energy(xc)

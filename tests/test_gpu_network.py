@@ -25,9 +25,9 @@ def _tuple(d, n, seed):
     log_h = d.final_h()
     x = d.state
     x_hat = x + log_h * log_h * np.tile([0.0, -9.81, 0.0], d.V)
-    d.set_options(api.default_options(tangent=1))
+    d.set_options(api.default_options(tangent=1, prolongation=0))
     g, blocks = d.assemble(x, x_hat=x_hat, h=log_h, mode=0, curvature=False)
-    d.set_options(api.default_options())
+    d.set_options(api.default_options(prolongation=0))
     rp, ci = oracle_py.Scene("sheet", n, seed=seed, plane=True).pattern()
     A = ml.bsr_matrix(rp, ci, blocks)
     b = -g
