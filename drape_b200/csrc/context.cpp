@@ -482,10 +482,18 @@ AttemptResult Context::newton(double h, double scale, double tolerance, int max_
         kcheck(launch_refine_residual(host_.R, row_ptr_.ptr, col_idx_.ptr, DevBsr{a0_.ptr, a1_.ptr, a2_.ptr}, g_.ptr,
                                      sol_.ptr, b_.ptr, partial_.ptr, kReduceGrid, stream_),
               "refine");
-        PcgResult pc = direction_solve(opt_.refine_rtol, opt_.pcg_max_iterations);
-        res.pcg_iterations += pc.iterations;
-        rec.pcg_iterations += pc.iterations;
-        if (pc.status != kPcgBreakdown) kcheck(launch_add_rows(host_.R, sol_.ptr, px_.ptr, stream_), "add");
+        // The correction solve on the f64 residual r = -g - A d stops once the direction meets its forcing target
+        // (|r| <= eta |g|) or r has fallen by refine_rtol, whichever comes first: it fixes what the f32 solve left
+        // above the target, and takes no iteration when the target already holds.
+        const double rn = std::sqrt(reduce_partials(kReduceGrid, 0, kRefine));
+        const double target = rn > 0.0 ? eta * norm / rn : 1.0;
+        const double rtol = std::max(opt_.refine_rtol, target);
+        if (rtol < 1.0) {
+          PcgResult pc = direction_solve(rtol, opt_.pcg_max_iterations);
+          res.pcg_iterations += pc.iterations;
+          rec.pcg_iterations += pc.iterations;
+          if (pc.status != kPcgBreakdown) kcheck(launch_add_rows(host_.R, sol_.ptr, px_.ptr, stream_), "add");
+        }
       }
       if (host_.R < host_.V)  // fixed vertices keep a zero direction
         check(cudaMemsetAsync(d_.ptr, 0, nv * sizeof(double), stream_), "memset");

@@ -208,16 +208,17 @@ __global__ void __launch_bounds__(32 * GalerkinShape<kSrcW>::kWarps) galerkin_ke
   const int nc = dst.n, nf = src.n, X = I % nc, Y = I / nc;
   GalerkinEntry* L = list[warp];
   // fine support row s = lane (lanes 0..8): its first entry and count
+  // (a stencil source reserves its w^2 slots for every support row, inside the grid or not, so row s's entries start
+  // at s w^2)
   int i = -1, first = 0, len = 0;
   if (lane < 9) {
     const int fx = 2 * X + lane % 3 - 1, fy = 2 * Y + lane / 3 - 1;
+    if (!kSrcBsr) len = kSrcW2;
     if (fx >= 0 && fy >= 0 && fx < nf && fy < nf) {
       i = fy * nf + fx;
       if (kSrcBsr) {
         first = fine.row_ptr[i];
         len = fine.row_ptr[i + 1] - first;
-      } else {
-        len = kSrcW2;
       }
     }
   }
@@ -261,21 +262,45 @@ __global__ void __launch_bounds__(32 * GalerkinShape<kSrcW>::kWarps) galerkin_ke
     }
   }
   __syncwarp();
+  const unsigned staged = __ballot_sync(0xffffffffu, lane < 9 && i >= 0);  // support rows inside the fine grid
   if (lane < kMgStencil) {
     double acc[9];
 #pragma unroll
     for (int e = 0; e < 9; ++e) acc[e] = 0.0;
     int J;
     if (stencil_neighbour(nc, 5, X, Y, lane, &J)) {
-      const int JX = J % nc, JY = J / nc;
-      for (int t = 0; t < total; ++t) {
-        const GalerkinEntry& E = L[t];
-        if (E.jx < 0) continue;
-        const double wj = w1d(E.jx, JX) * w1d(E.jy, JY);
-        if (wj == 0.0) continue;
-        const double w = E.w * wj;
+      if (kSrcBsr) {  // the fine row's entries are its BSR blocks: find the ones whose column J interpolates
+        const int JX = J % nc, JY = J / nc;
+        for (int t = 0; t < total; ++t) {
+          const GalerkinEntry& E = L[t];
+          if (E.jx < 0) continue;
+          const double wj = w1d(E.jx, JX) * w1d(E.jy, JY);
+          if (wj == 0.0) continue;
+          const double w = E.w * wj;
 #pragma unroll
-        for (int e = 0; e < 9; ++e) acc[e] += w * E.m[e];
+          for (int e = 0; e < 9; ++e) acc[e] += w * E.m[e];
+        }
+      } else {
+        // A stencil source's entry for fine support row i = 2I + a and column j = 2J + c sits at offset
+        // b = j - i = 2 (J - I) + c - a of row a's staged stencil: the (a, c) pairs enumerate the terms directly.
+        constexpr int h = kSrcW / 2;
+        const int dX = lane % 5 - 2, dY = lane / 5 - 2;
+        for (int sa = 0; sa < 9; ++sa) {
+          if (!((staged >> sa) & 1u)) continue;
+          const int ax = sa % 3 - 1, ay = sa / 3 - 1;
+          const double wa = (ax ? 0.5 : 1.0) * (ay ? 0.5 : 1.0);
+#pragma unroll
+          for (int sc = 0; sc < 9; ++sc) {
+            const int cx = sc % 3 - 1, cy = sc / 3 - 1;
+            const int bx = 2 * dX + cx - ax, by = 2 * dY + cy - ay;
+            if (bx < -h || bx > h || by < -h || by > h) continue;
+            const GalerkinEntry& E = L[sa * kSrcW2 + (by + h) * kSrcW + bx + h];
+            if (E.jx < 0) continue;  // column outside the fine grid
+            const double w = wa * (cx ? 0.5 : 1.0) * (cy ? 0.5 : 1.0);
+#pragma unroll
+            for (int e = 0; e < 9; ++e) acc[e] += w * E.m[e];
+          }
+        }
       }
     }
 #pragma unroll

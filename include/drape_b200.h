@@ -67,8 +67,11 @@ typedef struct {
   int32_t forcing;             /* 0: fixed pcg_rtol; 1: Eisenstat-Walker (e4_rules.rs:15-22) */
   int32_t replace_every;       /* PCG residual replacement period (0: never) */
   double replace_above;
-  int32_t refine;              /* 1: one f64 residual refinement of every Newton direction */
-  double refine_rtol;          /* relative tolerance of the refinement solve */
+  int32_t refine;              /* 1: one f64 residual refinement of every Newton direction: r = -g - A d in f64
+                                  and a correction solve on it */
+  double refine_rtol;          /* the correction solve stops once |r| <= eta |g| (the direction's forcing target)
+                                  or r has fallen by this factor, whichever comes first; no solve when the target
+                                  already holds */
   int32_t curvature;           /* 1: keep the barrier's b'(I - nn^T)/|x - c| Hessian term (not SPD) */
   int32_t preconditioner;      /* 0: block Jacobi (the reference's); 1: multilevel V-cycle over the structured grid with
                                   omega-Jacobi smoothing, in flexible PCG; 2: the same V-cycle with the fine-level

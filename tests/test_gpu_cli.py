@@ -131,7 +131,8 @@ def test_comparer_verdict_on_cold_and_prolong_runs():
         for n, c in ((17, c17), (33, c33)):
             subprocess.run([oracle_py.CLI, "e7-generate", "--n", str(n), "--edit", "base", "--out", c], check=True,
                            capture_output=True)
-        subprocess.run([oracle_py.CLI, "e7-solve", "--dir", c17, "--mode", "cold"], check=True, capture_output=True)
+        for c in (c17, c33):  # the oracle's cold references: its equilibrium gives the representation floor
+            subprocess.run([oracle_py.CLI, "e7-solve", "--dir", c, "--mode", "cold"], check=True, capture_output=True)
         _run("--case", c17, "--mode", "cold")
         o17 = oracle_py.Scene("reference", 17, edit="base")
         verdict, details = e7_compare.compare(c17, "cold", o17)
