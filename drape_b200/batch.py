@@ -15,7 +15,7 @@ from drape_b200 import api, batch_shards
 from drape_b200.scenes import batch_scenes
 
 
-def batch_workload(drapes, workers, budget, preconditioner, absolute=1e-6):
+def batch_workload(drapes, workers, budget, preconditioner, absolute=1e-6, forcing=1):
     """Every drape of the batched configuration solved cold to |grad E_s| <= `absolute`, `workers` at a time. Under
     torchrun (WORLD_SIZE > 1, one process per GPU) each rank solves its row-balanced share on its own GPU
     (drape_b200.batch_shards) and the ranks combine only their results; rank 0 returns the job's line."""
@@ -39,7 +39,7 @@ def batch_workload(drapes, workers, budget, preconditioner, absolute=1e-6):
         n, seed, radius, young = scenes[i]
         d = api.Drape.sheet(n, seed=seed, radius=radius, young=young, plane=True, device=local,
                             options=api.default_options(preconditioner=preconditioner, time_budget_s=budget,
-                                                        equilibrium_absolute=absolute))
+                                                        equilibrium_absolute=absolute, forcing=forcing))
         if net is not None:
             d.set_network(net)
         ds.append(d)
@@ -64,7 +64,8 @@ def batch_workload(drapes, workers, budget, preconditioner, absolute=1e-6):
         per_n[str(n)] = {"drapes": len(idx), "median_s": float(np.median(seconds_all[idx]))}
     solved = int(round(counts["solved"]))
     return {"workload": "batch", "drapes": drapes, "workers": workers, "n_gpus": world,
-            "preconditioner": preconditioner, "budget_s": budget, "tolerance_N": absolute, "solved": solved,
+            "preconditioner": preconditioner, "budget_s": budget, "tolerance_N": absolute,
+            "forcing": ["fixed rtol 1e-6", "eisenstat-walker"][forcing], "solved": solved,
             "total_s": total, "solves_per_s": solved / total if total > 0 else 0.0,
             "p50_s": float(np.percentile(seconds_all, 50)), "p99_s": float(np.percentile(seconds_all, 99)),
             "max_s": float(seconds_all.max()), "sum_device_s": counts["sum_device_s"],
@@ -81,11 +82,13 @@ def main(argv=None):
     ap.add_argument("--preconditioner", default="learned", choices=["jacobi", "multilevel", "learned"])
     ap.add_argument("--budget", type=float, default=0.0, help="the solver's own time budget per drape, s (0: none)")
     ap.add_argument("--absolute", type=float, default=1e-6, help="stop at |grad E_s| <= this (N)")
+    ap.add_argument("--forcing", type=int, default=1, choices=[0, 1],
+                    help="1 (default): Eisenstat-Walker forcing of the Newton directions; 0: fixed PCG rtol 1e-6")
     args = ap.parse_args(argv)
     # more hardware queues than the default 8, for streams of many drapes (read when CUDA starts)
     os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
     pre = {"jacobi": 0, "multilevel": 1, "learned": 2}[args.preconditioner]
-    out = batch_workload(args.drapes, args.workers, args.budget, pre, args.absolute)
+    out = batch_workload(args.drapes, args.workers, args.budget, pre, args.absolute, args.forcing)
     if int(os.environ.get("RANK", "0")) == 0:
         print(json.dumps(out), flush=True)
     return 0
