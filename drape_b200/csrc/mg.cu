@@ -1028,6 +1028,8 @@ struct DirectionArgs {
   const float* zrp_partial;
   int zr_count;
   float* pq_partial;
+  cudaGraphConditionalHandle cond;  // the solve graph's WHILE condition (fused update: this kernel ends the body)
+  int set_cond;                     // clear the condition once the solve is done
 };
 
 // beta (Polak-Ribiere form of flexible CG) = z.(r - r_prev) / rz_old;  p = z + beta p_old;  q = A p.
@@ -1055,7 +1057,10 @@ __global__ void __launch_bounds__(kRowThreads) direction_kernel(DirectionArgs a)
   const int iterations = st->iterations;
   const float rz_old = st->rz_old;
   pdl_wait();
-  if (st->done) return;
+  if (st->done) {
+    if (a.set_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(a.cond, 0);
+    return;
+  }
   const float zr = sum_partials(a.zr_partial, a.zr_count);
   const float zrp = sum_partials(a.zrp_partial, a.zr_count);
   const bool first = iterations == 0;
@@ -1084,6 +1089,7 @@ __global__ void __launch_bounds__(kRowThreads) direction_kernel(DirectionArgs a)
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     st->zr = zr;
     st->beta = beta;
+    st->has_direction = 1;  // update_restrict_kernel applies it
   }
 }
 
@@ -1231,6 +1237,124 @@ __global__ void __launch_bounds__(kRowThreads) update_residual_kernel(UpdateArgs
   }
 }
 
+// The update fused with the first restriction (bilinear prolongation, three or more restricted levels): at the start
+// of iteration k it applies iteration k-1's update and then restricts, one warp per coarse row I as restrict_kernel.
+// The warp stages the 7 x 7 fine window around 2I (the nine support rows and their columns): r' = r - alpha q (no
+// update at k = 0) and z_0 = S0 r' at every window vertex, recomputed by each coarse row that needs them (local
+// once alpha is known), so no CTA waits for another's update. The coarse row owns the fine rows 2I + (0|1, 0|1):
+// it writes their r', z_0 and x += alpha p and their |r'|^2 partial, which the next kernel (restrict_kernel<5,
+// true>) turns into the stopping test. Buffers: u.r_cur the residual of iteration k-1 (r at k = 0), u.r_next the
+// residual of iteration k, u.p the direction of iteration k-1 (at k = 0 the start leaves b in both residual buffers).
+__global__ void __launch_bounds__(kRestrictThreads) update_restrict_kernel(UpdateArgs u, RestrictArgs a) {
+  __shared__ float3 rn_s[kRestrictRows][49], z0_s[kRestrictRows][49];
+  MgState* st = u.state;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int I = blockIdx.x * kRestrictRows + warp;
+  const bool row_ok = I < a.dst.rows;
+  const int nc = a.dst.n, nf = a.src.n;
+  const int X = I % nc, Y = I / nc, cx = 2 * X, cy = 2 * Y;
+  const int s = lane / 3, k3 = lane % 3, ax = s % 3 - 1, by = s / 3 - 1;
+  const int fx = cx + ax, fy = cy + by;
+  const bool has_row = row_ok && lane < 27 && fx >= 0 && fy >= 0 && fx < nf && fy < nf;
+  const int i = has_row ? fy * nf + fx : 0;
+  const int it = st->iterations;  // updates so far (the previous fused kernel's, many kernels back)
+  // Before the wait: the support rows' structure and blocks, the window's r and S0, the owned rows' x, the coarse
+  // smoother; q, p and the partial p.q are the previous kernel's (the direction).
+  int jj[9];
+  int k0 = 0, k1 = 0;
+  if (has_row) {
+    k0 = a.fine.row_ptr[i] + k3;
+    k1 = a.fine.row_ptr[i + 1];
+  }
+#pragma unroll
+  for (int t = 0; t < 9; ++t) {
+    jj[t] = has_row && k0 + 3 * t < k1 ? a.fine.col_idx[k0 + 3 * t] : -1;
+    if (jj[t] >= 0) prefetch_block(a.fine.A, k0 + 3 * t);
+  }
+  int wv[2];
+  float3 rc[2], xo[2];
+  float sm0[2][9];
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const int w = lane + 32 * q, vx = cx + w % 7 - 3, vy = cy + w / 7 - 3;
+    wv[q] = row_ok && w < 49 && vx >= 0 && vy >= 0 && vx < nf && vy < nf ? vy * nf + vx : -1;
+    rc[q] = wv[q] >= 0 ? f3(u.r_cur[wv[q]]) : make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+    for (int e = 0; e < 9; ++e) sm0[q][e] = wv[q] >= 0 ? u.S0[e * u.R + wv[q]] : 0.0f;
+    const bool owned = wv[q] >= 0 && (w % 7 == 3 || w % 7 == 4) && (w / 7 == 3 || w / 7 == 4);
+    xo[q] = owned ? f3(u.x[wv[q]]) : make_float3(0.f, 0.f, 0.f);
+  }
+  float smd[9];
+  const bool writer = lane == 0 && row_ok && !a.coarsest;
+#pragma unroll
+  for (int e = 0; e < 9; ++e) smd[e] = writer ? a.dst.S[e * a.dst.rows + I] : 0.0f;
+  pdl_wait();
+  if (st->done) return;
+  // a direction exists once the first iteration's direction kernel has run
+  const bool update = st->has_direction != 0;
+  float alpha = 0.0f, pq = 0.0f, zr = 0.0f;
+  if (update) {
+    pq = sum_partials(u.pq_partial, u.pq_count);
+    zr = st->zr;
+    alpha = zr / pq;
+    if (!(pq > 0.0f) || !isfinite(alpha)) {
+      if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->pq = pq;
+        st->status = kStatusBreakdown;
+        st->done = 1;
+      }
+      return;
+    }
+  }
+  float rr = 0.0f;
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const int w = lane + 32 * q;
+    if (wv[q] < 0) continue;
+    const float3 rn = update ? sub3(rc[q], scale3(alpha, f3(u.q[wv[q]]))) : rc[q];
+    const float3 z0 = mul(sm0[q], rn);
+    rn_s[warp][w] = rn;
+    z0_s[warp][w] = z0;
+    if ((w % 7 == 3 || w % 7 == 4) && (w / 7 == 3 || w / 7 == 4)) {  // an owned fine row
+      if (update) {
+        u.r_next[wv[q]] = pack(rn);
+        u.x[wv[q]] = pack(add3(xo[q], scale3(alpha, f3(u.p[wv[q]]))));
+      }
+      u.z_pre[wv[q]] = pack(z0);
+      rr += dot3(rn, rn);
+    }
+  }
+  __syncwarp();
+  float3 t = make_float3(0.f, 0.f, 0.f);
+  if (has_row) {
+    float3 acc = make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      const int j = jj[q];
+      if (j < 0) continue;
+      const int w = (j / nf - cy + 3) * 7 + (j % nf - cx + 3);
+      float m[9];
+      load_block(a.fine.A, k0 + 3 * q, m);
+      acc = add3(acc, mul(m, z0_s[warp][w]));
+    }
+    const float wgt = (ax ? 0.5f : 1.0f) * (by ? 0.5f : 1.0f);
+    t = scale3(wgt, k3 == 0 ? sub3(rn_s[warp][(by + 3) * 7 + ax + 3], acc) : scale3(-1.0f, acc));
+  }
+  t = warp_sum3(t);
+  if (lane == 0 && row_ok) {
+    a.dst.r[I] = pack(t);
+    if (!a.coarsest) a.dst.z[I] = pack(mul(smd, t));
+  }
+  rr = cta_sum(rr);
+  if (threadIdx.x == 0) u.rr_partial[blockIdx.x] = rr;
+  if (update && blockIdx.x == 0 && threadIdx.x == 0) {
+    st->pq = pq;
+    st->alpha = alpha;
+    st->rz_old = zr;
+    st->iterations = it + 1;
+  }
+}
+
 struct InitArgs {
   int R;
   const float4* b;
@@ -1256,7 +1380,7 @@ __global__ void __launch_bounds__(kUpdateThreads) init_kernel(InitArgs a) {
     const float3 b = f3(a.b[i]);
     a.x[i] = zero;
     a.r0[i] = pack(b);
-    a.r1[i] = zero;
+    a.r1[i] = pack(b);  // the fused update-restriction reads the previous residual from here at the start
     a.p0[i] = zero;
     a.p1[i] = zero;
     a.z_pre[i] = pack(smooth(a.S0, a.R, i, b, false));
@@ -1286,7 +1410,11 @@ MgLevel level0(const MgDevice& d, int parity) {
 }
 
 // The V-cycle on level-0 right-hand side r[parity] with z_pre already in lv[0].z; result in lv[0].e.
-cudaError_t launch_cycle(const MgDevice& d, int parity, bool in_pcg, bool pdl, cudaStream_t s, int* launches) {
+// Inside flexible PCG with the bilinear prolongation and at least two restricted levels, `fused` (non-null) carries
+// the update of the previous iteration, which update_restrict_kernel applies with the first restriction; the
+// stopping test then moves to the second restriction.
+cudaError_t launch_cycle(const MgDevice& d, int parity, bool in_pcg, bool pdl, cudaStream_t s, int* launches,
+                         const UpdateArgs* fused = nullptr) {
   const int L = d.levels;
   MgState* st = in_pcg ? d.state : nullptr;
   const bool smoothed = d.smoothed != 0;
@@ -1326,9 +1454,12 @@ cudaError_t launch_cycle(const MgDevice& d, int parity, bool in_pcg, bool pdl, c
     a.coarsest = l + 2 == L;
     a.state = st;
     a.rr_partial = d.partial + kPartRr * kMgPartials;
-    a.rr_count = smoothed ? row_grid(d.fine.R) : update_grid(d.fine.R);  // the update's CTA count
+    // the update's CTA count (the fused update-restriction writes one slot per CTA of the first restriction)
+    a.rr_count = fused ? restrict_grid(d.lv[1].rows) : smoothed ? row_grid(d.fine.R) : update_grid(d.fine.R);
     const int grid = restrict_grid(a.dst.rows);
-    if (l == 0 && in_pcg) e = launch(restrict_kernel<0, true>, grid, kRestrictThreads, s, pdl, a);
+    if (l == 0 && fused) e = launch(update_restrict_kernel, grid, kRestrictThreads, s, pdl, *fused, a);
+    else if (l == 1 && fused) e = launch(restrict_kernel<5, true>, grid, kRestrictThreads, s, pdl, a);
+    else if (l == 0 && in_pcg) e = launch(restrict_kernel<0, true>, grid, kRestrictThreads, s, pdl, a);
     else if (l == 0) e = launch(restrict_kernel<0, false>, grid, kRestrictThreads, s, pdl, a);
     else if (a.src.w == 7) e = launch(restrict_kernel<7, false>, grid, kRestrictThreads, s, pdl, a);
     else e = launch(restrict_kernel<5, false>, grid, kRestrictThreads, s, pdl, a);
@@ -1597,8 +1728,24 @@ namespace {
 cudaError_t launch_body(const MgDevice& d, cudaGraphConditionalHandle cond, bool graph, bool pdl, cudaStream_t s,
                         int* launches) {
   const int R = d.fine.R;
+  // bilinear prolongation with two or more restricted levels: each iteration's update runs fused with the next
+  // iteration's first restriction (update_restrict_kernel), and the direction kernel ends the graph body
+  const bool fused = !d.smoothed && d.levels >= 4;
   for (int par = 0; par < 2; ++par) {
-    cudaError_t e = launch_cycle(d, par, true, pdl, s, launches);
+    UpdateArgs fa{};
+    fa.R = R;
+    fa.p = d.p[1 - par];
+    fa.q = d.q;
+    fa.r_cur = d.r[1 - par];
+    fa.r_next = d.r[par];
+    fa.x = d.x;
+    fa.S0 = d.lv[0].S;
+    fa.z_pre = d.lv[0].z;
+    fa.state = d.state;
+    fa.pq_partial = d.partial + kPartPq * kMgPartials;
+    fa.pq_count = row_grid(R);
+    fa.rr_partial = d.partial + kPartRr * kMgPartials;
+    cudaError_t e = launch_cycle(d, par, true, pdl, s, launches, fused ? &fa : nullptr);
     if (e != cudaSuccess) return e;
     DirectionArgs da{};
     da.fine = d.fine;
@@ -1611,7 +1758,14 @@ cudaError_t launch_body(const MgDevice& d, cudaGraphConditionalHandle cond, bool
     da.zrp_partial = d.partial + kPartZrPrev * kMgPartials;
     da.zr_count = row_grid(R);
     da.pq_partial = d.partial + kPartPq * kMgPartials;
+    da.cond = cond;
+    da.set_cond = fused && graph && par == 1;
     if ((e = launch(direction_kernel, row_grid(R), kRowThreads, s, pdl, da)) != cudaSuccess) return e;
+    if (fused) {
+      *launches += 1;
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+      continue;
+    }
     UpdateArgs ua{};
     ua.R = R;
     ua.p = d.p[par];

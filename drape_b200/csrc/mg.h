@@ -62,7 +62,8 @@ struct MgLevel {
 // while CTA 0 writes slot w & 1, so no CTA reads a word another CTA of the same kernel writes.
 struct MgState {
   float rr0, rr, zr, pq, alpha, beta, rz_old, tol2;
-  int iterations, status, done, max_iterations, stall_window, pad;
+  int iterations, status, done, max_iterations, stall_window;
+  int has_direction;  // set by the first direction kernel: the fused update-restriction has a direction to apply
   float stall_rr[2];
 };
 
