@@ -1,7 +1,8 @@
 """Extract the reference's stored known answers for the drape path into tests/golden/reference_values.json.
 
-Run once in a checkout that has the reference tree (the path is the first argument, default
-/root/reference); the JSON it writes is committed so the test suite never reads the reference tree.
+Run once where the reference tree is checked out, with its path as the one argument
+(`python tests/golden/make_golden.py <reference checkout>`); the JSON it writes is committed so the test suite never
+reads the reference tree.
 
 Sources (paths inside the reference project):
   experiments/cases/<kind>-n<N>/reference.json   E1 block-Jacobi PCG iteration counts, f64 and f32, the
@@ -55,4 +56,6 @@ def main(root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <reference checkout>")
+    main(sys.argv[1])
