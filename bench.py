@@ -9,8 +9,9 @@ residual at which the converged state lies within 1e-4 m of the f64 equilibrium;
 1e-6 N Newton tolerance is reported beside it ("secondary": the same run, read from its step records).
 Direction solver (--preconditioner): learned (default: the multilevel V-cycle flexible PCG with the shipped
 network's fine smoother), multilevel (spectral Jacobi smoothing), jacobi (the reference's block-Jacobi PCG).
---compare jacobi (default) adds one device-timed block-Jacobi solve of the same workload after the timed steps, the
-learned-vs-Jacobi comparison of the metric (all: also multilevel and learned; none: skip). Synthetic scene (the
+--compare all (default) adds one device-timed solve of the same workload with each other direction solver after the
+timed steps: block Jacobi (the learned-vs-Jacobi comparison of the metric) and the multilevel preconditioner without
+the network (what the network adds); jacobi: block Jacobi only; none: skip. Synthetic scene (the
 reference ships no dataset; seeded jitter, seed 0).
 
 value: seconds per converged solve with the problem resident in HBM (CUDA-event-timed solve, max over ranks).
@@ -593,7 +594,7 @@ def main():
                          "(run-e7.ts:22 forcing: true; e4_rules.rs:15-22); 0 a fixed PCG rtol 1e-6")
     ap.add_argument("--prolongation", type=int, default=0, choices=[0, 1],
                     help="multilevel fine-to-coarse prolongation: 0 bilinear (default), 1 smoothed once")
-    ap.add_argument("--compare", default="jacobi", choices=["none", "jacobi", "all"],
+    ap.add_argument("--compare", default="all", choices=["none", "jacobi", "all"],
                     help="after the timed steps, one device-timed solve of the same workload with each other solver")
     ap.add_argument("--probe", default=None, choices=["cycle", "network", "spmv", "solve"],
                     help="run one stand-alone profiling workload instead of the benchmark (see probe())")

@@ -1216,8 +1216,8 @@ Network::Network(int dev, uint64_t seed) : device(dev) {
   adam_m.alloc(kNnParams);
   adam_v.alloc(kNnParams);
   bf16.alloc(kNnBf16);
-  // Glorot-uniform weights from a 64-bit LCG, zero biases, a zero output layer (f = 0.976: the untrained network
-  // is just under the multilevel preconditioner's spectral smoother).
+  // Glorot-uniform weights from a 64-bit LCG, zero biases, a zero output layer (f = 0.916: the untrained network
+  // is a little under the multilevel preconditioner's spectral smoother).
   std::vector<float> p(kNnParams, 0.0f);
   uint64_t state = seed * 6364136223846793005ULL + 1442695040888963407ULL;
   auto uniform = [&]() {

@@ -328,8 +328,8 @@ drape_status drape_pcg_profile(drape_ctx* ctx, int64_t* out7, int32_t clear);
  * w_out[64] b_out. The file format is "DRAPENN1", an int32 count, then the f32 values (little-endian). */
 #define DRAPE_NETWORK_PARAMETERS 34177
 typedef struct drape_network drape_network;
-/* Glorot-uniform weights from `seed`, zero biases and a zero output layer (f = 0.976: the untrained network gives
- * just under the multilevel preconditioner's spectral smoother). */
+/* Glorot-uniform weights from `seed`, zero biases and a zero output layer (f = 0.916: the untrained network gives
+ * a little under the multilevel preconditioner's spectral smoother). */
 drape_status drape_network_create(int32_t device, uint64_t seed, drape_network** out);
 void drape_network_destroy(drape_network* net);
 drape_status drape_network_load(drape_network* net, const char* path);

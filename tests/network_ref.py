@@ -16,7 +16,7 @@ OFF_L0 = OFF_BIN + H
 OFF_WO = OFF_L0 + LAYERS * LAYER_SIZE
 OFF_BO = OFF_WO + H
 N_PARAMS = OFF_BO + 1
-SPAN, SHIFT = np.float32(0.5), np.float32(3.0)  # f = 0.5 + SPAN sigmoid(o + SHIFT) in (0.5, 1); f(0) = 0.976
+SPAN, SHIFT = np.float32(0.5), np.float32(1.6)  # f = 0.5 + SPAN sigmoid(o + SHIFT) in (0.5, 1); f(0) = 0.916
 
 
 def bf16(a):
