@@ -82,6 +82,9 @@ Context::Context(const HostProblem& problem, const drape_options& options, int d
   check(cudaSetDevice(device_), "cudaSetDevice");
   check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
   for (auto& e : ev_) check(cudaEventCreate(&e), "cudaEventCreate");
+  check(cudaStreamCreateWithFlags(&side_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  check(cudaEventCreateWithFlags(&setup_fork_, cudaEventDisableTiming), "cudaEventCreate");
+  check(cudaEventCreateWithFlags(&setup_join_, cudaEventDisableTiming), "cudaEventCreate");
   check(cudaMallocHost(&pinned_, kSlots * sizeof(double)), "cudaMallocHost");
   check(cudaMallocHost(&pinned_state_, sizeof(PcgSyncHeader)), "cudaMallocHost");
   check(cudaMallocHost(&pinned_mg_, sizeof(MgState) + 16), "cudaMallocHost");
@@ -90,13 +93,17 @@ Context::Context(const HostProblem& problem, const drape_options& options, int d
 
 Context::~Context() {
   if (stream_) cudaStreamSynchronize(stream_);
+  if (side_stream_) cudaStreamSynchronize(side_stream_);
   for (auto& e : ev_)
     if (e) cudaEventDestroy(e);
+  if (setup_fork_) cudaEventDestroy(setup_fork_);
+  if (setup_join_) cudaEventDestroy(setup_join_);
   if (sync_event_) cudaEventDestroy(sync_event_);
   if (pinned_) cudaFreeHost(pinned_);
   if (pinned_state_) cudaFreeHost(pinned_state_);
   if (pinned_mg_) cudaFreeHost(pinned_mg_);
   if (mg_graph_) cudaGraphExecDestroy(mg_graph_);
+  if (side_stream_) cudaStreamDestroy(side_stream_);
   if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -1069,7 +1076,7 @@ void Context::mg_prepare() {
   const float omega = opt_.smoother_omega > 0 ? float(opt_.smoother_omega) : 0.0f;  // 0: spectral damping
   const bool reuse = omega == 0.0f && mg_setups_since_power_ < 4;
   mg_setups_since_power_ = reuse ? mg_setups_since_power_ + 1 : 1;
-  kcheck(mg_setup(mg_, omega, true, reuse, stream_), "multilevel set-up");
+  kcheck(mg_setup(mg_, omega, true, reuse, stream_, side_stream_, setup_fork_, setup_join_), "multilevel set-up");
   // fine smoother, Galerkin products, coarse smoothers, coarsest inverse; the power method (twice with the
   // smoothed prolongation: the fine level first) and its scaling; Sp
   kernels_ += 2 * (mg_levels_ - 1) + (omega > 0 ? 0 : (reuse ? 0 : (kMgPowerSteps + 1) * (mg_.smoothed ? 2 : 1)) +
@@ -1080,6 +1087,8 @@ void Context::mg_prepare() {
     kcheck(nn_forward(nnb_, net_->view(), mg_.omega, mg_.lv[0].S, stream_), "preconditioner network");
     kernels_ += 2 + kNnLayers;  // features, input layer, message-passing layers, head
   }
+  // the coarsest inverse (side stream) before anything that follows on the main stream
+  check(cudaStreamWaitEvent(stream_, setup_join_, 0), "join");
   mg_stale_ = false;
 }
 

@@ -186,6 +186,10 @@ class Context {
   drape_options opt_;
   int device_ = 0;
   cudaStream_t stream_ = nullptr;
+  // the hierarchy set-up's second stream: the coarsest inverse runs there beside the smoother scaling and the
+  // network (fork after the last Galerkin product, join before the solve)
+  cudaStream_t side_stream_ = nullptr;
+  cudaEvent_t setup_fork_ = nullptr, setup_join_ = nullptr;
   cudaEvent_t sync_event_ = nullptr;  // set_blocking_sync's event (null: cudaStreamSynchronize)
   bool blocking_sync_ = false;
   DevProblem dp_{};

@@ -88,6 +88,7 @@ struct PcgArgs {
   long long spin_limit; // clock cycles a wait lasts before giving up
   long long* timing;    // optional [8]: CTA 0's cycles in phase A, its CTA sum, barrier A, phase B, CTA sum,
                         // barrier B, iterations (null: not recorded)
+  int bulk;             // stage the rows with bulk copies (set by launch_pcg when the planes are 16-byte aligned)
 };
 
 // One allocation per context, cleared before every launch: the result, the error flag, the broadcast words,
@@ -108,6 +109,9 @@ struct PcgLaunch {
 // Cooperative launch of the whole PCG solve; `cfg.grid` <= co-resident CTAs (see pcg_max_grid).
 cudaError_t launch_pcg(const PcgArgs& a, const PcgLaunch& cfg, cudaStream_t s);
 size_t pcg_smem_bytes(int cap_rows, int cap_blocks, bool matrix_in_smem);
+// Words of shared memory each 4-byte matrix plane (a2, column indices) takes: cap_blocks plus the up to 3 words
+// before a CTA's first block that a 16-byte aligned bulk copy brings along, rounded up to 16 bytes.
+__host__ __device__ inline int pcg_word_plane(int cap_blocks) { return ((cap_blocks + 3) & ~3) + 4; }
 int pcg_max_grid(int threads, int lanes_per_row, size_t smem, bool matrix_in_smem);
 
 // y = A p (f32 BSR times float4-per-row vector): the stand-alone SpMV of the roofline measurement.

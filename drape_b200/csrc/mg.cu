@@ -520,20 +520,20 @@ __global__ void __launch_bounds__(32 * kGsWarps, 3) galerkin_smoothed_kernel(MgF
   }
 }
 
-// Dense inverse of the coarsest operator by Gauss-Jordan elimination with partial pivoting (implicit row
-// exchanges), f64 in shared memory, one CTA. Step k: warp 0 picks the unused row p with the largest |M[p][k]|;
-// every row i != p subtracts (M[i][k] / M[p][k]) row p; row p is scaled by 1 / M[p][k]. Afterwards column k is
-// the unit vector at row perm[k], so row k of the inverse is row perm[k] of the right half.
+// Dense inverse of the coarsest operator by block Gauss-Jordan elimination over its 3x3 vertex blocks, f64 in shared
+// memory, one CTA. The operator is a Galerkin product of a symmetric positive definite matrix, so every pivot block
+// (a Schur complement's diagonal block) is symmetric positive definite and no pivoting is needed: step k inverts
+// the pivot block P = M[k][k] by its adjugate, scales block row k by P^{-1} and subtracts M[i][k] (block row k) from
+// every other block row i. Afterwards the right half holds the inverse. A pivot block whose determinant is not
+// positive and finite (the operator is not positive definite) sets *error, which hands the system to block-Jacobi
+// PCG. Two CTA barriers per block step (25 steps for the 75 x 75 operator of n = 5).
 __global__ void __launch_bounds__(1024) coarse_inverse_kernel(MgLevel lv, float* inv, int* error) {
   extern __shared__ double M[];  // [m][2m]
-  __shared__ double s_fac[3 * kMgCoarsestRowsMax];
-  __shared__ double s_row[6 * kMgCoarsestRowsMax];
-  __shared__ int s_used[3 * kMgCoarsestRowsMax], s_perm[3 * kMgCoarsestRowsMax];
-  __shared__ int s_piv;
+  __shared__ double s_row[3][6 * kMgCoarsestRowsMax];
+  __shared__ double s_fac[3 * kMgCoarsestRowsMax][3];
   const int m = 3 * lv.rows, w = 2 * m, n = lv.n;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, warps = blockDim.x >> 5;
   for (int t = threadIdx.x; t < m * w; t += blockDim.x) M[t] = 0.0;
-  for (int t = threadIdx.x; t < m; t += blockDim.x) s_used[t] = 0;
   __syncthreads();
   const int w2 = lv.w * lv.w;
   for (int t = threadIdx.x; t < lv.rows * w2; t += blockDim.x) {
@@ -544,49 +544,44 @@ __global__ void __launch_bounds__(1024) coarse_inverse_kernel(MgLevel lv, float*
   }
   for (int t = threadIdx.x; t < m; t += blockDim.x) M[t * w + m + t] = 1.0;
   __syncthreads();
-  for (int k = 0; k < m; ++k) {
-    if (warp == 0) {
-      double best = -1.0;
-      int piv = -1;
-      for (int i = lane; i < m; i += 32)
-        if (!s_used[i]) {
-          const double v = fabs(M[i * w + k]);
-          if (v > best) best = v, piv = i;
-        }
-#pragma unroll
-      for (int o = 16; o; o >>= 1) {
-        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-        const int op = __shfl_xor_sync(0xffffffffu, piv, o);
-        if (ob > best || (ob == best && op >= 0 && (piv < 0 || op < piv))) best = ob, piv = op;
-      }
-      if (lane == 0) {
-        if (piv < 0 || !(best > 0.0) || !isfinite(best)) {
-          *error = 1;
-          piv = piv < 0 ? k : piv;
-        }
-        s_piv = piv;
-        s_used[piv] = 1;
-        s_perm[k] = piv;
-      }
+  for (int k = 0; k < lv.rows; ++k) {
+    const int kb = 3 * k;
+    // Columns left of kb are eliminated (unit columns) and right-half columns past m + kb + 2 are still unit
+    // columns with zeros in block row k, so the step touches columns kb .. m + kb + 2 only.
+    const int c_end = m + kb + 3;
+    // P^{-1} by the adjugate, in every thread (nine broadcast reads)
+    const double a = M[kb * w + kb], b = M[kb * w + kb + 1], c = M[kb * w + kb + 2];
+    const double d = M[(kb + 1) * w + kb], e = M[(kb + 1) * w + kb + 1], f = M[(kb + 1) * w + kb + 2];
+    const double g = M[(kb + 2) * w + kb], h = M[(kb + 2) * w + kb + 1], i9 = M[(kb + 2) * w + kb + 2];
+    const double c00 = e * i9 - f * h, c01 = c * h - b * i9, c02 = b * f - c * e;
+    const double c10 = f * g - d * i9, c11 = a * i9 - c * g, c12 = c * d - a * f;
+    const double c20 = d * h - e * g, c21 = b * g - a * h, c22 = a * e - b * d;
+    const double det = a * c00 + b * c10 + c * c20;
+    const bool ok = det > 0.0 && isfinite(det);
+    if (!ok && threadIdx.x == 0) *error = 1;
+    const double rd = ok ? 1.0 / det : 0.0;
+    for (int t = threadIdx.x; t < 3 * (c_end - kb); t += blockDim.x) {
+      const int r = t / (c_end - kb), col = kb + t % (c_end - kb);
+      const double p0 = r == 0 ? c00 : r == 1 ? c10 : c20;  // row r of P^{-1} (times det)
+      const double p1 = r == 0 ? c01 : r == 1 ? c11 : c21;
+      const double p2 = r == 0 ? c02 : r == 1 ? c12 : c22;
+      s_row[r][col] = rd * (p0 * M[kb * w + col] + p1 * M[(kb + 1) * w + col] + p2 * M[(kb + 2) * w + col]);
+    }
+    for (int t = threadIdx.x; t < 3 * m; t += blockDim.x) {
+      const int r = t / 3, q = t % 3;
+      s_fac[r][q] = r >= kb && r < kb + 3 ? 0.0 : M[r * w + kb + q];
     }
     __syncthreads();
-    const int p = s_piv;
-    const double d = M[p * w + k];
-    const double rd = d != 0.0 ? 1.0 / d : 0.0;
-    // Columns left of k are already eliminated: zero in the pivot row, so no row changes there. Only columns
-    // k .. 2m - 1 are touched (rows by warp, columns by lane).
-    for (int c = k + threadIdx.x; c < w; c += blockDim.x) s_row[c] = M[p * w + c] * rd;
-    for (int i = threadIdx.x; i < m; i += blockDim.x) s_fac[i] = i == p ? 0.0 : M[i * w + k];
-    __syncthreads();
-    const int warps = blockDim.x >> 5;
-    for (int i = warp; i < m; i += warps) {
-      double* row = M + i * w;
-      const double f = s_fac[i];
-      for (int c = k + lane; c < w; c += 32) row[c] = i == p ? s_row[c] : row[c] - f * s_row[c];
+    for (int r = warp; r < m; r += warps) {
+      double* row = M + r * w;
+      const bool pivot_row = r >= kb && r < kb + 3;
+      const double f0 = s_fac[r][0], f1 = s_fac[r][1], f2 = s_fac[r][2];
+      for (int col = kb + lane; col < c_end; col += 32)
+        row[col] = pivot_row ? s_row[r - kb][col] : row[col] - (f0 * s_row[0][col] + f1 * s_row[1][col] + f2 * s_row[2][col]);
     }
     __syncthreads();
   }
-  for (int t = threadIdx.x; t < m * m; t += blockDim.x) inv[t] = float(M[s_perm[t / m] * w + m + t % m]);
+  for (int t = threadIdx.x; t < m * m; t += blockDim.x) inv[t] = float(M[(t / m) * w + m + t % m]);
 }
 
 // ---------------------------------------------------------------------------------------------- the cycle
@@ -1635,7 +1630,8 @@ cudaError_t power_method(const MgDevice& d, int first, int end, cudaStream_t s) 
 
 }  // namespace
 
-cudaError_t mg_setup(const MgDevice& d, float omega, bool fine_smoother, bool reuse_omega, cudaStream_t s) {
+cudaError_t mg_setup(const MgDevice& d, float omega, bool fine_smoother, bool reuse_omega, cudaStream_t s,
+                     cudaStream_t side, cudaEvent_t fork, cudaEvent_t join) {
   if (d.levels < 2) return cudaErrorInvalidValue;
   cudaError_t e;
   const int first = fine_smoother ? 0 : 1, end = d.levels - 1;  // smoothed levels
@@ -1669,6 +1665,26 @@ cudaError_t mg_setup(const MgDevice& d, float omega, bool fine_smoother, bool re
       jacobi_smoother_kernel<false><<<(c.rows + 255) / 256, 256, 0, s>>>(d.fine, c, fixed);
     }
   }
+  {  // the coarsest inverse needs only the last Galerkin product
+    const MgLevel& top = d.lv[d.levels - 1];
+    const int m = 3 * top.rows;
+    const size_t smem = size_t(m) * 2 * m * sizeof(double);
+    // The ceiling is one process-wide setting: the largest coarsest level's size for every call, so that
+    // concurrent set-ups of different hierarchies never lower it under another's launch.
+    constexpr int kCoarseSmemMax = 3 * kMgCoarsestRowsMax * 2 * 3 * kMgCoarsestRowsMax * int(sizeof(double));
+    if ((e = cudaFuncSetAttribute(coarse_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kCoarseSmemMax)) != cudaSuccess)
+      return e;
+    cudaStream_t inv_stream = s;
+    if (side) {
+      if ((e = cudaEventRecord(fork, s)) != cudaSuccess || (e = cudaStreamWaitEvent(side, fork, 0)) != cudaSuccess)
+        return e;
+      inv_stream = side;
+    }
+    coarse_inverse_kernel<<<1, 1024, smem, inv_stream>>>(top, d.coarse_inv, d.error);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (side && (e = cudaEventRecord(join, side)) != cudaSuccess) return e;
+  }
   if (spectral) {
     // without the smoothed prolongation every smoothed level in one power method; with it, the rest
     const int from = d.smoothed && first == 0 ? 1 : first;
@@ -1678,16 +1694,6 @@ cudaError_t mg_setup(const MgDevice& d, float omega, bool fine_smoother, bool re
       scale_smoother_kernel<<<(count + 255) / 256, 256, 0, s>>>(d.lv[l].S, count, d.omega + l);
     }
   }
-  const MgLevel& top = d.lv[d.levels - 1];
-  const int m = 3 * top.rows;
-  const size_t smem = size_t(m) * 2 * m * sizeof(double);
-  // The ceiling is one process-wide setting: the largest coarsest level's size for every call, so that concurrent
-  // set-ups of different hierarchies never lower it under another's launch.
-  constexpr int kCoarseSmemMax = 3 * kMgCoarsestRowsMax * 2 * 3 * kMgCoarsestRowsMax * int(sizeof(double));
-  if ((e = cudaFuncSetAttribute(coarse_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kCoarseSmemMax)) !=
-      cudaSuccess)
-    return e;
-  coarse_inverse_kernel<<<1, 1024, smem, s>>>(top, d.coarse_inv, d.error);
   return cudaGetLastError();
 }
 

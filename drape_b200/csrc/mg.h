@@ -113,8 +113,12 @@ int mg_level_count(int n);
 // the highest modes; the sheet drape's fine level has lambda ~ 3.4, so a fixed 0.6 is already unstable there.
 // `reuse_omega` skips the power method and scales by the omega_l of the last one (systems of one PTC attempt
 // change little from one Newton update to the next).
+// With a `side` stream the coarsest inverse runs there, after `fork` (recorded on s behind the last Galerkin
+// product), and `join` is recorded behind it: the caller makes s wait for `join` before the cycle reads the inverse,
+// so that the smoother scaling and whatever the caller queues next (the network) overlap the inverse.
 constexpr int kMgPowerSteps = 10;
-cudaError_t mg_setup(const MgDevice& d, float omega, bool fine_smoother, bool reuse_omega, cudaStream_t s);
+cudaError_t mg_setup(const MgDevice& d, float omega, bool fine_smoother, bool reuse_omega, cudaStream_t s,
+                     cudaStream_t side = nullptr, cudaEvent_t fork = nullptr, cudaEvent_t join = nullptr);
 
 // Flexible PCG: clear the state and start from x = 0, r = b.
 cudaError_t mg_pcg_init(const MgDevice& d, float tol2, int max_iterations, int stall_window, cudaStream_t s);

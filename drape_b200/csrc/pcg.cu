@@ -20,6 +20,8 @@
 // update_dot, direction, reduce, residual.
 #include <cuda_runtime.h>
 
+#include <cstdint>
+
 #include "kernels.h"
 
 namespace drape {
@@ -123,6 +125,41 @@ __device__ __forceinline__ void group_reduce(float& y0, float& y1, float& y2) {
   }
 }
 
+// Bulk global->shared copies (cp.async.bulk, the TMA engine's untiled form) completing on a CTA mbarrier.
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+// Orders the generic-proxy initialisation of the barrier before the async proxy's use of it.
+__device__ __forceinline__ void fence_proxy_async_shared() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+// dst and src 16-byte aligned, bytes a multiple of 16 (the instruction's rules; the callers guarantee them).
+__device__ __forceinline__ void bulk_copy_g2s(unsigned dst, const void* src, unsigned bytes, unsigned bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               ::"r"(dst), "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+// Polls the barrier's phase `parity` for at most `limit` clock cycles; true when the phase completed.
+__device__ __forceinline__ bool mbar_wait_parity(unsigned bar, unsigned parity, long long limit) {
+  const long long t0 = clock64();
+  while (true) {
+    unsigned done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (clock64() - t0 > limit) return false;
+  }
+}
+
 __device__ __forceinline__ void apply(float4 m0, float4 m1, float m8, float4 p, float& y0, float& y1, float& y2) {
   y0 += m0.x * p.x + m0.y * p.y + m0.z * p.z;
   y1 += m0.w * p.x + m1.x * p.y + m1.y * p.z;
@@ -144,22 +181,61 @@ __global__ void __launch_bounds__(1024) pcg_kernel(PcgArgs a) {
   float4* qs = ps + cap;
   float4* bs = qs + cap;
   float4* dv = bs + cap;  // 3 per row
+  // The 4-byte planes (a2, column indices) hold cap_blocks + 4 words rounded up to 16 bytes: block kb0 + k sits at
+  // word (kb0 & 3) + k, so that a bulk copy starting at the 16-byte boundary below kb0 lands on a 16-byte boundary.
+  const int cw = MSMEM ? pcg_word_plane(a.cap_blocks) : 0, sh = kb0 & 3;
   float4* m0s = dv + 3 * cap;
   float4* m1s = m0s + (MSMEM ? a.cap_blocks : 0);
-  float* m8s = reinterpret_cast<float*>(m1s + (MSMEM ? a.cap_blocks : 0));
-  int* cols = reinterpret_cast<int*>(m8s + (MSMEM ? a.cap_blocks : 0));
-  int* rp = cols + (MSMEM ? a.cap_blocks : 0);  // n + 1 local row offsets
+  float* m8b = reinterpret_cast<float*>(m1s + (MSMEM ? a.cap_blocks : 0));
+  int* colb = reinterpret_cast<int*>(m8b + cw);
+  int* rp = colb + cw;  // n + 1 local row offsets
+  float* m8s = m8b + sh;
+  int* cols = colb + sh;
 
-  // ---- stage the CTA's rows
+  // ---- stage the CTA's rows: one bulk copy (TMA, cp.async.bulk) per plane, completing on an mbarrier. The a0/a1
+  // planes are 16-byte blocks; the 4-byte planes copy whole 16-byte words from the boundary at or below kb0 and
+  // load the last (s + nb) % 4 words plainly. Without 16-byte aligned planes the rows are loaded plainly.
+  __shared__ __align__(8) unsigned long long stage_bar;
+  const bool bulk = MSMEM && a.bulk && nb > 0;
+  const unsigned bar = smem_addr(&stage_bar);
+  const int words = (sh + nb) & ~3;  // words of each 4-byte plane the bulk copy moves
+  if (bulk && threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    fence_proxy_async_shared();
+    mbar_arrive_expect_tx(bar, 32u * unsigned(nb) + 8u * unsigned(words));
+    bulk_copy_g2s(smem_addr(m0s), a.A.a0 + kb0, 16u * unsigned(nb), bar);
+    bulk_copy_g2s(smem_addr(m1s), a.A.a1 + kb0, 16u * unsigned(nb), bar);
+    if (words > 0) {
+      bulk_copy_g2s(smem_addr(m8b), a.A.a2 + (kb0 - sh), 4u * unsigned(words), bar);
+      bulk_copy_g2s(smem_addr(colb), a.col_idx + (kb0 - sh), 4u * unsigned(words), bar);
+    }
+  }
   for (int i = threadIdx.x; i <= n; i += blockDim.x) rp[i] = a.row_ptr[r0 + i] - kb0;
-  if (MSMEM)
+  if (bulk) {
+    for (int j = words + threadIdx.x; j < sh + nb; j += blockDim.x) {
+      m8b[j] = a.A.a2[kb0 - sh + j];
+      colb[j] = a.col_idx[kb0 - sh + j];
+    }
+  } else if (MSMEM) {
     for (int k = threadIdx.x; k < nb; k += blockDim.x) {
       m0s[k] = a.A.a0[kb0 + k];
       m1s[k] = a.A.a1[kb0 + k];
       m8s[k] = a.A.a2[kb0 + k];
       cols[k] = a.col_idx[kb0 + k];
     }
+  }
   __syncthreads();
+  if (bulk) {
+    // Every thread waits for the copies' bytes (phase 0 of the barrier), at most spin_limit cycles. A CTA whose
+    // copies did not land sets the error flag, waits once more for them to drain and returns; the other CTAs then
+    // give up at their first reduce barrier.
+    const bool landed = mbar_wait_parity(bar, 0, a.spin_limit);
+    if (__syncthreads_or(!landed)) {
+      if (threadIdx.x == 0) atomicExch(a.error, 1);
+      mbar_wait_parity(bar, 0, a.spin_limit);
+      return;
+    }
+  }
   // ---- setup: D^-1 (adjugate, pcg.rs:479-492), x = 0, r = b, z = D^-1 r, p = z; partial r.z, r.r
   float acc[2] = {0.0f, 0.0f};
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -487,7 +563,8 @@ cudaError_t allow_dynamic_smem(const void* fn) {
 }  // namespace
 
 size_t pcg_smem_bytes(int cap_rows, int cap_blocks, bool msmem) {
-  return size_t(cap_rows) * (6 * 16 + 3 * 16) + (msmem ? size_t(cap_blocks) * (16 + 16 + 4 + 4) : 0) +
+  return size_t(cap_rows) * (6 * 16 + 3 * 16) +
+         (msmem ? size_t(cap_blocks) * (16 + 16) + size_t(pcg_word_plane(cap_blocks)) * (4 + 4) : 0) +
          size_t(cap_rows + 1) * 4;
 }
 
@@ -508,6 +585,8 @@ cudaError_t launch_pcg(const PcgArgs& a, const PcgLaunch& cfg, cudaStream_t s) {
   cudaError_t e = allow_dynamic_smem(fn);
   if (e != cudaSuccess) return e;
   PcgArgs args = a;
+  const auto aligned = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
+  args.bulk = cfg.matrix_in_smem && aligned(a.A.a0) && aligned(a.A.a1) && aligned(a.A.a2) && aligned(a.col_idx);
   void* params[] = {&args};
   return cudaLaunchCooperativeKernel(fn, dim3(cfg.grid), dim3(cfg.threads), params, cfg.smem, s);
 }
