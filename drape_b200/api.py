@@ -38,7 +38,7 @@ class Options(ctypes.Structure):
         ("max_halvings", ctypes.c_int32), ("time_budget_s", ctypes.c_double), ("pcg_grid", ctypes.c_int32),
         ("pcg_threads", ctypes.c_int32), ("pcg_lanes", ctypes.c_int32), ("progress", ctypes.c_int32),
         ("newton_start", ctypes.c_int32), ("tangent", ctypes.c_int32), ("smoother_omega", ctypes.c_double),
-        ("prolongation", ctypes.c_int32), ("pad_options", ctypes.c_int32),
+        ("prolongation", ctypes.c_int32), ("pcg_single_reduction", ctypes.c_int32),
     ]
 
 

@@ -101,6 +101,7 @@ void drape_default_options(drape_options* o) {
   o->max_halvings = 30;
   o->time_budget_s = 0.0;
   o->prolongation = 0;
+  o->pcg_single_reduction = 1;
 }
 
 drape_status drape_create(const drape_problem_view* v, const drape_options* options, int32_t device, drape_ctx** out) {

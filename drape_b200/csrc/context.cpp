@@ -268,9 +268,11 @@ void Context::configure_pcg() {
       cap_rows = std::max(cap_rows, r1 - r0);
       cap_blocks = std::max(cap_blocks, host_.row_ptr[r1] - host_.row_ptr[r0]);
     }
-    c.matrix_in_smem = pcg_smem_bytes(cap_rows, cap_blocks, true) <= 200 * 1024;
-    c.smem = pcg_smem_bytes(cap_rows, cap_blocks, c.matrix_in_smem);
-    const int fit = pcg_max_grid(c.threads, c.lanes_per_row, c.smem, c.matrix_in_smem);
+    // sized for the single-reduction form (three more row vectors), which the two-reduction form fits in too
+    c.matrix_in_smem = pcg_smem_bytes(cap_rows, cap_blocks, true, true) <= 200 * 1024;
+    c.smem = pcg_smem_bytes(cap_rows, cap_blocks, c.matrix_in_smem, true);
+    const int fit = std::min(pcg_max_grid(c.threads, c.lanes_per_row, c.smem, c.matrix_in_smem, true),
+                             pcg_max_grid(c.threads, c.lanes_per_row, c.smem, c.matrix_in_smem, false));
     if (fit <= 0) throw std::invalid_argument("the PCG rows of one CTA do not fit in shared memory");
     if (grid <= fit) {
       c.grid = grid;
@@ -281,7 +283,7 @@ void Context::configure_pcg() {
     grid = fit;
   }
   pcg_cfg_ = c;
-  pcg_sync_.alloc((sizeof(PcgSyncHeader) + 32 * size_t(c.grid) + 7) / 8);  // 2 parities x 2 words x grid
+  pcg_sync_.alloc((sizeof(PcgSyncHeader) + 80 * size_t(c.grid) + 7) / 8);  // 2 parities x 5 words x grid
   pcg_timing_.alloc(8);
   check(cudaMemsetAsync(pcg_timing_.ptr, 0, 8 * sizeof(long long), stream_), "memset");
 }
@@ -369,9 +371,19 @@ PcgResult Context::pcg(double rtol, int max_iterations) {
   a.replace_above2 = float(opt_.replace_above * opt_.replace_above);
   a.spin_limit = 4000000000LL;  // ~2 s of SM clock per wait
   a.timing = pcg_timing_.ptr;
+  PcgLaunch cfg = pcg_cfg_;
+  cfg.single_reduction = opt_.pcg_single_reduction != 0 && opt_.replace_every == 0;
+  if (cfg.single_reduction) {
+    if (pmw_[0].n < size_t(host_.R))
+      for (auto* v : {&pmw_[0], &pmw_[1], &pms_[0], &pms_[1]}) v->alloc(host_.R);
+    a.mw[0] = pmw_[0].ptr;
+    a.mw[1] = pmw_[1].ptr;
+    a.ms[0] = pms_[0].ptr;
+    a.ms[1] = pms_[1].ptr;
+  }
   check(cudaMemsetAsync(pcg_sync_.ptr, 0, pcg_sync_.n * sizeof(unsigned long long), stream_), "memset");
   check(cudaEventRecord(ev_[0], stream_), "event");
-  kcheck(launch_pcg(a, pcg_cfg_, stream_), "pcg launch");
+  kcheck(launch_pcg(a, cfg, stream_), "pcg launch");
   check(cudaEventRecord(ev_[1], stream_), "event");
   check(cudaMemcpyAsync(pinned_state_, pcg_sync_.ptr, sizeof(PcgSyncHeader), cudaMemcpyDeviceToHost, stream_), "read");
   sync();

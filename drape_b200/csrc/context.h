@@ -264,6 +264,7 @@ class Context {
   DeviceArray<float4> a0_, a1_;
   DeviceArray<float> a2_;
   DeviceArray<float4> b_, px_, pz_, pp0_, pp1_, pq_, sol_, corr_;
+  DeviceArray<float4> pmw_[2], pms_[2];  // the single-reduction PCG's published M w and M s
   DeviceArray<unsigned long long> pcg_sync_;  // PcgSyncHeader + 2 * grid partial words
   double* pinned_ = nullptr;
   PcgSyncHeader* pinned_state_ = nullptr;

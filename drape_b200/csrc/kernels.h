@@ -76,7 +76,7 @@ struct PcgArgs {
   float4* z;            // published z (gathered by the fused direction update)
   float4* p0;           // published p, double-buffered
   float4* p1;
-  unsigned long long* slots;  // [2 parities][2 values][grid] per-CTA (generation, partial) words
+  unsigned long long* slots;  // [2 parities][2 values; 5 single-reduction][grid] (generation, partial) words
   unsigned long long* bcast;  // unused (kept for the layout of PcgSyncHeader)
   int* error;           // set when a wait gave up (the kernel returned early)
   PcgState* state;
@@ -89,6 +89,9 @@ struct PcgArgs {
   long long* timing;    // optional [8]: CTA 0's cycles in phase A, its CTA sum, barrier A, phase B, CTA sum,
                         // barrier B, iterations (null: not recorded)
   int bulk;             // stage the rows with bulk copies (set by launch_pcg when the planes are 16-byte aligned)
+  // single-reduction form only: published M w and M s, double-buffered (p0 / p1 carry u)
+  float4* mw[2];
+  float4* ms[2];
 };
 
 // One allocation per context, cleared before every launch: the result, the error flag, the broadcast words,
@@ -103,16 +106,17 @@ struct PcgSyncHeader {
 struct PcgLaunch {
   int grid = 0, threads = 1024, lanes_per_row = 8;
   bool matrix_in_smem = true;
+  bool single_reduction = false;  // one grid reduction per iteration (needs PcgArgs::mw, ms; no replacement)
   size_t smem = 0;
 };
 
 // Cooperative launch of the whole PCG solve; `cfg.grid` <= co-resident CTAs (see pcg_max_grid).
 cudaError_t launch_pcg(const PcgArgs& a, const PcgLaunch& cfg, cudaStream_t s);
-size_t pcg_smem_bytes(int cap_rows, int cap_blocks, bool matrix_in_smem);
+size_t pcg_smem_bytes(int cap_rows, int cap_blocks, bool matrix_in_smem, bool single_reduction = false);
 // Words of shared memory each 4-byte matrix plane (a2, column indices) takes: cap_blocks plus the up to 3 words
 // before a CTA's first block that a 16-byte aligned bulk copy brings along, rounded up to 16 bytes.
 __host__ __device__ inline int pcg_word_plane(int cap_blocks) { return ((cap_blocks + 3) & ~3) + 4; }
-int pcg_max_grid(int threads, int lanes_per_row, size_t smem, bool matrix_in_smem);
+int pcg_max_grid(int threads, int lanes_per_row, size_t smem, bool matrix_in_smem, bool single_reduction = false);
 
 // y = A p (f32 BSR times float4-per-row vector): the stand-alone SpMV of the roofline measurement.
 cudaError_t launch_spmv(int R, const int* row_ptr, const int* col_idx, DevBsr A, const float4* p, float4* y,

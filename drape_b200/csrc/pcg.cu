@@ -13,8 +13,10 @@
 // fixed order and publishes (generation, total) words that every CTA waits for. No atomics, so every CTA takes
 // the same alpha, beta and stop decision and the solve is deterministic; every wait gives up after `spin_limit`
 // cycles, sets `*error` and the kernel returns, so a stalled launch cannot hang the GPU.
+// That is the reference's two-reduction iteration; the default form (SINGLE, see pcg_kernel) takes one phase and one
+// reduce barrier per iteration through the Chronopoulos-Gear recurrences.
 // Residual replacement (r = b - A x every `replace_every` iterations while rr > replace_above^2 rr0, keeping p)
-// follows pcg.rs:213-223. Block rows are processed by groups of LPR lanes with xor-shuffle reductions; every row
+// follows pcg.rs:213-223 (two-reduction form only). Block rows are processed by groups of LPR lanes with xor-shuffle reductions; every row
 // loop has a CTA-uniform trip count so all lanes reach the shuffles.
 // Reference semantics: pcg.rs:271-296 (solve), 389-439 (State), 479-492 (invert3); WGSL cg_init, spmv_dot,
 // update_dot, direction, reduce, residual.
@@ -29,6 +31,10 @@ namespace {
 
 __device__ __forceinline__ float4 f4(float a, float b, float c) { return make_float4(a, b, c, 0.0f); }
 __device__ __forceinline__ float dot3(float4 a, float4 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+// s a + b per component, rounded once (the same bits wherever it is evaluated)
+__device__ __forceinline__ float4 fma4(float s, float4 a, float4 b) {
+  return f4(__fmaf_rn(s, a.x, b.x), __fmaf_rn(s, a.y, b.y), __fmaf_rn(s, a.z, b.z));
+}
 __device__ __forceinline__ unsigned long long pack(unsigned gen, float v) {
   return (static_cast<unsigned long long>(gen) << 32) | __float_as_uint(v);
 }
@@ -69,13 +75,16 @@ __device__ __forceinline__ unsigned long long load_acquire(const unsigned long l
 // thread's earlier stores of published vectors); thread t of every CTA acquire-polls CTA t's words (all words in
 // parallel, blockDim.x >= gridDim.x, host-checked); every CTA then sums the words in the same fixed order.
 // Words alternate between two buffers by generation parity: a CTA can only rewrite a buffer after every CTA has
-// published the next generation, i.e. after every CTA has read this one.
-template <int NV> __device__ __forceinline__ bool reduce_barrier(const PcgArgs& a, unsigned gen, float* vals) {
+// published the next generation, i.e. after every CTA has read this one. Each parity holds STRIDE values per CTA
+// (2 for the two-reduction iteration, 3 for the single-reduction one).
+template <int NV, int STRIDE = 2>
+__device__ __forceinline__ bool reduce_barrier(const PcgArgs& a, unsigned gen, float* vals) {
+  static_assert(NV <= STRIDE, "more values than slots");
   __shared__ float words[NV][1024];
-  __shared__ float totals[2];
+  __shared__ float totals[NV];
   __shared__ int bad;
   const unsigned G = gridDim.x;
-  unsigned long long* slots = a.slots + (gen & 1u) * 2u * G;
+  unsigned long long* slots = a.slots + (gen & 1u) * unsigned(STRIDE) * G;
   if (threadIdx.x == 0) {
     bad = 0;
 #pragma unroll
@@ -166,7 +175,22 @@ __device__ __forceinline__ void apply(float4 m0, float4 m1, float m8, float4 p, 
   y2 += m1.z * p.x + m1.w * p.y + m8 * p.z;
 }
 
-template <int LPR, bool MSMEM>
+// The single-reduction iteration (SINGLE, Chronopoulos-Gear PCG: A. T. Chronopoulos and C. W. Gear, J. Comput.
+// Appl. Math. 25 (1989) 153-168) carries w = A u and s = A p (a recurrence), so that one grid reduction per
+// iteration gives every dot product the next step needs:
+//   s = w + beta s, p = u + beta p, x += alpha p, r -= alpha s, u = M r,
+//   w = A u;  gamma = r.u, delta = w.u, rho = r.r, u.s + p.w, p.s  (one reduce barrier);
+//   beta = gamma / gamma_old, p.A p = delta + beta (u.s + p.w) + beta^2 p.s, alpha = gamma / p.A p.
+// (Chronopoulos and Gear take p.A p = delta - beta gamma / alpha_old, which assumes exact orthogonality and broke
+// down in f32 on the reference's tension system after ~100 iterations; the expansion over the current vectors does
+// not.)
+// The SpMV runs in the same phase that forms u, so a CTA forms the u of each gathered column itself, from what
+// the column's owner published in the previous iteration: u_old = M r_old, M w_old and M s_older, as
+// u_old - alpha (M w_old + beta M s_older) (= M r in exact arithmetic; one step's rounding away from the owner's
+// M r, which the owner recomputes directly every iteration, so the difference never accumulates: carrying u itself
+// as a recurrence stagnated at a relative residual of ~4e-6 on the reference's tension system). The published
+// vectors are double-buffered by iteration parity. Residual replacement is not available in this form.
+template <int LPR, bool MSMEM, bool SINGLE>
 __global__ void __launch_bounds__(1024) pcg_kernel(PcgArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int G = gridDim.x, cta = blockIdx.x;
@@ -181,10 +205,13 @@ __global__ void __launch_bounds__(1024) pcg_kernel(PcgArgs a) {
   float4* qs = ps + cap;
   float4* bs = qs + cap;
   float4* dv = bs + cap;  // 3 per row
+  float4* ss = dv + 3 * cap;                  // SINGLE: s = A p
+  float4* mws = ss + (SINGLE ? cap : 0);      // SINGLE: M w
+  float4* mss = mws + (SINGLE ? cap : 0);     // SINGLE: M s
   // The 4-byte planes (a2, column indices) hold cap_blocks + 4 words rounded up to 16 bytes: block kb0 + k sits at
   // word (kb0 & 3) + k, so that a bulk copy starting at the 16-byte boundary below kb0 lands on a 16-byte boundary.
   const int cw = MSMEM ? pcg_word_plane(a.cap_blocks) : 0, sh = kb0 & 3;
-  float4* m0s = dv + 3 * cap;
+  float4* m0s = mss + (SINGLE ? cap : 0);
   float4* m1s = m0s + (MSMEM ? a.cap_blocks : 0);
   float* m8b = reinterpret_cast<float*>(m1s + (MSMEM ? a.cap_blocks : 0));
   int* colb = reinterpret_cast<int*>(m8b + cw);
@@ -258,8 +285,9 @@ __global__ void __launch_bounds__(1024) pcg_kernel(PcgArgs a) {
     xs[i] = f4(0.f, 0.f, 0.f);
     rs[i] = b;
     zs[i] = z;
-    ps[i] = z;
-    a.p0[r0 + i] = z;
+    ps[i] = SINGLE ? f4(0.f, 0.f, 0.f) : z;  // SINGLE: p, s, ms of iteration -1 are zero (beta_0 = 0)
+    if (SINGLE) ss[i] = mss[i] = f4(0.f, 0.f, 0.f);
+    a.p0[r0 + i] = z;                         // SINGLE: u_0, read by iteration 0's gathers
     acc[0] += dot3(b, z);
     acc[1] += dot3(b, b);
   }
@@ -276,6 +304,98 @@ __global__ void __launch_bounds__(1024) pcg_kernel(PcgArgs a) {
   const int passes = (n + groups - 1) / groups;
   long long tm[7] = {0, 0, 0, 0, 0, 0, 0};
 
+  if constexpr (SINGLE) {
+    float gamma = rz;  // gamma of the previous iteration
+    for (int k = 0; status == kPcgRunning; ++k) {
+      const long long t_a0 = clock64();
+      const int rd = k & 1;  // read the buffers of parity k & 1, write the other
+      // own rows to iteration k (alpha, beta of iteration k - 1)
+      if (k > 0)
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+          const float4 sv = fma4(beta, ss[i], qs[i]), pv = fma4(beta, ps[i], zs[i]);
+          const float4 r = fma4(-alpha, sv, rs[i]);
+          ss[i] = sv;
+          ps[i] = pv;
+          xs[i] = fma4(alpha, pv, xs[i]);
+          rs[i] = r;
+          zs[i] = f4(dot3(dv[3 * i], r), dot3(dv[3 * i + 1], r), dot3(dv[3 * i + 2], r));
+          mss[i] = f4(dot3(dv[3 * i], sv), dot3(dv[3 * i + 1], sv), dot3(dv[3 * i + 2], sv));
+        }
+      __syncthreads();
+      // w = A u; u of each gathered column from its published u, mw, ms (iteration k - 1)
+      const float4* Ur = rd ? a.p1 : a.p0;
+      const float4* MWr = rd ? a.mw[1] : a.mw[0];
+      const float4* MSr = rd ? a.ms[1] : a.ms[0];
+      float4* Uw = rd ? a.p0 : a.p1;
+      float4* MWw = rd ? a.mw[0] : a.mw[1];
+      float4* MSw = rd ? a.ms[0] : a.ms[1];
+      float part[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+      for (int pass = 0; pass < passes; ++pass) {
+        const int i = pass * groups + group;
+        const bool active = i < n;
+        float y0 = 0.f, y1 = 0.f, y2 = 0.f;
+        const int kb = active ? rp[i] : 0, ke = active ? rp[i + 1] : 0;
+        for (int kk = kb + gl; kk < ke; kk += LPR) {
+          const int c = MSMEM ? cols[kk] : __ldg(a.col_idx + kb0 + kk);
+          float4 uc = __ldcg(Ur + c);
+          if (k > 0) uc = fma4(-alpha, fma4(beta, __ldcg(MSr + c), __ldcg(MWr + c)), uc);
+          if (MSMEM)
+            apply(m0s[kk], m1s[kk], m8s[kk], uc, y0, y1, y2);
+          else
+            apply(__ldg(a.A.a0 + kb0 + kk), __ldg(a.A.a1 + kb0 + kk), __ldg(a.A.a2 + kb0 + kk), uc, y0, y1, y2);
+        }
+        group_reduce<LPR>(y0, y1, y2);
+        if (active && gl == 0) {
+          const float4 w = f4(y0, y1, y2), u = zs[i], r = rs[i];
+          const float4 mw = f4(dot3(dv[3 * i], w), dot3(dv[3 * i + 1], w), dot3(dv[3 * i + 2], w));
+          qs[i] = w;
+          mws[i] = mw;
+          Uw[r0 + i] = u;
+          MWw[r0 + i] = mw;
+          MSw[r0 + i] = mss[i];
+          const float4 pv = ps[i], sv = ss[i];  // p, s of iteration k - 1 (zero at k = 0)
+          part[0] += dot3(r, u);
+          part[1] += dot3(w, u);
+          part[2] += dot3(r, r);
+          part[3] += dot3(u, sv) + dot3(pv, w);
+          part[4] += dot3(pv, sv);
+        }
+      }
+      float t3[5];
+      const long long t_a1 = clock64();
+      cta_sum<5>(part, t3);
+      const long long t_a2 = clock64();
+      if (!reduce_barrier<5, 5>(a, gen++, t3)) return;
+      if (a.timing && cta == 0 && threadIdx.x == 0) {
+        tm[0] += t_a1 - t_a0;
+        tm[1] += t_a2 - t_a1;
+        tm[2] += clock64() - t_a2;
+        tm[6] += 1;
+      }
+      const float g = t3[0], d = t3[1];
+      rr = t3[2];
+      it = k;
+      if (k > 0 && rr <= a.tol2 * rr0) {
+        status = kPcgConverged;
+        break;
+      }
+      if (k >= a.max_iterations) {
+        status = kPcgIterationLimit;
+        break;
+      }
+      beta = k == 0 ? 0.0f : g / gamma;
+      // p.A p of the coming direction p = u + beta p_old, expanded over the dots of this phase (no conjugacy or
+      // orthogonality assumed, unlike the textbook delta - beta gamma / alpha, which loses p.A p in f32)
+      pq = d + beta * t3[3] + beta * beta * t3[4];
+      if (!(pq > 0.0f) || !isfinite(pq) || !isfinite(beta)) {
+        status = kPcgBreakdown;
+        break;
+      }
+      alpha = g / pq;
+      gamma = g;
+      rz = g;
+    }
+  } else
   while (status == kPcgRunning) {
     // ---- phase A: p (fused update), q = A p, partial p.q
     long long t_a0 = clock64();
@@ -533,16 +653,14 @@ __global__ void add_rows_kernel(int R, float4* d, const float4* e) {
   }
 }
 
-const void* pcg_fn(int lpr, bool msmem) {
-  if (msmem) {
-    if (lpr == 4) return reinterpret_cast<const void*>(&pcg_kernel<4, true>);
-    if (lpr == 8) return reinterpret_cast<const void*>(&pcg_kernel<8, true>);
-    if (lpr == 16) return reinterpret_cast<const void*>(&pcg_kernel<16, true>);
-  } else {
-    if (lpr == 4) return reinterpret_cast<const void*>(&pcg_kernel<4, false>);
-    if (lpr == 8) return reinterpret_cast<const void*>(&pcg_kernel<8, false>);
-    if (lpr == 16) return reinterpret_cast<const void*>(&pcg_kernel<16, false>);
-  }
+const void* pcg_fn(int lpr, bool msmem, bool single) {
+#define DRAPE_PCG_FN(L, M, S) \
+  if (lpr == L && msmem == M && single == S) return reinterpret_cast<const void*>(&pcg_kernel<L, M, S>);
+  DRAPE_PCG_FN(4, true, false) DRAPE_PCG_FN(8, true, false) DRAPE_PCG_FN(16, true, false)
+  DRAPE_PCG_FN(4, false, false) DRAPE_PCG_FN(8, false, false) DRAPE_PCG_FN(16, false, false)
+  DRAPE_PCG_FN(4, true, true) DRAPE_PCG_FN(8, true, true) DRAPE_PCG_FN(16, true, true)
+  DRAPE_PCG_FN(4, false, true) DRAPE_PCG_FN(8, false, true) DRAPE_PCG_FN(16, false, true)
+#undef DRAPE_PCG_FN
   return nullptr;
 }
 
@@ -562,14 +680,14 @@ cudaError_t allow_dynamic_smem(const void* fn) {
 
 }  // namespace
 
-size_t pcg_smem_bytes(int cap_rows, int cap_blocks, bool msmem) {
-  return size_t(cap_rows) * (6 * 16 + 3 * 16) +
+size_t pcg_smem_bytes(int cap_rows, int cap_blocks, bool msmem, bool single) {
+  return size_t(cap_rows) * ((single ? 9 : 6) * 16 + 3 * 16) +
          (msmem ? size_t(cap_blocks) * (16 + 16) + size_t(pcg_word_plane(cap_blocks)) * (4 + 4) : 0) +
          size_t(cap_rows + 1) * 4;
 }
 
-int pcg_max_grid(int threads, int lanes_per_row, size_t smem, bool msmem) {
-  const void* fn = pcg_fn(lanes_per_row, msmem);
+int pcg_max_grid(int threads, int lanes_per_row, size_t smem, bool msmem, bool single) {
+  const void* fn = pcg_fn(lanes_per_row, msmem, single);
   if (!fn) return 0;
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
@@ -580,7 +698,9 @@ int pcg_max_grid(int threads, int lanes_per_row, size_t smem, bool msmem) {
 }
 
 cudaError_t launch_pcg(const PcgArgs& a, const PcgLaunch& cfg, cudaStream_t s) {
-  const void* fn = pcg_fn(cfg.lanes_per_row, cfg.matrix_in_smem);
+  const void* fn = pcg_fn(cfg.lanes_per_row, cfg.matrix_in_smem, cfg.single_reduction);
+  if (cfg.single_reduction && (a.replace_every > 0 || !a.mw[0] || !a.mw[1] || !a.ms[0] || !a.ms[1]))
+    return cudaErrorInvalidValue;
   if (!fn || cfg.threads % 32 != 0 || cfg.threads > 1024 || cfg.grid < 1) return cudaErrorInvalidValue;
   cudaError_t e = allow_dynamic_smem(fn);
   if (e != cudaSuccess) return e;

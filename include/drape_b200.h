@@ -93,7 +93,9 @@ typedef struct {
   int32_t prolongation;        /* multilevel fine-to-coarse prolongation: 0 (default) bilinear; 1 bilinear smoothed
                                   once, (I - (4/3) lambda^{-1} D^{-1} A) P (smoothed aggregation's prolongation
                                   smoothing; level 1 becomes a 7 x 7 stencil) */
-  int32_t pad_options;
+  int32_t pcg_single_reduction; /* block-Jacobi PCG iteration form: 1 (default) one grid reduction per iteration
+                                    (Chronopoulos-Gear recurrences), used when replace_every == 0; 0 the
+                                    reference's two-reduction iteration (pcg.rs:271-296) */
 } drape_options;
 
 /* Outcome of drape_solve_equilibrium (gpu-result.json fields, run-e7.ts:100-106). */
