@@ -332,6 +332,34 @@ FULL_SOLVE = {
             16.661, 17.251, 18.468, 18.843, 19.546, 20.746, 21.452, 21.662, 22.632, 23.599, 24.356, 25.289, 25.68,
             26.142, 26.613, 27.442, 28.568, 28.888, 29.68, 29.961, 30.231],
     },
+    (129, 1, 0, 1e-07): {
+        "seconds": 8965.712,
+        "steps": 431,
+        "newton": 3237,
+        "seconds_to_1e-6": 8472.771,
+        "host": "Intel(R) Xeon(R) Processor (build container, no clock in its CPU name), 1 core",
+        "seconds_at_step": [
+            0.366, 0.785, 1.292, 1.955, 2.884, 4.157, 7.064, 39.91, 49.63, 60.976, 75.578, 77.355, 83.323,
+            102.033, 147.126, 168.781, 211.59, 236.475, 270.9, 317.883, 337.182, 376.098, 407.167, 424.768,
+            452.334, 491.779, 520.002, 557.394, 573.288, 605.738, 616.951, 650.855, 658.577, 686.719, 697.442,
+            724.934, 738.759, 766.848, 782.684, 816.623, 847.555, 859.376, 884.996, 895.156, 918.974, 930.145,
+            956.158, 972.904, 1000.422, 1016.028, 1045.767, 1065.109, 1091.45, 1103.847, 1137.064, 1161.043,
+            1190.085, 1207.554, 1247.183, 1268.312, 1298.316, 1313.962, 1342.654, 1369.212, 1415.393, 1446.949,
+            1479.8, 1507.294, 1517.52, 1541.615, 1573.308, 1598.021, 1604.048, 1630.966, 1636.861, 1656.489,
+            1685.51, 1712.012, 1721.576, 1741.144, 1766.459, 1789.404, 1796.173, 1812.526, 1838.282, 1866.343,
+            1885.819, 1889.903, 1900.014, 1926.695, 1935.9, 1961.043, 1978.794, 2009.695, 2020.099, 2053.388,
+            2059.87, 2096.711, 2106.306, 2140.13, 2151.13, 2185.051, 2195.781, 2221.775, 2229.619, 2261.79,
+            2270.308, 2300.819, 2309.233, 2337.192, 2346.582, 2384.263, 2410.179, 2414.277, 2422.433, 2450.38,
+            2463.091, 2490.254, 2504.239, 2529.289, 2553.123, 2557.752, 2569.641, 2600.317, 2610.187, 2644.243,
+            2656.823, 2692.477, 2701.367, 2729.738, 2740.825, 2775.218, 2790.942, 2820.022, 2835.408, 2873.889,
+            2886.011, 2917.516, 2926.682, 2952.542, 2974.35, 3006.1, 3020.875, 3051.847, 3067.346, 3101.975,
+            3106.224, 3149.233, 3160.137, 3200.28, 3224.53, 3260.222, 3277.43, 3316.132, 3337.037, 3367.234,
+            3394.34, 3417.197, 3437.013, 3467.221, 3480.286, 3515.739, 3544.973, 3550.751, 3568.507, 3601.066,
+            3616.833, 3649.984, 3670.063, 3674.519, 3696.005, 3699.037, 3724.183, 3754.382, 3766.618, 3800.24,
+            3810.846, 3850.346, 3864.678, 3892.855, 3901.142, 3936.882, 3944.365, 3981.211, 4005.19, 4008.95,
+            4020.785, 4053.378, 4065.284, 4097.417, 4116.42, 4145.252, 4160.847, 4172.001, 4189.752, 4218.832,
+            4233.571, 4272.941, 4276.733, 4305.249],
+    },
 }
 
 
