@@ -9,6 +9,9 @@
 // (state->done) every kernel returns at once, so a launch sequence longer than needed costs only launch latency.
 #include <cuda_runtime.h>
 
+#include <cooperative_groups.h>
+
+#include "bulk.cuh"
 #include "mg.h"
 
 namespace drape {
@@ -55,6 +58,24 @@ cudaError_t launch(void (*kernel)(Params...), int grid, int block, cudaStream_t 
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(block);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+// The same with dynamic shared memory (the kernel's ceiling raised to it first).
+template <typename... Params, typename... Args>
+cudaError_t launch_smem(void (*kernel)(Params...), int grid, int block, size_t smem, cudaStream_t s, bool pdl,
+                        Args... args) {
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -911,6 +932,229 @@ __global__ void __launch_bounds__(1024) tail_kernel(MgLevel T, MgLevel C, const 
   }
 }
 
+// The last three levels (n = 17, 9, 5: every hierarchy of five or more levels ends with them) in ONE launch of an
+// 8-CTA thread-block cluster, replacing the restriction 17 -> 9, tail_kernel and the prolongation 9 -> 17. Each
+// CTA owns a contiguous slice of the n17 rows (<= 37) and of the n9 rows (<= 11); before the programmatic wait it
+// stages its slice of both stencils into shared memory with bulk copies (the stencils are static within a solve)
+// and the coarsest inverse and smoother blocks with plain loads, so the cycle's products read shared memory. The
+// CTAs exchange the vectors that cross slices (t_17, z_9, t_9, e_9) through distributed shared memory, five
+// cluster barriers in all:
+//   t_17 = r_17 - A_17 z_17 (own rows)                                   | sync
+//   r_9 = P^T t_17, z_9 = S_9 r_9 (own rows)                             | sync
+//   t_9 = r_9 - A_9 z_9 (own rows)                                       | sync
+//   r_5 = P^T t_9, e_5 = A_5^{-1} r_5 (every CTA, all 25 rows); y_9 = z_9 + P e_5 on the fly;
+//   e_9 = y_9 + S_9^T (r_9 - A_9 y_9) (own rows)                         | sync
+//   every CTA copies all of e_9                                          | sync
+//   y_17 = z_17 + P e_9 on the fly; e_17 = y_17 + S_17^T (r_17 - A_17 y_17) (own rows, to global memory).
+// The same operations as restrict_kernel, tail_kernel and prolong_kernel on these levels, summed in another order.
+constexpr int kT3Ranks = 8;
+constexpr int kT3Threads = 512;
+constexpr int kT3N3 = 17, kT3N4 = 9, kT3N5 = 5;
+constexpr int kT3Rows3 = kT3N3 * kT3N3, kT3Rows4 = kT3N4 * kT3N4, kT3Rows5 = kT3N5 * kT3N5;
+constexpr int kT3Per3 = (kT3Rows3 + kT3Ranks - 1) / kT3Ranks;  // 37 n17 rows per CTA
+constexpr int kT3Per4 = (kT3Rows4 + kT3Ranks - 1) / kT3Ranks;  // 11 n9 rows per CTA
+constexpr int kT3M5 = 3 * kT3Rows5;                              // 75 unknowns on the coarsest level
+constexpr size_t kT3Smem = size_t(kT3Per3 + kT3Per4) * kMgStencil * 3 * sizeof(float4) + kT3M5 * kT3M5 * sizeof(float);
+constexpr long long kT3Spin = 2000000000LL;  // ~1 s of SM clock for the staging copies
+
+struct Tail3Args {
+  MgLevel L3, L4, L5;   // n = 17, 9, 5
+  const float* inv;     // the coarsest inverse, [75][75]
+  const MgState* state;
+  int* error;           // set to 3 if the staging copies did not land
+};
+
+// Block o of row `row` of a stencil slice in shared memory times v.
+__device__ __forceinline__ float3 slice_apply(const float4* A, int row, int o, float3 v) {
+  const float4* b = A + (row * kMgStencil + o) * 3;
+  const float4 u = b[0], w = b[1], t = b[2];
+  const float m[9] = {u.x, u.y, u.z, u.w, w.x, w.y, w.z, w.w, t.x};
+  return mul(m, v);
+}
+
+// (P e)(fine vertex x, y) from a coarse correction stored as 3 floats per row (nc columns).
+__device__ __forceinline__ float3 interpolate_flat(const float* e, int nc, int x, int y) {
+  const int X0 = x >> 1, Y0 = y >> 1, nx = (x & 1) ? 2 : 1, ny = (y & 1) ? 2 : 1;
+  const float w = ((x & 1) ? 0.5f : 1.0f) * ((y & 1) ? 0.5f : 1.0f);
+  float3 s = make_float3(0.f, 0.f, 0.f);
+  for (int b = 0; b < ny; ++b)
+    for (int a = 0; a < nx; ++a) {
+      const int J = (Y0 + b) * nc + X0 + a;
+      s = add3(s, scale3(w, make_float3(e[3 * J], e[3 * J + 1], e[3 * J + 2])));
+    }
+  return s;
+}
+
+// S^T d for the smoother block of local row k of a shared-memory slice [9][P].
+template <int P>
+__device__ __forceinline__ float3 smooth_local(const float (&S)[9][P], int k, float3 d) {
+  return make_float3(S[0][k] * d.x + S[3][k] * d.y + S[6][k] * d.z, S[1][k] * d.x + S[4][k] * d.y + S[7][k] * d.z,
+                     S[2][k] * d.x + S[5][k] * d.y + S[8][k] * d.z);
+}
+
+__global__ void __cluster_dims__(kT3Ranks, 1, 1) __launch_bounds__(kT3Threads) tail3_kernel(Tail3Args a) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = int(cluster.block_rank());
+  extern __shared__ __align__(16) unsigned char t3_smem[];
+  float4* A3s = reinterpret_cast<float4*>(t3_smem);       // [kT3Per3][25][3]
+  float4* A4s = A3s + kT3Per3 * kMgStencil * 3;            // [kT3Per4][25][3]
+  float* invs = reinterpret_cast<float*>(A4s + kT3Per4 * kMgStencil * 3);  // [75][75]
+  __shared__ float S3s[9][kT3Per3], S4s[9][kT3Per4];
+  __shared__ float4 t3s[kT3Per3], r4s[kT3Per4], z4s[kT3Per4], t4s[kT3Per4], e4s[kT3Per4];
+  __shared__ float4 t4_all[kT3Rows4], e4_all[kT3Rows4];
+  __shared__ float r5s[kT3M5], e5s[kT3M5];
+  __shared__ __align__(8) unsigned long long stage_bar;
+  const int i0 = rank * kT3Per3, n3 = min(kT3Rows3, i0 + kT3Per3) - i0;
+  const int I0 = rank * kT3Per4, n4 = max(0, min(kT3Rows4, I0 + kT3Per4) - I0);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, warps = kT3Threads / 32;
+  // Before the wait: the static operands (stencil slices by bulk copy, the inverse and the smoother blocks).
+  const unsigned bar = smem_addr(&stage_bar);
+  const unsigned bytes3 = unsigned(n3) * kMgStencil * 3 * 16u, bytes4 = unsigned(n4) * kMgStencil * 3 * 16u;
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    fence_proxy_async_shared();
+    mbar_arrive_expect_tx(bar, bytes3 + bytes4);
+    bulk_copy_g2s(smem_addr(A3s), a.L3.A + size_t(i0) * kMgStencil * 3, bytes3, bar);
+    if (n4 > 0) bulk_copy_g2s(smem_addr(A4s), a.L4.A + size_t(I0) * kMgStencil * 3, bytes4, bar);
+  }
+  for (int t = threadIdx.x; t < kT3M5 * kT3M5; t += kT3Threads) invs[t] = a.inv[t];
+  for (int t = threadIdx.x; t < 9 * kT3Per3; t += kT3Threads) {
+    const int e = t / kT3Per3, k = t % kT3Per3;
+    S3s[e][k] = k < n3 ? a.L3.S[e * kT3Rows3 + i0 + k] : 0.0f;
+  }
+  for (int t = threadIdx.x; t < 9 * kT3Per4; t += kT3Threads) {
+    const int e = t / kT3Per4, k = t % kT3Per4;
+    S4s[e][k] = k < n4 ? a.L4.S[e * kT3Rows4 + I0 + k] : 0.0f;
+  }
+  __syncthreads();  // the barrier's initialisation before any thread waits on it
+  pdl_wait();
+  // The copies write this CTA's shared memory: wait for them before anything else, a return included.
+  const bool landed = __syncthreads_and(mbar_wait_parity(bar, 0, kT3Spin));
+  if (!landed) {
+    if (threadIdx.x == 0) atomicExch(a.error, 3);
+    mbar_wait_parity(bar, 0, kT3Spin);
+  }
+  if (a.state && a.state->done) return;  // the same word in every CTA: all leave before the first cluster barrier
+
+  // t_17 = r_17 - A_17 z_17 on the own rows: 8 lanes per row, 64 rows per pass (every lane reaches the shuffles)
+  {
+    const int g = threadIdx.x & (kLanes - 1), k = threadIdx.x / kLanes;
+    const bool active = k < n3;
+    const int i = i0 + k, X = i % kT3N3, Y = i / kT3N3;
+    float3 acc = make_float3(0.f, 0.f, 0.f);
+    if (active)
+      for (int o = g; o < kMgStencil; o += kLanes) {
+        int j;
+        if (stencil_neighbour(kT3N3, 5, X, Y, o, &j)) acc = add3(acc, slice_apply(A3s, k, o, f3(a.L3.z[j])));
+      }
+    acc = group_sum(acc);
+    if (active && g == 0) t3s[k] = pack(sub3(f3(a.L3.r[i]), acc));
+  }
+  cluster.sync();
+  // r_9 = P^T t_17, z_9 = S_9 r_9 on the own n9 rows: one warp per row, lanes 0..8 the support rows
+  if (warp < n4) {
+    const int I = I0 + warp, X = I % kT3N4, Y = I / kT3N4;
+    float3 t = make_float3(0.f, 0.f, 0.f);
+    if (lane < 9) {
+      const int ax = lane % 3 - 1, by = lane / 3 - 1, fx = 2 * X + ax, fy = 2 * Y + by;
+      if (fx >= 0 && fy >= 0 && fx < kT3N3 && fy < kT3N3) {
+        const int j = fy * kT3N3 + fx;
+        const float4* src = cluster.map_shared_rank(t3s, j / kT3Per3);
+        t = scale3((ax ? 0.5f : 1.0f) * (by ? 0.5f : 1.0f), f3(src[j % kT3Per3]));
+      }
+    }
+    t = warp_sum3(t);
+    if (lane == 0) {
+      float sm[9];
+#pragma unroll
+      for (int e = 0; e < 9; ++e) sm[e] = S4s[e][warp];
+      r4s[warp] = pack(t);
+      z4s[warp] = pack(mul(sm, t));
+    }
+  }
+  cluster.sync();
+  // t_9 = r_9 - A_9 z_9 on the own n9 rows: one warp per row, lane o < 25 the stencil offset
+  if (warp < n4) {
+    const int I = I0 + warp, X = I % kT3N4, Y = I / kT3N4;
+    float3 acc = make_float3(0.f, 0.f, 0.f);
+    int J;
+    if (lane < kMgStencil && stencil_neighbour(kT3N4, 5, X, Y, lane, &J)) {
+      const float4* zr = cluster.map_shared_rank(z4s, J / kT3Per4);
+      acc = slice_apply(A4s, warp, lane, f3(zr[J % kT3Per4]));
+    }
+    acc = warp_sum3(acc);
+    if (lane == 0) t4s[warp] = pack(sub3(f3(r4s[warp]), acc));
+  }
+  cluster.sync();
+  // every CTA: all of t_9, r_5 = P^T t_9, e_5 = A_5^{-1} r_5
+  for (int J = threadIdx.x; J < kT3Rows4; J += kT3Threads) t4_all[J] = cluster.map_shared_rank(t4s, J / kT3Per4)[J % kT3Per4];
+  __syncthreads();
+  for (int K = warp; K < kT3Rows5; K += warps) {
+    const int X = K % kT3N5, Y = K / kT3N5;
+    float3 r = make_float3(0.f, 0.f, 0.f);
+    if (lane < 9) {
+      const int ax = lane % 3 - 1, by = lane / 3 - 1, fx = 2 * X + ax, fy = 2 * Y + by;
+      if (fx >= 0 && fy >= 0 && fx < kT3N4 && fy < kT3N4)
+        r = scale3((ax ? 0.5f : 1.0f) * (by ? 0.5f : 1.0f), f3(t4_all[fy * kT3N4 + fx]));
+    }
+    r = warp_sum3(r);
+    if (lane == 0) {
+      r5s[3 * K] = r.x;
+      r5s[3 * K + 1] = r.y;
+      r5s[3 * K + 2] = r.z;
+    }
+  }
+  __syncthreads();
+  for (int k = warp; k < kT3M5; k += warps) {
+    float v = 0.0f;
+    for (int j = lane; j < kT3M5; j += 32) v += invs[k * kT3M5 + j] * r5s[j];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) e5s[k] = v;
+  }
+  __syncthreads();
+  // e_9 = y_9 + S_9^T (r_9 - A_9 y_9), y_9 = z_9 + P e_5 formed at each neighbour
+  if (warp < n4) {
+    const int I = I0 + warp, X = I % kT3N4, Y = I / kT3N4;
+    float3 acc = make_float3(0.f, 0.f, 0.f);
+    int J;
+    if (lane < kMgStencil && stencil_neighbour(kT3N4, 5, X, Y, lane, &J)) {
+      const float4* zr = cluster.map_shared_rank(z4s, J / kT3Per4);
+      const float3 y = add3(f3(zr[J % kT3Per4]), interpolate_flat(e5s, kT3N5, J % kT3N4, J / kT3N4));
+      acc = slice_apply(A4s, warp, lane, y);
+    }
+    acc = warp_sum3(acc);
+    if (lane == 0) {
+      const float3 y = add3(f3(z4s[warp]), interpolate_flat(e5s, kT3N5, X, Y));
+      e4s[warp] = pack(add3(y, smooth_local(S4s, warp, sub3(f3(r4s[warp]), acc))));
+    }
+  }
+  cluster.sync();
+  for (int J = threadIdx.x; J < kT3Rows4; J += kT3Threads) e4_all[J] = cluster.map_shared_rank(e4s, J / kT3Per4)[J % kT3Per4];
+  cluster.sync();  // no CTA leaves while another still reads its shared memory
+  // e_17 = y_17 + S_17^T (r_17 - A_17 y_17), y_17 = z_17 + P e_9 formed at each neighbour
+  {
+    const int g = threadIdx.x & (kLanes - 1), k = threadIdx.x / kLanes;
+    const bool active = k < n3;
+    const int i = i0 + k, X = i % kT3N3, Y = i / kT3N3;
+    float3 acc = make_float3(0.f, 0.f, 0.f);
+    if (active)
+      for (int o = g; o < kMgStencil; o += kLanes) {
+        int j;
+        if (stencil_neighbour(kT3N3, 5, X, Y, o, &j)) {
+          const float3 y = add3(f3(a.L3.z[j]), interpolate(e4_all, kT3N4, j % kT3N3, j / kT3N3));
+          acc = add3(acc, slice_apply(A3s, k, o, y));
+        }
+      }
+    acc = group_sum(acc);
+    if (active && g == 0) {
+      const float3 y = add3(f3(a.L3.z[i]), interpolate(e4_all, kT3N4, X, Y));
+      a.L3.e[i] = pack(add3(y, smooth_local(S3s, k, sub3(f3(a.L3.r[i]), acc))));
+    }
+  }
+}
+
 struct ProlongArgs {
   MgFine fine;       // level-0 operator (kFine)
   MgLevel lv;        // level l: r, z (pre-smoothed), S, A; writes e
@@ -1408,6 +1652,14 @@ MgLevel level0(const MgDevice& d, int parity) {
 // Inside flexible PCG with the bilinear prolongation and at least two restricted levels, `fused` (non-null) carries
 // the update of the previous iteration, which update_restrict_kernel applies with the first restriction; the
 // stopping test then moves to the second restriction.
+// tail3_kernel applies when the hierarchy ends with the 5 x 5-stencil levels n = 17, 9, 5 below at least two more
+// levels (the restriction 1 -> 2, which holds the flexible PCG's stopping test, stays a kernel of its own).
+bool use_tail3(const MgDevice& d) {
+  const int L = d.levels;
+  return L >= 5 && d.lv[L - 3].n == kT3N3 && d.lv[L - 2].n == kT3N4 && d.lv[L - 1].n == kT3N5 &&
+         d.lv[L - 3].w == 5 && d.lv[L - 2].w == 5;
+}
+
 cudaError_t launch_cycle(const MgDevice& d, int parity, bool in_pcg, bool pdl, cudaStream_t s, int* launches,
                          const UpdateArgs* fused = nullptr) {
   const int L = d.levels;
@@ -1434,9 +1686,11 @@ cudaError_t launch_cycle(const MgDevice& d, int parity, bool in_pcg, bool pdl, c
       return e;
     ++*launches;
   }
-  // with three or more levels, the last two run in one CTA (tail_kernel: level L - 2 is a stencil level, n <= 9)
-  const bool tail = L >= 3;
-  const int last_restricted = tail ? L - 2 : L - 1;
+  // with five or more levels the last three (n = 17, 9, 5) run in one 8-CTA cluster (tail3_kernel); otherwise, with
+  // three or more, the last two run in one CTA (tail_kernel: level L - 2 is a stencil level, n <= 9)
+  const bool tail3 = use_tail3(d);
+  const bool tail = !tail3 && L >= 3;
+  const int last_restricted = tail3 ? L - 3 : tail ? L - 2 : L - 1;
   for (int l = 0; l < last_restricted; ++l) {
     RestrictArgs a{};
     a.fine = d.fine;
@@ -1461,10 +1715,21 @@ cudaError_t launch_cycle(const MgDevice& d, int parity, bool in_pcg, bool pdl, c
     if (e != cudaSuccess) return e;
     ++*launches;
   }
-  e = tail ? launch(tail_kernel, 1, 1024, s, pdl, d.lv[L - 2], d.lv[L - 1], (const float*)d.coarse_inv,
-                    (const MgState*)st)
-           : launch(coarse_solve_kernel, 1, 1024, s, pdl, d.lv[L - 1], (const float*)d.coarse_inv,
-                    (const MgState*)st);
+  if (tail3) {
+    Tail3Args ta{};
+    ta.L3 = d.lv[L - 3];
+    ta.L4 = d.lv[L - 2];
+    ta.L5 = d.lv[L - 1];
+    ta.inv = d.coarse_inv;
+    ta.state = st;
+    ta.error = d.error;
+    e = launch_smem(tail3_kernel, kT3Ranks, kT3Threads, kT3Smem, s, pdl, ta);
+  } else {
+    e = tail ? launch(tail_kernel, 1, 1024, s, pdl, d.lv[L - 2], d.lv[L - 1], (const float*)d.coarse_inv,
+                      (const MgState*)st)
+             : launch(coarse_solve_kernel, 1, 1024, s, pdl, d.lv[L - 1], (const float*)d.coarse_inv,
+                      (const MgState*)st);
+  }
   if (e != cudaSuccess) return e;
   ++*launches;
   for (int l = last_restricted - 1; l >= 0; --l) {

@@ -83,17 +83,41 @@ def test_vcycle_matches_reference(system33, prolongation):
         assert np.linalg.norm(z - zr) <= 1e-3 * np.linalg.norm(zr), np.linalg.norm(z - zr) / np.linalg.norm(zr)
 
 
+@pytest.fixture(scope="module")
+def system65():
+    d, rp, ci, blocks, grad = _mid_drape_system(65)
+    return d, ml.bsr_matrix(rp, ci, blocks), blocks, grad
+
+
+def test_vcycle_with_the_cluster_tail_matches_reference(system65):
+    """n65 has five levels (65, 33, 17, 9, 5), so its last three run in one 8-CTA thread-block cluster
+    (tail3_kernel) instead of a restriction, tail_kernel and a prolongation: the cycle still matches the f64 one."""
+    d, A, blocks, grad = system65
+    d.set_options(api.default_options(preconditioner=1))
+    H = _reference(A, 65, 0)
+    assert [l.shape[0] // 3 for l in H.A][-3:] == [289, 81, 25]
+    rng = np.random.default_rng(4)
+    for r in (-grad, rng.standard_normal(3 * d.R)):
+        z = d.precondition(r, blocks=blocks)
+        zr = H.vcycle(r)
+        assert np.linalg.norm(z - zr) <= 1e-3 * np.linalg.norm(zr), np.linalg.norm(z - zr) / np.linalg.norm(zr)
+
+
 @pytest.mark.parametrize("prolongation", [0, 1])
 def test_multilevel_pcg_converges_in_far_fewer_iterations(system33, prolongation):
     d, A, blocks, grad = system33
     b = -grad
     d.set_options(api.default_options(preconditioner=1, prolongation=prolongation))
+    # The iteration count against the f64 cycle's at rtol 1e-4: below that the f32 solve approaches its attainable
+    # accuracy on this system (its true f64 residual stays near 2e-4 of |b| however far the recursive one falls),
+    # where f32 iterations grow beyond the f64 count without saying anything about the cycle.
+    H = _reference(A, 33, prolongation)
+    x, info = d.pcg(b, 1e-4, 2000, blocks=blocks)
+    _, k_ref, st = ml.flexible_pcg(A, b, H.vcycle, 1e-4, 2000)
+    assert info["status"] == "converged" and st == "converged", info
+    assert abs(info["iterations"] - k_ref) <= 5 + 0.25 * k_ref, (info["iterations"], k_ref)
     x, info = d.pcg(b, 1e-6, 2000, blocks=blocks)
     assert info["status"] == "converged", info
-    H = _reference(A, 33, prolongation)
-    _, k_ref, st = ml.flexible_pcg(A, b, H.vcycle, 1e-6, 2000)
-    assert st == "converged"
-    assert abs(info["iterations"] - k_ref) <= 5 + 0.25 * k_ref, (info["iterations"], k_ref)
     d.set_options(api.default_options(preconditioner=0))
     xj, jac = d.pcg(b, 1e-6, 20000, blocks=blocks)
     d.set_options(api.default_options(preconditioner=1, prolongation=prolongation))
