@@ -1237,7 +1237,7 @@ Network::Network(int dev, uint64_t seed) : device(dev) {
   adam_m.alloc(kNnParams);
   adam_v.alloc(kNnParams);
   bf16.alloc(kNnBf16);
-  // Glorot-uniform weights from a 64-bit LCG, zero biases, a zero output layer (f = 0.916: the untrained network
+  // Glorot-uniform weights from a 64-bit LCG, zero biases, a zero output layer (f = 0.9: the untrained network
   // is a little under the multilevel preconditioner's spectral smoother).
   std::vector<float> p(kNnParams, 0.0f);
   uint64_t state = seed * 6364136223846793005ULL + 1442695040888963407ULL;
@@ -1417,7 +1417,7 @@ double Context::network_gradient_host(Network& net, const float* blocks, const d
     check(cudaMemcpyAsync(o.data(), nn_o_.ptr, host_.R * sizeof(float), cudaMemcpyDeviceToHost, stream_), "download");
     sync();
     for (int i = 0; i < host_.R; ++i)
-      factors[i] = 0.5f + kNnFactorSpan / (1.0f + std::exp(-(o[i] + kNnFactorShift)));
+      factors[i] = kNnFactorLow + kNnFactorSpan / (1.0f + std::exp(-(o[i] + kNnFactorShift)));
   }
   sync();
   return loss;

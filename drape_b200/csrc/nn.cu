@@ -182,7 +182,8 @@ __global__ void __launch_bounds__(128) layer_kernel(NnBuffers b, const float* in
   }
 }
 
-// o_i = w_o . h4_i + b_o; f_i = 0.5 + sigmoid(o_i) scales row i of the smoother S [9][R] (if given).
+// o_i = w_o . h4_i + b_o; f_i = kNnFactorLow + kNnFactorSpan sigmoid(o_i + kNnFactorShift) scales row i of the
+// smoother S [9][R] (if given).
 __global__ void head_kernel(NnBuffers b, const float* params, float* S) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= b.R) return;
@@ -191,7 +192,7 @@ __global__ void head_kernel(NnBuffers b, const float* params, float* S) {
   for (int n = 0; n < kH; ++n) o += params[kNnOffWo + n] * h4[n];
   b.o[i] = o;
   if (S) {
-    const float f = 0.5f + kNnFactorSpan * sigmoid(o + kNnFactorShift);
+    const float f = kNnFactorLow + kNnFactorSpan * sigmoid(o + kNnFactorShift);
 #pragma unroll
     for (int e = 0; e < 9; ++e) S[e * b.R + i] *= f;
   }

@@ -1,5 +1,5 @@
 // The preconditioner network: a mesh message-passing network that predicts, per fine-level row, a factor on the
-// multilevel preconditioner's Jacobi smoother (S_i = f_i omega D_i^{-1}, f_i in (0.5, 1)). It has no
+// multilevel preconditioner's Jacobi smoother (S_i = f_i omega D_i^{-1}, f_i in (0.8, 1)). It has no
 // counterpart in the reference. Trained on (matrix, right-hand side, PCG solution) tuples of drape solves to
 // minimise the A-norm error of one V-cycle; the flexible PCG around it (block Jacobi as fallback) decides
 // convergence on its own residual, so the converged state never depends on the network.
@@ -31,12 +31,16 @@ constexpr int kNnParams = kNnOffBo + 1;  // 34,177
 constexpr int kNnBf16 = kNnIn * kNnHidden + kNnLayers * 2 * kNnHidden * kNnHidden;  // transposed bf16 weights
 constexpr int kNnRowsPerCta = 64;       // forward layer tile (4 warps x 16 rows)
 constexpr int kNnBackRows = 32;         // backward tile
-// Smoother factor f = 0.5 + kNnFactorSpan sigmoid(o + kNnFactorShift) in (0.5, 1): f omega_0 never exceeds the
-// spectral damping omega_0, so the preconditioned operator MA stays positive definite (above f = 1 its lowest
-// eigenvalue turns negative on the drape's late-stage systems). The shift puts the trained network's operating
-// point (f ~ 0.6, o ~ -3) where the earlier (0.5, 1.135) range had it; the untrained network (o = 0) gives 0.916.
-constexpr float kNnFactorSpan = 0.5f;
-constexpr float kNnFactorShift = 1.6f;
+// Smoother factor f = kNnFactorLow + kNnFactorSpan sigmoid(o + kNnFactorShift) in (0.8, 1): f omega_0 never exceeds
+// the spectral damping omega_0, so the preconditioned operator MA stays positive definite (above f = 1 its lowest
+// eigenvalue turns negative on the drape's late-stage systems), and never falls below 0.8 omega_0: on those
+// systems flexible PCG takes the same iterations for any factor in [0.8, 1] and more below it, where the one-cycle
+// training loss (which rewards damping the bulk of the spectrum) had driven a (0.5, 1) network (f ~ 0.6: 10-35 %
+// more iterations per Newton step and slower solves than the spectral smoother on every bench seed). The untrained
+// network (o = 0) gives 0.9.
+constexpr float kNnFactorLow = 0.8f;
+constexpr float kNnFactorSpan = 0.2f;
+constexpr float kNnFactorShift = 0.0f;
 
 // Device buffers of one network evaluation / training pass over R rows and B blocks (owned by the caller).
 struct NnBuffers {

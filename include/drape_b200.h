@@ -324,13 +324,13 @@ drape_status drape_time_multilevel(drape_ctx* ctx, int32_t iterations, float* ou
 drape_status drape_pcg_profile(drape_ctx* ctx, int64_t* out7, int32_t clear);
 
 /* The preconditioner network (no counterpart in the reference): a 4-layer mesh message-passing network (hidden
- * width 64, BF16 weights, FP32 accumulation) that predicts, per fine-level row, a factor f in (0.5, 1) on the
+ * width 64, BF16 weights, FP32 accumulation) that predicts, per fine-level row, a factor f in (0.8, 1) on the
  * multilevel preconditioner's Jacobi smoother; options.preconditioner = 2 uses the network attached to the
  * context. Parameters: DRAPE_NETWORK_PARAMETERS f32 values, layout W_in[16][64] b_in[64], 4 x (W[128][64] b[64]),
  * w_out[64] b_out. The file format is "DRAPENN1", an int32 count, then the f32 values (little-endian). */
 #define DRAPE_NETWORK_PARAMETERS 34177
 typedef struct drape_network drape_network;
-/* Glorot-uniform weights from `seed`, zero biases and a zero output layer (f = 0.916: the untrained network gives
+/* Glorot-uniform weights from `seed`, zero biases and a zero output layer (f = 0.9: the untrained network gives
  * a little under the multilevel preconditioner's spectral smoother). */
 drape_status drape_network_create(int32_t device, uint64_t seed, drape_network** out);
 void drape_network_destroy(drape_network* net);

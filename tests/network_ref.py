@@ -16,7 +16,7 @@ OFF_L0 = OFF_BIN + H
 OFF_WO = OFF_L0 + LAYERS * LAYER_SIZE
 OFF_BO = OFF_WO + H
 N_PARAMS = OFF_BO + 1
-SPAN, SHIFT = np.float32(0.5), np.float32(1.6)  # f = 0.5 + SPAN sigmoid(o + SHIFT) in (0.5, 1); f(0) = 0.916
+LOW, SPAN, SHIFT = np.float32(0.8), np.float32(0.2), np.float32(0.0)  # f = LOW + SPAN sigmoid(o + SHIFT) in (0.8, 1); f(0) = 0.9
 
 
 def bf16(a):
@@ -88,7 +88,7 @@ def forward(params, feat, row_ptr, col_idx, w, bf=True):
         X = np.concatenate([hs[-1], aggregate(row_ptr, col_idx, w, hs[-1])], axis=1)
         hs.append(np.maximum(r(X) @ r(Ws[l]) + bs[l], 0.0))
     o = hs[-1] @ w_o + b_o
-    return hs, o, 0.5 + SPAN / (1.0 + np.exp(-(o + SHIFT)))
+    return hs, o, LOW + SPAN / (1.0 + np.exp(-(o + SHIFT)))
 
 
 def backward(params, feat, row_ptr, col_idx, w, hs, o, dfac):

@@ -83,19 +83,16 @@ def test_vcycle_matches_reference(system33, prolongation):
         assert np.linalg.norm(z - zr) <= 1e-3 * np.linalg.norm(zr), np.linalg.norm(z - zr) / np.linalg.norm(zr)
 
 
-@pytest.fixture(scope="module")
-def system65():
-    d, rp, ci, blocks, grad = _mid_drape_system(65)
-    return d, ml.bsr_matrix(rp, ci, blocks), blocks, grad
-
-
-def test_vcycle_with_the_cluster_tail_matches_reference(system65):
-    """n65 has five levels (65, 33, 17, 9, 5), so its last three run in one 8-CTA thread-block cluster
-    (tail3_kernel) instead of a restriction, tail_kernel and a prolongation: the cycle still matches the f64 one."""
-    d, A, blocks, grad = system65
+@pytest.mark.parametrize("n", [65, 129])
+def test_vcycle_with_the_cluster_tail_matches_reference(n):
+    """n65 and n129 have five and six levels, ending with 33, 17, 9, 5: their last three run in one 8-CTA
+    thread-block cluster (tail3_kernel) instead of a restriction, tail_kernel and a prolongation. The cycle still
+    matches the f64 one."""
+    d, rp, ci, blocks, grad = _mid_drape_system(n, steps=12)
+    A = ml.bsr_matrix(rp, ci, blocks)
     d.set_options(api.default_options(preconditioner=1))
-    H = _reference(A, 65, 0)
-    assert [l.shape[0] // 3 for l in H.A][-3:] == [289, 81, 25]
+    H = _reference(A, n, 0)
+    assert [l.shape[0] // 3 for l in H.A][-4:] == [1089, 289, 81, 25]
     rng = np.random.default_rng(4)
     for r in (-grad, rng.standard_normal(3 * d.R)):
         z = d.precondition(r, blocks=blocks)
