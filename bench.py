@@ -360,6 +360,34 @@ FULL_SOLVE = {
             4020.785, 4053.378, 4065.284, 4097.417, 4116.42, 4145.252, 4160.847, 4172.001, 4189.752, 4218.832,
             4233.571, 4272.941, 4276.733, 4305.249],
     },
+    (129, 1, 0, 5e-08): {
+        "seconds": 9193.558,
+        "steps": 436,
+        "newton": 3279,
+        "seconds_to_1e-6": 8649.817,
+        "host": "Intel(R) Xeon(R) Processor (build container, no clock in its CPU name), 1 core",
+        "seconds_at_step": [
+            0.252, 0.612, 1.096, 1.582, 2.365, 3.349, 5.371, 33.773, 40.415, 47.943, 59.426, 61.023, 66.331,
+            78.808, 114.158, 134.0, 169.197, 186.085, 216.042, 259.513, 277.803, 313.968, 338.487, 349.592,
+            369.932, 397.142, 416.001, 443.805, 455.403, 477.934, 487.788, 515.175, 522.002, 544.106, 553.037,
+            575.63, 587.111, 609.718, 621.84, 650.712, 681.015, 693.89, 721.145, 731.462, 757.417, 769.124,
+            798.536, 817.143, 844.958, 861.303, 887.201, 902.953, 929.686, 941.799, 973.687, 999.004, 1023.507,
+            1042.622, 1076.475, 1096.883, 1126.009, 1142.787, 1169.243, 1193.203, 1232.283, 1256.089, 1288.835,
+            1317.036, 1330.465, 1355.946, 1388.652, 1417.296, 1423.726, 1452.473, 1459.956, 1479.496, 1508.75,
+            1535.79, 1547.649, 1573.039, 1605.517, 1637.682, 1646.987, 1666.15, 1699.002, 1732.166, 1755.795,
+            1761.438, 1771.386, 1804.027, 1815.003, 1846.583, 1865.054, 1896.579, 1907.436, 1939.068, 1947.003,
+            1984.09, 1994.73, 2028.816, 2040.063, 2073.508, 2085.412, 2113.371, 2120.736, 2146.498, 2157.908,
+            2189.732, 2198.322, 2228.088, 2237.589, 2267.755, 2291.004, 2294.499, 2304.595, 2334.036, 2345.801,
+            2375.588, 2386.53, 2410.338, 2436.403, 2442.512, 2455.995, 2484.389, 2493.58, 2524.913, 2537.127,
+            2577.346, 2588.525, 2626.421, 2636.767, 2669.054, 2683.327, 2713.382, 2728.029, 2764.962, 2774.044,
+            2802.209, 2810.59, 2839.018, 2862.827, 2891.149, 2904.568, 2937.023, 2949.91, 2984.113, 2989.636,
+            3029.815, 3039.927, 3075.211, 3095.64, 3126.841, 3142.973, 3174.855, 3194.216, 3226.962, 3251.485,
+            3276.493, 3299.24, 3334.378, 3347.114, 3379.064, 3406.31, 3413.33, 3434.548, 3471.193, 3486.602,
+            3521.737, 3544.813, 3549.583, 3572.984, 3576.27, 3604.912, 3643.004, 3659.79, 3694.014, 3704.601,
+            3744.314, 3759.744, 3792.812, 3803.279, 3838.689, 3846.635, 3880.548, 3903.499, 3905.987, 3916.138,
+            3952.336, 3966.76, 4003.56, 4022.422, 4060.229, 4082.336, 4093.159, 4116.376, 4146.725, 4158.566,
+            4194.236, 4197.347, 4222.262],
+    },
 }
 
 
