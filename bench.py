@@ -552,7 +552,7 @@ def probe(args):
         d = api.Drape.sheet(args.n, seed=args.seed, plane=bool(args.plane),
                             options=api.default_options(preconditioner=pre, equilibrium_absolute=args.absolute,
                                                         time_budget_s=args.budget, prolongation=args.prolongation,
-                                                        forcing=args.forcing))
+                                                        forcing=args.forcing, progress=1))
         if pre == 2:
             d.set_network(api.Network.trained())
         log = d.solve_equilibrium(check=False)
