@@ -109,3 +109,38 @@ def test_learned_preconditioner_solve_reaches_an_f64_equilibrium(n):
     oracle = oracle_py.Scene("sheet", n, seed=0, plane=True)
     err, e_rel, r64 = _polished_error(oracle, gpu.state)
     assert r64 <= 1.01e-7 and err <= 1e-4 and e_rel <= 1e-9, (r64, err, e_rel)
+
+
+def test_what_the_shipped_network_gains_on_held_out_n129_systems(record_property):
+    """The trained network against the identical method without it (the multilevel preconditioner with the
+    spectral smoother), on held-out systems of the n129 bench scene (seed 0 is never trained on) at PTC depths 20
+    and 80: flexible PCG iterations to rtol 1e-6 and the host time of each solve. The shipped network gains
+    nothing on these systems (its factors sit near the lower bound of (0.8, 1), where the iteration count rises a
+    little), so the test states that loss and bounds it: both converge and the network costs at most 25 % more
+    iterations. The figures are recorded as test properties."""
+    import time
+    from drape_b200 import train_preconditioner as tp
+    net = api.Network.trained()
+    d, tuples, _ = tp.drape_tuples(129, 0, 0.25, 5e5, (20, 80), probes=0)
+    assert tuples
+    out = {}
+    for name, pre in (("multilevel", 1), ("learned", 2)):
+        d.set_options(api.default_options(preconditioner=pre))
+        if pre == 2:
+            d.set_network(net)
+        its, secs = [], []
+        for blocks, b, _ in tuples:
+            d.pcg(b, 1e-6, 2000, blocks=blocks)  # warm: hierarchy, graph
+            t0 = time.perf_counter()
+            _, info = d.pcg(b, 1e-6, 2000, blocks=blocks)
+            secs.append(time.perf_counter() - t0)
+            assert info["status"] == "converged", (name, info)
+            its.append(info["iterations"])
+        out[name] = (its, secs)
+    gain = [m / l for m, l in zip(out["multilevel"][0], out["learned"][0])]
+    record_property("pcg_iterations_multilevel", out["multilevel"][0])
+    record_property("pcg_iterations_learned", out["learned"][0])
+    record_property("seconds_multilevel", out["multilevel"][1])
+    record_property("seconds_learned", out["learned"][1])
+    record_property("iteration_gain_multilevel_over_learned", gain)
+    assert all(g >= 1 / 1.25 for g in gain), out
