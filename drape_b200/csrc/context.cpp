@@ -85,6 +85,9 @@ Context::Context(const HostProblem& problem, const drape_options& options, int d
   check(cudaStreamCreateWithFlags(&side_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
   check(cudaEventCreateWithFlags(&setup_fork_, cudaEventDisableTiming), "cudaEventCreate");
   check(cudaEventCreateWithFlags(&setup_join_, cudaEventDisableTiming), "cudaEventCreate");
+  check(cudaStreamCreateWithFlags(&net_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  check(cudaEventCreateWithFlags(&fine_ready_, cudaEventDisableTiming), "cudaEventCreate");
+  check(cudaEventCreateWithFlags(&net_done_, cudaEventDisableTiming), "cudaEventCreate");
   check(cudaMallocHost(&pinned_, kSlots * sizeof(double)), "cudaMallocHost");
   check(cudaMallocHost(&pinned_state_, sizeof(PcgSyncHeader)), "cudaMallocHost");
   check(cudaMallocHost(&pinned_mg_, sizeof(MgState) + 16), "cudaMallocHost");
@@ -94,16 +97,20 @@ Context::Context(const HostProblem& problem, const drape_options& options, int d
 Context::~Context() {
   if (stream_) cudaStreamSynchronize(stream_);
   if (side_stream_) cudaStreamSynchronize(side_stream_);
+  if (net_stream_) cudaStreamSynchronize(net_stream_);
   for (auto& e : ev_)
     if (e) cudaEventDestroy(e);
   if (setup_fork_) cudaEventDestroy(setup_fork_);
   if (setup_join_) cudaEventDestroy(setup_join_);
+  if (fine_ready_) cudaEventDestroy(fine_ready_);
+  if (net_done_) cudaEventDestroy(net_done_);
   if (sync_event_) cudaEventDestroy(sync_event_);
   if (pinned_) cudaFreeHost(pinned_);
   if (pinned_state_) cudaFreeHost(pinned_state_);
   if (pinned_mg_) cudaFreeHost(pinned_mg_);
   if (mg_graph_) cudaGraphExecDestroy(mg_graph_);
   if (side_stream_) cudaStreamDestroy(side_stream_);
+  if (net_stream_) cudaStreamDestroy(net_stream_);
   if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -1088,7 +1095,11 @@ void Context::mg_prepare() {
   const float omega = opt_.smoother_omega > 0 ? float(opt_.smoother_omega) : 0.0f;  // 0: spectral damping
   const bool reuse = omega == 0.0f && mg_setups_since_power_ < 4;
   mg_setups_since_power_ = reuse ? mg_setups_since_power_ + 1 : 1;
-  kcheck(mg_setup(mg_, omega, true, reuse, stream_, side_stream_, setup_fork_, setup_join_), "multilevel set-up");
+  const bool network = opt_.preconditioner == 2;
+  bool fine_ready = false;
+  kcheck(mg_setup(mg_, omega, true, reuse, stream_, side_stream_, setup_fork_, setup_join_,
+                  network ? fine_ready_ : nullptr, &fine_ready),
+         "multilevel set-up");
   // fine smoother, Galerkin products, coarse smoothers, coarsest inverse; the power method (twice with the
   // smoothed prolongation: the fine level first) and its scaling; Sp
   kernels_ += 2 * (mg_levels_ - 1) + (omega > 0 ? 0 : (reuse ? 0 : (kMgPowerSteps + 1) * (mg_.smoothed ? 2 : 1)) +
@@ -1096,7 +1107,14 @@ void Context::mg_prepare() {
   if (opt_.preconditioner == 2) {
     if (!net_) throw std::invalid_argument("preconditioner 2 needs a preconditioner network (drape_set_network)");
     ensure_nn_buffers();
-    kcheck(nn_forward(nnb_, net_->view(), mg_.omega, mg_.lv[0].S, stream_), "preconditioner network");
+    if (fine_ready) {  // beside the Galerkin products, joined before the solve
+      check(cudaStreamWaitEvent(net_stream_, fine_ready_, 0), "wait");
+      kcheck(nn_forward(nnb_, net_->view(), mg_.omega, mg_.lv[0].S, net_stream_), "preconditioner network");
+      check(cudaEventRecord(net_done_, net_stream_), "event");
+      check(cudaStreamWaitEvent(stream_, net_done_, 0), "join");
+    } else {
+      kcheck(nn_forward(nnb_, net_->view(), mg_.omega, mg_.lv[0].S, stream_), "preconditioner network");
+    }
     kernels_ += 2 + kNnLayers;  // features, input layer, message-passing layers, head
   }
   // the coarsest inverse (side stream) before anything that follows on the main stream

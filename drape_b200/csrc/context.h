@@ -190,6 +190,10 @@ class Context {
   // network (fork after the last Galerkin product, join before the solve)
   cudaStream_t side_stream_ = nullptr;
   cudaEvent_t setup_fork_ = nullptr, setup_join_ = nullptr;
+  // ... and the network's stream, when the set-up reuses its spectral estimates: the network needs only the fine
+  // level, so it runs beside the Galerkin products (from fine_ready_ to net_done_)
+  cudaStream_t net_stream_ = nullptr;
+  cudaEvent_t fine_ready_ = nullptr, net_done_ = nullptr;
   cudaEvent_t sync_event_ = nullptr;  // set_blocking_sync's event (null: cudaStreamSynchronize)
   bool blocking_sync_ = false;
   DevProblem dp_{};

@@ -1896,13 +1896,23 @@ cudaError_t power_method(const MgDevice& d, int first, int end, cudaStream_t s) 
 }  // namespace
 
 cudaError_t mg_setup(const MgDevice& d, float omega, bool fine_smoother, bool reuse_omega, cudaStream_t s,
-                     cudaStream_t side, cudaEvent_t fork, cudaEvent_t join) {
+                     cudaStream_t side, cudaEvent_t fork, cudaEvent_t join, cudaEvent_t fine_ready,
+                     bool* fine_ready_recorded) {
   if (d.levels < 2) return cudaErrorInvalidValue;
   cudaError_t e;
   const int first = fine_smoother ? 0 : 1, end = d.levels - 1;  // smoothed levels
   const double fixed = omega > 0.0f ? omega : 1.0;              // D^{-1} alone before the power method
   const bool spectral = omega <= 0.0f && first < end;
   if (fine_smoother) jacobi_smoother_kernel<true><<<(d.fine.R + 255) / 256, 256, 0, s>>>(d.fine, d.lv[0], fixed);
+  // Reusing the spectral estimates, the fine smoother is final right away: scale it now and mark the point, so that
+  // whatever needs only the fine level (the network) can run beside the Galerkin products.
+  const bool early_fine = fine_ready && spectral && reuse_omega && first == 0 && !d.smoothed;
+  if (fine_ready_recorded) *fine_ready_recorded = early_fine;
+  if (early_fine) {
+    const int count = 9 * d.lv[0].rows;
+    scale_smoother_kernel<<<(count + 255) / 256, 256, 0, s>>>(d.lv[0].S, count, d.omega);
+    if ((e = cudaEventRecord(fine_ready, s)) != cudaSuccess) return e;
+  }
   int l0 = 0;  // first level whose Galerkin product the bilinear loop below forms
   if (d.smoothed) {
     // The smoothed prolongation needs the level-0 spectral estimate before level 1 exists: power method on the
@@ -1954,7 +1964,7 @@ cudaError_t mg_setup(const MgDevice& d, float omega, bool fine_smoother, bool re
     // without the smoothed prolongation every smoothed level in one power method; with it, the rest
     const int from = d.smoothed && first == 0 ? 1 : first;
     if (!reuse_omega && from < end && (e = power_method(d, from, end, s)) != cudaSuccess) return e;
-    for (int l = first; l < end; ++l) {
+    for (int l = early_fine ? 1 : first; l < end; ++l) {
       const int count = 9 * d.lv[l].rows;
       scale_smoother_kernel<<<(count + 255) / 256, 256, 0, s>>>(d.lv[l].S, count, d.omega + l);
     }

@@ -117,8 +117,11 @@ int mg_level_count(int n);
 // product), and `join` is recorded behind it: the caller makes s wait for `join` before the cycle reads the inverse,
 // so that the smoother scaling and whatever the caller queues next (the network) overlap the inverse.
 constexpr int kMgPowerSteps = 10;
+// With `fine_ready`, a set-up that reuses the spectral estimates scales the fine smoother first and records the
+// event behind it (*fine_ready_recorded = true): the fine level's smoother is final there.
 cudaError_t mg_setup(const MgDevice& d, float omega, bool fine_smoother, bool reuse_omega, cudaStream_t s,
-                     cudaStream_t side = nullptr, cudaEvent_t fork = nullptr, cudaEvent_t join = nullptr);
+                     cudaStream_t side = nullptr, cudaEvent_t fork = nullptr, cudaEvent_t join = nullptr,
+                     cudaEvent_t fine_ready = nullptr, bool* fine_ready_recorded = nullptr);
 
 // Flexible PCG: clear the state and start from x = 0, r = b.
 cudaError_t mg_pcg_init(const MgDevice& d, float tol2, int max_iterations, int stall_window, cudaStream_t s);
