@@ -23,8 +23,8 @@ namespace {
 constexpr int WARPS_PER_CTA = 4;
 // Four resident CTAs per SM for assemble_rows (16 warps; 156 KB of its shared staging): the register cap this
 // sets (128 per thread, a few spilled) hides more of the f64 latency than 192 registers at 8 warps. Measured at
-// n129: 0.293 ms per assembly against 0.372 ms (two or three CTAs) and 0.343 ms (five, heavier spills); register
-// allocation does not change the arithmetic, so the blocks are bitwise the same.
+// n129: 0.293 ms per assembly against 0.372 ms (two CTAs, no cap), 0.311 ms (three) and 0.343 ms (five, heavier
+// spills); register allocation does not change the arithmetic, so the blocks are bitwise the same.
 constexpr int kAssembleMinCtas = 4;
 
 __device__ __forceinline__ double warp_sum(double v) {
