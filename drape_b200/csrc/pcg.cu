@@ -172,8 +172,7 @@ __global__ void __launch_bounds__(1024) pcg_kernel(PcgArgs a) {
   float4* bs = qs + cap;
   float4* dv = bs + cap;  // 3 per row
   float4* ss = dv + 3 * cap;                  // SINGLE: s = A p
-  float4* mws = ss + (SINGLE ? cap : 0);      // SINGLE: M w
-  float4* mss = mws + (SINGLE ? cap : 0);     // SINGLE: M s
+  float4* mss = ss + (SINGLE ? cap : 0);      // SINGLE: M s (published for the gathers)
   // The 4-byte planes (a2, column indices) hold cap_blocks + 4 words rounded up to 16 bytes: block kb0 + k sits at
   // word (kb0 & 3) + k, so that a bulk copy starting at the 16-byte boundary below kb0 lands on a 16-byte boundary.
   const int cw = MSMEM ? pcg_word_plane(a.cap_blocks) : 0, sh = kb0 & 3;
@@ -315,7 +314,6 @@ __global__ void __launch_bounds__(1024) pcg_kernel(PcgArgs a) {
           const float4 w = f4(y0, y1, y2), u = zs[i], r = rs[i];
           const float4 mw = f4(dot3(dv[3 * i], w), dot3(dv[3 * i + 1], w), dot3(dv[3 * i + 2], w));
           qs[i] = w;
-          mws[i] = mw;
           Uw[r0 + i] = u;
           MWw[r0 + i] = mw;
           MSw[r0 + i] = mss[i];
@@ -647,7 +645,7 @@ cudaError_t allow_dynamic_smem(const void* fn) {
 }  // namespace
 
 size_t pcg_smem_bytes(int cap_rows, int cap_blocks, bool msmem, bool single) {
-  return size_t(cap_rows) * ((single ? 9 : 6) * 16 + 3 * 16) +
+  return size_t(cap_rows) * ((single ? 8 : 6) * 16 + 3 * 16) +
          (msmem ? size_t(cap_blocks) * (16 + 16) + size_t(pcg_word_plane(cap_blocks)) * (4 + 4) : 0) +
          size_t(cap_rows + 1) * 4;
 }
