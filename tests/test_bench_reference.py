@@ -86,3 +86,14 @@ def test_a_large_workload_without_record_reports_the_bare_sample(fake):
     fake.n = 129
     r = bench.cpu_baseline(fake)
     assert FakeScene.budgets == [20.0] and r["sample_only"] and r["value"] == 20.0
+
+
+def test_the_committed_whole_solve_records_are_consistent():
+    """Each committed record of the oracle's whole solve: cumulative step times that grow, end no later than the
+    whole solve, and a 1e-6 N crossing inside it; the n129 ones cover the bench's default stop."""
+    assert (129, 1, 0, 5e-08) in bench.FULL_SOLVE
+    for key, r in bench.FULL_SOLVE.items():
+        t = r["seconds_at_step"]
+        assert t and all(a <= b for a, b in zip(t, t[1:])), key
+        assert t[-1] <= r["seconds"] and len(t) <= r["steps"] and r["seconds_to_1e-6"] <= r["seconds"], key
+        assert r["newton"] >= r["steps"], key
